@@ -1,0 +1,403 @@
+"""Benchmark: PIMC++ bisection moves on one B200 (config C2 by default).
+
+Workload (synthetic, seeded; the reference publishes no dataset): 512
+Lennard-Jones He-4 atoms at 0.02186 A^-3, T = 1.5 K, M = 128 time slices,
+PAtricubicFit pair action on a 200x50x50 (q, y, t) grid, bisection level 4,
+one chain.  A step is a batch of `--moves` BisectionBlock moves run on the
+device by one launch of the bisection kernel.
+
+Arms:
+  default            the CUDA library: FP64 and mixed-precision device moves.
+  --impl reference   the reference's CPU algorithm (the FP64 oracle
+                     restatement; the reference itself cannot be built here)
+                     on all host cores, one independent chain per core.
+
+Prints one JSON line (rank 0).  Under torchrun each rank runs an independent
+replica chain on its own GPU (the reference's clone parallelism); `value`
+adds all ranks' pair evaluations over the slowest rank's time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import multiprocessing as mp
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "pair-action evals/s & bisection moves/s, mixed vs FP64 GPU at ΔS relerr≤1e-6"
+UNIT = "pair-action evals/s"
+# Algorithmic bytes per tricubic pair evaluation: partner at two slices (48 B
+# FP64 / 24 B FP32) + 8 nodes x 8 coefficients (512 B FP64 / 256 B FP32).
+BYTES_PER_EVAL = {"fp64": 560, "mixed": 280}
+
+
+def load_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def c2_setup(nq=200, ny=50, nt=50):
+    from pimcplusplus_b200 import workloads as W
+    cfg = dict(W.CONFIGS["C2"])
+    tau, box = W.derived(cfg)
+    tabs = W.tricubic_tables(box[0], tau, cfg["levels"], nq=nq, ny=ny, nt=nt)
+    return cfg, tau, box, tabs
+
+
+def initial_path(n, slices, box, seed, radius):
+    """Uniform random positions with an exclusion radius, every slice equal
+    (InitRandomFixed semantics, InitPaths.cc:966-999, from a numpy stream)."""
+    rng = np.random.default_rng(seed)
+    pts = np.zeros((n, 3))
+    for i in range(n):
+        for _ in range(1000):
+            c = (rng.random(3) - 0.5) * box
+            d = pts[:i] - c
+            d -= np.round(d / box) * box
+            if i == 0 or np.min(np.sum(d * d, axis=1)) >= 4 * radius * radius:
+                break
+        pts[i] = c
+    return np.repeat(pts[None], slices, axis=0)
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle samples during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax.append(float(f[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+# CPU arm: the oracle (FP64 restatement of the reference's loops)
+# ---------------------------------------------------------------------------
+def _pair_evals_of(records, n, levels):
+    """Pair evaluations the reference performs for these moves (old+new, all
+    stages attempted; ShortRange at every level)."""
+    total = 0
+    for r in records:
+        attempted = r.stages_passed + (0 if r.accepted else 1)
+        for k in range(attempted):
+            level = levels - 1 - k
+            total += 2 * (n - 1) * ((1 << levels) >> level)
+    return total
+
+
+def _cpu_worker(args):
+    seed, seconds, nq, ny, nt = args
+    import oracle as O
+    cfg, tau, box, tabs = c2_setup(nq, ny, nt)
+    qg, yg, tg, umat, dumat, pg, pot = tabs
+    n, slices, L = cfg["N"], cfg["M"] + 1, cfg["levels"]
+    s = O.System(n, slices, box, tau, 6.0596, 0)
+    pa = O.PairAction.tricubic(qg, yg, tg, tau, umat, dumat, pg, pot)
+    s.set_pa(pa)
+    s.set_path(initial_path(n, slices, box, seed, 0.45 * 2.556))
+    s.bisection_config(L, 1)
+    s.rng_seed(seed)
+    s.run_bisection(20)  # warm-up
+    evals = moves = acc = 0
+    t0 = time.perf_counter()
+    while time.perf_counter() - t0 < seconds:
+        recs = s.run_bisection(50)
+        evals += _pair_evals_of(recs, n, L)
+        moves += len(recs)
+        acc += sum(r.accepted for r in recs)
+    dt = time.perf_counter() - t0
+    return evals, moves, acc, dt
+
+
+def cpu_baseline(cores, seconds):
+    import oracle as O
+    O.build()
+    if cores == 1:
+        res = [_cpu_worker((1000, seconds, 200, 50, 50))]
+    else:
+        ctx = mp.get_context("spawn")
+        with ctx.Pool(cores) as pool:
+            res = pool.map(_cpu_worker, [(1000 + i, seconds, 200, 50, 50) for i in range(cores)])
+    evals = sum(r[0] for r in res)
+    moves = sum(r[1] for r in res)
+    acc = sum(r[2] for r in res)
+    dt = max(r[3] for r in res)
+    return dict(value=evals / dt, moves_per_s=moves / dt, accepted_per_s=acc / dt, cores=cores,
+                sample=f"{moves} moves of C2 (FP64 oracle, {cores} independent chain(s), {dt:.1f} s)")
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    cores = os.cpu_count() or 1
+    seconds = max(2.0, min(20.0, 60.0 / max(1, args.steps + args.warmup)))
+    for _ in range(args.warmup):
+        cpu_baseline(cores, 1.0)
+    vals = []
+    last = None
+    for _ in range(args.steps):
+        last = cpu_baseline(cores, seconds)
+        vals.append(last["value"])
+    value = float(np.mean(vals))
+    cfg, tau, box, _ = c2_setup(8, 4, 4)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": seconds * 1000.0, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": W_NAME, "N": 512, "M": 128, "levels": 4, "table": "tricubic 200x50x50"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port", "sample": last["sample"]},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "moves_per_s": last["moves_per_s"],
+        "note": "reference cannot be built here (Blitz++, SPRNG2, GSL, HDF5, LAPACK absent); "
+                "its loops are timed through the FP64 oracle restatement",
+    }
+    print(json.dumps(line), flush=True)
+
+
+W_NAME = "C2: 512 LJ He-4, rho 0.02186/A^3, T=1.5 K, M=128, PAtricubicFit 200x50x50, bisection level 4, 1 chain"
+
+
+# ---------------------------------------------------------------------------
+# GPU arm
+# ---------------------------------------------------------------------------
+def run_ours(args):
+    import torch
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+    torch.cuda.set_device(local)
+    import pimcplusplus_b200 as P
+
+    cfg, tau, box, tabs = c2_setup()
+    qg, yg, tg, umat, dumat, pg, pot = tabs
+    n, slices, L = cfg["N"], cfg["M"] + 1, cfg["levels"]
+    start = initial_path(n, slices, box, 17 + rank, 0.45 * 2.556)
+
+    def make(precision, shadow=False, cl=args.cluster, threads=args.threads):
+        d = P.PathData(n, slices, box, tau, 6.0596, 0, device=local)
+        d.pa_tricubic(qg, yg, tg, tau, umat, dumat, pg, pot)
+        d.set_path(start)
+        bb = P.BisectionBlock(d, L, 1, precision=precision, shadow=shadow, cluster_ctas=cl, threads_per_cta=threads)
+        bb.seed(1000 + rank)
+        return d, bb
+
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=f"cuda:{local}")
+
+    def timed(precision):
+        d, bb = make(precision)
+        stream = torch.cuda.ExternalStream(P.lib().pimc_stream(d.h), device=f"cuda:{local}")
+        for _ in range(args.warmup):
+            bb.launch_async(args.moves)
+        d.synchronize()
+        s0 = bb.stats()
+        times = []
+        sampler = ClockSampler(local) if rank == 0 else None
+        if sampler:
+            sampler.start()
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        for _ in range(args.steps):
+            with torch.cuda.stream(stream):
+                flush.zero_()  # L2 flush between steps, outside the timed events
+                e0 = torch.cuda.Event(enable_timing=True)
+                e1 = torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                bb.launch_async(args.moves)
+                e1.record(stream)
+            e1.synchronize()
+            times.append(e0.elapsed_time(e1))
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        clocks = sampler.stop() if sampler else None
+        s1 = bb.stats()
+        if s1["status"]:
+            raise RuntimeError(f"device status {s1['status']}")
+        ms = float(np.sum(times))
+        st = {k: s1[k] - s0[k] for k in ("moves", "accepted", "pair_evals", "stages_attempted")}
+        d.close()
+        return ms, st, clocks
+
+    def agg(ms, st):
+        if not dist:
+            return ms, st
+        t = torch.tensor([ms], dtype=torch.float64, device=f"cuda:{local}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        v = torch.tensor([st["pair_evals"], st["moves"], st["accepted"]], dtype=torch.float64,
+                         device=f"cuda:{local}")
+        dist.all_reduce(v)
+        return float(t.item()), dict(pair_evals=int(v[0].item()), moves=int(v[1].item()),
+                                     accepted=int(v[2].item()))
+
+    ms64, st64, _ = timed(P.FP64)
+    ms32, st32, clocks = timed(P.MIXED)
+    ms64, st64 = agg(ms64, st64)
+    ms32, st32 = agg(ms32, st32)
+
+    # dS accuracy of the mixed path: mixed decisions with the FP64 terms alongside
+    d, bb = make(P.MIXED, shadow=True)
+    bb.MakeMoves(200, trace=False)
+    rec, sh = bb.MakeMoves(args.accuracy_moves, trace=True)
+    d.close()
+    m = rec["dS_shadow"] != 0.0
+    rel = np.abs(rec["dS"][m] - rec["dS_shadow"][m]) / np.abs(rec["dS_shadow"][m])
+    flip_rate = sh["flips"] / max(1, sh["stages_attempted"])
+
+    # end to end through the public API: host path in, moves, path + counters out
+    d, bb = make(P.MIXED)
+    host = start.copy()
+    for _ in range(2):
+        d.set_path(host)
+        bb.MakeMoves(args.moves, trace=False)
+        host = d.get_path(P.OLDMODE)
+    e2e_t, e2e_evals = 0.0, 0
+    for _ in range(args.steps):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        d.set_path(host)
+        _, st = bb.MakeMoves(args.moves, trace=False)
+        host = d.get_path(P.OLDMODE)
+        e2e_t += time.perf_counter() - t0
+    e2e_evals = bb.stats()["pair_evals"]
+    d.close()
+    e2e_evals_timed = e2e_evals * args.steps / (args.steps + 2)
+    if dist:
+        t = torch.tensor([e2e_t], dtype=torch.float64, device=f"cuda:{local}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_t = float(t.item())
+        v = torch.tensor([e2e_evals_timed], dtype=torch.float64, device=f"cuda:{local}")
+        dist.all_reduce(v)
+        e2e_evals_timed = float(v.item())
+
+    if rank == 0:
+        peak, peak_kind = load_peaks()
+        value = st32["pair_evals"] / (ms32 / 1000.0)
+        value64 = st64["pair_evals"] / (ms64 / 1000.0)
+        per_launch_bytes = st32["pair_evals"] / world / args.steps * BYTES_PER_EVAL["mixed"]
+        achieved = per_launch_bytes / (ms32 / args.steps / 1000.0) / 1e9
+        traffic = None
+        prof = os.path.join(ROOT, "profiles", "bisection_c2_traffic.json")
+        if os.path.exists(prof):
+            with open(prof) as f:
+                pj = json.load(f)
+            traffic = pj.get("dram_bytes_per_pair_eval_mixed", 0) * st32["pair_evals"] / world / args.steps
+        cpu = cpu_baseline(1, args.cpu_seconds) if world == 1 and not args.no_cpu else None
+        path_bytes = n * slices * 3 * 8
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms32 / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32 pair terms / f64 sums", "data": "synthetic",
+            "config": {"workload": W_NAME, "moves_per_step": args.moves, "cluster_ctas": args.cluster,
+                       "threads_per_cta": args.threads,
+                       "l2": "flushed between steps by a 256 MiB write outside the timed events",
+                       "parallelism": f"replicas x{world}"},
+            "moves_per_s": st32["moves"] / (ms32 / 1000.0),
+            "accepted_moves_per_s": st32["accepted"] / (ms32 / 1000.0),
+            "fp64": {"pair_evals_per_s": value64, "moves_per_s": st64["moves"] / (ms64 / 1000.0),
+                     "accepted_moves_per_s": st64["accepted"] / (ms64 / 1000.0), "ms_per_step": ms64 / args.steps},
+            "mixed_over_fp64": value / value64 if value64 else None,
+            "dS_relerr": {"median": float(np.median(rel)) if rel.size else None,
+                          "p99": float(np.quantile(rel, 0.99)) if rel.size else None,
+                          "max": float(np.max(rel)) if rel.size else None, "stages": int(rel.size),
+                          "flip_rate": flip_rate},
+            "e2e": {"value": e2e_evals_timed / e2e_t if e2e_t else None, "unit": UNIT,
+                    "h2d_bytes_per_step": path_bytes, "d2h_bytes_per_step": path_bytes + 48},
+            "gpu_launches": args.steps * 2,
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
+                         "bytes_per_eval": BYTES_PER_EVAL["mixed"],
+                         "kernel": "bisection_kernel<PA_TRICUBIC,float>"},
+            "clocks": clocks,
+        }
+        if cpu:
+            line["cpu_baseline"] = {"value": cpu["value"], "unit": UNIT, "cores": cpu["cores"], "kind": "port",
+                                    "sample": cpu["sample"]}
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--moves", type=int, default=2048)
+    ap.add_argument("--cluster", type=int, default=8)
+    ap.add_argument("--threads", type=int, default=256)
+    ap.add_argument("--accuracy-moves", type=int, default=1000)
+    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

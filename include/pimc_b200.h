@@ -1,0 +1,216 @@
+/*
+ * pimc_b200.h — C ABI of the B200 (sm_100a) action-evaluation library for
+ * PIMC++ path-integral Monte Carlo.
+ *
+ * The library owns device copies of the path (OLD/NEW mirrored, like
+ * MirroredClass), the pair-action tables and the rho_k cache, and evaluates
+ * the actions a bisection move needs.  Plain pointers and sizes only; every
+ * entry point returns an int status (0 = PIMC_OK) and never throws.  A
+ * context is not thread-safe: one context per host thread, one CUDA stream
+ * per context.
+ *
+ * Path layout everywhere: row-major [slice][particle][3] doubles, with
+ * num_time_slices = M+1 rows, the layout of PathClass::Path (Blitz
+ * Array<dVec,2>, PathClass.cc:295-443).
+ *
+ * Reference interfaces replaced (paths relative to the reference root):
+ *   ActionBaseClass::SingleAction / d_dBeta      PIMC++/src/Actions/ActionBase.h:43,57
+ *   ShortRangeClass::SingleAction / d_dBeta      PIMC++/src/Actions/ShortRangeClass.cc:191,316
+ *   KineticClass::SingleAction / d_dBeta         PIMC++/src/Actions/KineticClass.cc:33,187
+ *   LongRangeClass::SingleAction / d_dBeta       PIMC++/src/Actions/LongRangeClass.cc:273,374
+ *   PathClass::UpdateRho_ks                      PIMC++/src/PathClass.cc:649
+ *   PathClass::AcceptCopy / RejectCopy           PIMC++/src/PathClass.cc:797,865
+ *   DavidPAClass::Read(…Daviddmfile…)            Common/PairAction/DavidPAClass.h:144
+ *   PAtricubicFitClass::Read                     Common/PairAction/PAtricubicFit.cc:794
+ *   BisectionBlockClass::MakeMove                PIMC++/src/Moves/BisectionBlock.cc:380
+ */
+#ifndef PIMC_B200_H
+#define PIMC_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ---- */
+#define PIMC_OK 0
+#define PIMC_E_ARG 1      /* invalid argument (sizes, indices, null pointers) */
+#define PIMC_E_CUDA 2     /* a CUDA runtime call failed */
+#define PIMC_E_NAN 3      /* a kernel produced a non-finite action */
+#define PIMC_E_INDEX 4    /* a kernel saw an out-of-range index and skipped it */
+#define PIMC_E_CAP 5      /* a bounded device loop hit its iteration cap */
+#define PIMC_E_FILE 6     /* an input file is missing or malformed */
+#define PIMC_E_STATE 7    /* call out of order (e.g. no pair action set) */
+#define PIMC_E_NOMEM 8    /* device or host allocation failed */
+#define PIMC_E_STAGING 9  /* |S| > 1e50 on an accepted stage (StageClass.cc:74-85) */
+
+/* ---- enumerations ---- */
+#define PIMC_OLD 0
+#define PIMC_NEW 1
+#define PIMC_BOTH 2
+
+#define PIMC_FP64 0   /* plain FP64 evaluation */
+#define PIMC_MIXED 1  /* FP32 pair terms and phases, FP64 accumulation and Metropolis */
+
+#define PIMC_ACTION_SHORTRANGE 0
+#define PIMC_ACTION_KINETIC 1
+#define PIMC_ACTION_LONGRANGE 2
+
+#define PIMC_GRID_LINEAR 0
+#define PIMC_GRID_LOG 1
+
+typedef struct pimc_context pimc_context;
+
+/* The system a context simulates: PathClass::Read (PathClass.cc:123-278) and
+ * SpeciesClass::Read (SpeciesClass.cc:19-60) after input parsing. */
+typedef struct pimc_system_desc {
+  int num_particles;        /* N over all species */
+  int num_time_slices;      /* path rows, M+1 on one process (PathClass.cc:305) */
+  double box[3];            /* periodic box (all three dimensions periodic) */
+  double tau;               /* imaginary-time step */
+  int num_species;
+  const int *species_of;    /* [num_particles] species of each particle */
+  const double *lambda;     /* [num_species] hbar^2/(2m) */
+  int num_images;           /* Action{NumImages} for kinetic/sampling image sums */
+  int device;               /* CUDA device ordinal */
+} pimc_system_desc;
+
+const char *pimc_status_string(int status);
+int pimc_version(void);
+
+/* Creates a context on desc->device: allocates the path copies and a stream. */
+int pimc_create(const pimc_system_desc *desc, pimc_context **out);
+int pimc_destroy(pimc_context *ctx);
+/* Copies the last error message of this context into buf (NUL-terminated). */
+int pimc_last_error(pimc_context *ctx, char *buf, int len);
+
+/* ---- pair actions: PairMatrix(sp1,sp2) of ActionsClass (ActionsClass.cc:147-211) ---- */
+
+/* A DavidPAClass fit from an ASCII squarer .dm file (DavidPAClass.cc:635-912):
+ * the NMax==2 fit, column 0 = potential, last grid row zeroed, natural start /
+ * zero-slope end splines, TauPos chosen from desc->tau.  num_offdiag_terms is
+ * Fits{NumOffDiagonalTerms} of the PairAction section. */
+int pimc_pa_david_from_dm(pimc_context *ctx, int sp1, int sp2, const char *dm_path,
+                          int num_offdiag_terms);
+
+/* Host-only (no GPU needed): the reader behind pimc_pa_david_from_dm.
+ * pimc_dm_read_info reports the table shape; pimc_dm_read_tables fills
+ * [num_tau][num_grid][num_cols] arrays: ukj values and second derivatives,
+ * dukj values and second derivatives (any pointer may be NULL). */
+int pimc_dm_read_info(const char *dm_path, double desired_tau, int *num_grid, int *num_cols, int *num_tau,
+                      int *tau_pos, int *grid_type, double *grid_start, double *grid_end);
+int pimc_dm_read_tables(const char *dm_path, double desired_tau, double *ukj, double *ukj_d2, double *dukj,
+                        double *dukj_d2);
+
+/* The same fit from arrays already read: ukj and dukj are
+ * [num_tau][num_grid][num_cols] with column 0 the potential (the tempUkj2 /
+ * tempdUkj2 arrays of ReadDavidSquarerFile). */
+int pimc_pa_david(pimc_context *ctx, int sp1, int sp2, int grid_type, double grid_start,
+                  double grid_end, int num_grid, int num_cols, int num_tau, const double *ukj,
+                  const double *dukj, int tau_pos, int num_offdiag_terms);
+
+/* A PAtricubicFitClass fit (PAtricubicFit.cc:659-721,794-865): linear q, y, t
+ * grids given as {start, end, n}; umat/dumat are [num_betas][nq][ny][nt] node
+ * values for beta = smallest_beta * 2^level; the potential for the primitive
+ * fallback is a natural cubic spline (SplinePot, Common/PH/SplinePot.cc) on a
+ * linear grid {pot_start, pot_end, pot_n}, zero beyond pot_end. */
+int pimc_pa_tricubic(pimc_context *ctx, int sp1, int sp2, const double qgrid[3],
+                     const double ygrid[3], const double tgrid[3], int num_betas,
+                     double smallest_beta, const double *umat, const double *dumat, double pot_start,
+                     double pot_end, int pot_n, const double *pot_data);
+
+/* ---- path state (PathClass / MirroredClass) ---- */
+int pimc_set_path(pimc_context *ctx, int copy, const double *path);
+int pimc_get_path(pimc_context *ctx, int copy, double *path);
+
+/* ---- ActionBaseClass drop-in ---- */
+
+/* ActionBaseClass::SingleAction(slice1, slice2, activeParticles, level) of the
+ * action `action` on path copy `copy` (the reference's global ActiveCopy made
+ * explicit).  Short-range and kinetic sum links [slice1, slice2) with step
+ * 2^level; the long-range action sums slices [slice1, slice2] and, on the NEW
+ * copy, first updates rho_k like LongRangeClass::SingleAction. */
+int pimc_single_action(pimc_context *ctx, int action, int copy, int slice1, int slice2,
+                       const int *active, int n_active, int level, int precision, double *out);
+
+/* ActionBaseClass::d_dBeta(slice1, slice2, level) on the OLD copy. */
+int pimc_d_dbeta(pimc_context *ctx, int action, int slice1, int slice2, int level, double *out);
+
+/* PathClass::AcceptCopy / RejectCopy for slices [slice1, slice2] of the active
+ * particles (PutInBoxFast on NEW, then NEW->OLD; or OLD->NEW), rho_k included. */
+int pimc_accept_copy(pimc_context *ctx, int slice1, int slice2, const int *active, int n_active);
+int pimc_reject_copy(pimc_context *ctx, int slice1, int slice2, const int *active, int n_active);
+
+/* ---- long range (PathClass k-vectors, rho_k; LongRangeClass tables) ---- */
+
+/* PathClass::SetupkVecs3D (PathClass.cc:534-586); returns the count in *num_k. */
+int pimc_setup_kvecs(pimc_context *ctx, double kcutoff, int *num_k);
+int pimc_get_kvecs(pimc_context *ctx, double *kvecs /* [num_k][3] */);
+/* The breakup output of LongRangeClass::Init for the single species pair:
+ * arrays over levels (and k for *_k, [num_levels][num_k]). */
+int pimc_set_longrange(pimc_context *ctx, int num_levels, const double *ulong_k,
+                       const double *ulong_r0, const double *ushort_k0, const double *ulong_k0,
+                       const double *dulong_k, const double *dulong_r0, const double *dushort_k0,
+                       const double *dulong_k0, int use_background);
+/* PathClass::UpdateRho_ks() full recompute (PathClass.cc:710-718), and the
+ * incremental UpdateRho_ks(slice1, slice2, active, level) (:649-707). */
+int pimc_calc_rhok(pimc_context *ctx);
+int pimc_update_rhok(pimc_context *ctx, int slice1, int slice2, const int *active, int n_active,
+                     int level);
+int pimc_get_rhok(pimc_context *ctx, int copy, double *out /* [slices][num_k][2] */);
+
+/* ---- device-resident bisection moves (BisectionBlockClass::MakeMove) ---- */
+
+typedef struct pimc_bisection_desc {
+  int num_levels;                   /* Move{NumLevels} */
+  int steps_per_block;              /* Move{StepsPerBlock} */
+  int shortrange_at_higher_levels;  /* ShortRange in HigherLevelActions */
+  int use_longrange;                /* LongRange pushed at the lowest level */
+  int precision;                    /* PIMC_FP64 or PIMC_MIXED */
+  int shadow;                       /* also evaluate the other precision, for dS error */
+  int cluster_ctas;                 /* CTAs cooperating on one chain (1..16), 0 = auto */
+  int threads_per_cta;              /* 0 = auto */
+} pimc_bisection_desc;
+
+/* One move: the fields the accept trace is compared on. */
+typedef struct pimc_move_record {
+  int32_t slice1;
+  int32_t ptcl;
+  int32_t accepted;       /* whole move accepted */
+  int32_t stages_passed;  /* bisection stages accepted */
+  double dS[8];           /* S_new - S_old per stage attempted, highest level first */
+  double dS_shadow[8];    /* the same in the other precision (shadow mode), else 0 */
+} pimc_move_record;
+
+typedef struct pimc_bisection_stats {
+  int64_t moves;
+  int64_t accepted;
+  int64_t stages_attempted;
+  int64_t pair_evals;     /* U(q,z,s^2) evaluations, old+new, all stages attempted */
+  int64_t flips;          /* shadow mode: stage decisions the other precision would flip */
+  int32_t status;         /* device status word: 0, PIMC_E_NAN, PIMC_E_STAGING, PIMC_E_CAP */
+  int32_t pad;
+} pimc_bisection_stats;
+
+int pimc_bisection_setup(pimc_context *ctx, const pimc_bisection_desc *desc);
+/* Seeds the Local stream of the chain (Philox-4x32-10 key; counter reset). */
+int pimc_rng_seed(pimc_context *ctx, uint64_t seed);
+/* Runs n_blocks BisectionBlock moves on the device (OLD copy is the state;
+ * NEW is brought back in sync afterwards).  trace: n_blocks*steps_per_block
+ * records or NULL.  stats: accumulated since the last pimc_bisection_setup. */
+int pimc_run_bisection(pimc_context *ctx, int n_blocks, pimc_move_record *trace,
+                       pimc_bisection_stats *stats);
+/* Enqueues n_blocks moves on the context stream without synchronising or
+ * copying anything back (for timing); pimc_bisection_stats reads the totals. */
+int pimc_run_bisection_async(pimc_context *ctx, int n_blocks);
+int pimc_bisection_get_stats(pimc_context *ctx, pimc_bisection_stats *stats);
+int pimc_synchronize(pimc_context *ctx);
+/* The CUDA stream of the context (cudaStream_t as void*). */
+void *pimc_stream(pimc_context *ctx);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,354 @@
+"""B200-native action evaluation for PIMC++ path-integral Monte Carlo.
+
+Python host layer over the C ABI of libpimc_b200.so (include/pimc_b200.h).
+It mirrors the reference's Action interface: `ShortRangeClass`,
+`KineticClass` expose SingleAction(slice1, slice2, activeParticles, level) and
+d_dBeta(slice1, slice2, level) with the reference's argument meaning
+(PIMC++/src/Actions/ActionBase.h:43-57), `PathData.SetMode` selects the OLD
+or NEW mirrored copy (MirroredClass.cc:19), and `BisectionBlock` runs
+BisectionBlockClass::MakeMove (PIMC++/src/Moves/BisectionBlock.cc:380-451)
+entirely on the device.
+
+The CUDA library is required: importing this package raises ImportError if
+libpimc_b200.so is missing, and there is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libpimc_b200.so")
+
+if not os.path.exists(LIB_PATH):
+    raise ImportError(
+        f"{LIB_PATH} is missing: build it with `python -m pimcplusplus_b200.build_lib` (nvcc, sm_100a)")
+
+_lib = C.CDLL(LIB_PATH)
+
+PIMC_OK = 0
+OLDMODE, NEWMODE, BOTH = 0, 1, 2
+FP64, MIXED = 0, 1
+ACTION_SHORTRANGE, ACTION_KINETIC, ACTION_LONGRANGE = 0, 1, 2
+GRID_LINEAR, GRID_LOG = 0, 1
+
+STATUS = {
+    0: "ok", 1: "invalid argument", 2: "CUDA error", 3: "non-finite action", 4: "index out of range",
+    5: "device loop cap reached", 6: "file missing or malformed", 7: "call out of order", 8: "allocation failed",
+    9: "broken staging",
+}
+
+
+class PimcError(RuntimeError):
+    def __init__(self, status, msg=""):
+        super().__init__(f"{STATUS.get(status, status)} ({status}): {msg}")
+        self.status = status
+
+
+class SystemDesc(C.Structure):
+    _fields_ = [
+        ("num_particles", C.c_int),
+        ("num_time_slices", C.c_int),
+        ("box", C.c_double * 3),
+        ("tau", C.c_double),
+        ("num_species", C.c_int),
+        ("species_of", C.POINTER(C.c_int)),
+        ("lambda_", C.POINTER(C.c_double)),
+        ("num_images", C.c_int),
+        ("device", C.c_int),
+    ]
+
+
+class BisectionDesc(C.Structure):
+    _fields_ = [
+        ("num_levels", C.c_int),
+        ("steps_per_block", C.c_int),
+        ("shortrange_at_higher_levels", C.c_int),
+        ("use_longrange", C.c_int),
+        ("precision", C.c_int),
+        ("shadow", C.c_int),
+        ("cluster_ctas", C.c_int),
+        ("threads_per_cta", C.c_int),
+    ]
+
+
+class BisectionStats(C.Structure):
+    _fields_ = [
+        ("moves", C.c_int64),
+        ("accepted", C.c_int64),
+        ("stages_attempted", C.c_int64),
+        ("pair_evals", C.c_int64),
+        ("flips", C.c_int64),
+        ("status", C.c_int32),
+        ("pad", C.c_int32),
+    ]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_ if k != "pad"}
+
+
+MOVE_RECORD = np.dtype([
+    ("slice1", np.int32), ("ptcl", np.int32), ("accepted", np.int32), ("stages_passed", np.int32),
+    ("dS", np.float64, (8,)), ("dS_shadow", np.float64, (8,)),
+])
+
+_d, _i, _p = C.c_double, C.c_int, C.c_void_p
+_dp, _ip = C.POINTER(C.c_double), C.POINTER(C.c_int)
+_SIGS = {
+    "pimc_status_string": (C.c_char_p, [_i]),
+    "pimc_version": (_i, []),
+    "pimc_create": (_i, [C.POINTER(SystemDesc), C.POINTER(_p)]),
+    "pimc_destroy": (_i, [_p]),
+    "pimc_last_error": (_i, [_p, C.c_char_p, _i]),
+    "pimc_pa_david_from_dm": (_i, [_p, _i, _i, C.c_char_p, _i]),
+    "pimc_dm_read_info": (_i, [C.c_char_p, _d, _ip, _ip, _ip, _ip, _ip, _dp, _dp]),
+    "pimc_dm_read_tables": (_i, [C.c_char_p, _d, _dp, _dp, _dp, _dp]),
+    "pimc_pa_david": (_i, [_p, _i, _i, _i, _d, _d, _i, _i, _i, _dp, _dp, _i, _i]),
+    "pimc_pa_tricubic": (_i, [_p, _i, _i, _dp, _dp, _dp, _i, _d, _dp, _dp, _d, _d, _i, _dp]),
+    "pimc_set_path": (_i, [_p, _i, _dp]),
+    "pimc_get_path": (_i, [_p, _i, _dp]),
+    "pimc_single_action": (_i, [_p, _i, _i, _i, _i, _ip, _i, _i, _i, _dp]),
+    "pimc_d_dbeta": (_i, [_p, _i, _i, _i, _i, _dp]),
+    "pimc_accept_copy": (_i, [_p, _i, _i, _ip, _i]),
+    "pimc_reject_copy": (_i, [_p, _i, _i, _ip, _i]),
+    "pimc_setup_kvecs": (_i, [_p, _d, _ip]),
+    "pimc_get_kvecs": (_i, [_p, _dp]),
+    "pimc_set_longrange": (_i, [_p, _i, _dp, _dp, _dp, _dp, _dp, _dp, _dp, _dp, _i]),
+    "pimc_calc_rhok": (_i, [_p]),
+    "pimc_update_rhok": (_i, [_p, _i, _i, _ip, _i, _i]),
+    "pimc_get_rhok": (_i, [_p, _i, _dp]),
+    "pimc_bisection_setup": (_i, [_p, C.POINTER(BisectionDesc)]),
+    "pimc_rng_seed": (_i, [_p, C.c_uint64]),
+    "pimc_run_bisection": (_i, [_p, _i, _p, C.POINTER(BisectionStats)]),
+    "pimc_run_bisection_async": (_i, [_p, _i]),
+    "pimc_bisection_get_stats": (_i, [_p, C.POINTER(BisectionStats)]),
+    "pimc_synchronize": (_i, [_p]),
+    "pimc_stream": (_p, [_p]),
+}
+for _name, (_res, _args) in _SIGS.items():
+    _f = getattr(_lib, _name)
+    _f.restype = _res
+    _f.argtypes = _args
+
+EXPORTED = tuple(_SIGS)
+
+
+def lib():
+    return _lib
+
+
+def _dptr(a):
+    return a.ctypes.data_as(_dp)
+
+
+def _iptr(a):
+    return a.ctypes.data_as(_ip)
+
+
+def read_dm(path, desired_tau):
+    """Host-only: the DavidPA tables of a squarer .dm file as the library reads them.
+
+    Returns a dict with the grid, tau_pos and [num_tau][num_grid][num_cols]
+    arrays ukj, ukj_d2, dukj, dukj_d2 (column 0 = potential).
+    """
+    vals = [C.c_int() for _ in range(5)]
+    g0, g1 = C.c_double(), C.c_double()
+    rc = _lib.pimc_dm_read_info(path.encode(), desired_tau, *[C.byref(v) for v in vals], C.byref(g0), C.byref(g1))
+    if rc:
+        raise PimcError(rc, f"pimc_dm_read_info({path})")
+    ng, nc, nt, tp, gt = [v.value for v in vals]
+    arrs = [np.empty((nt, ng, nc)) for _ in range(4)]
+    rc = _lib.pimc_dm_read_tables(path.encode(), desired_tau, *[_dptr(a) for a in arrs])
+    if rc:
+        raise PimcError(rc, f"pimc_dm_read_tables({path})")
+    return dict(num_grid=ng, num_cols=nc, num_tau=nt, tau_pos=tp, grid_type=gt, grid_start=g0.value,
+                grid_end=g1.value, ukj=arrs[0], ukj_d2=arrs[1], dukj=arrs[2], dukj_d2=arrs[3])
+
+
+class PathData:
+    """Owns one pimc_context: path copies, pair action, device state.
+
+    The mirrored OLD/NEW path of PathClass (MirroredClass.h:23-200) lives on
+    the device; SetMode chooses which copy the Action objects evaluate, like
+    the reference's global ActiveCopy.
+    """
+
+    def __init__(self, num_particles, num_time_slices, box, tau, lam, num_images=0, device=0):
+        self.N = int(num_particles)
+        self.S = int(num_time_slices)
+        self.box = np.ascontiguousarray(box, dtype=np.float64)
+        self.tau = float(tau)
+        self.lam = float(lam)
+        self._species = np.zeros(self.N, dtype=np.int32)
+        self._lambda = np.array([lam], dtype=np.float64)
+        d = SystemDesc()
+        d.num_particles = self.N
+        d.num_time_slices = self.S
+        for i in range(3):
+            d.box[i] = self.box[i]
+        d.tau = self.tau
+        d.num_species = 1
+        d.species_of = _iptr(self._species)
+        d.lambda_ = _dptr(self._lambda)
+        d.num_images = int(num_images)
+        d.device = int(device)
+        h = _p()
+        rc = _lib.pimc_create(C.byref(d), C.byref(h))
+        if rc:
+            raise PimcError(rc, "pimc_create")
+        self.h = h
+        self.mode = OLDMODE
+        self._keep = []
+
+    def close(self):
+        if getattr(self, "h", None):
+            _lib.pimc_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+    def _check(self, rc, what):
+        if rc:
+            buf = C.create_string_buffer(512)
+            _lib.pimc_last_error(self.h, buf, 512)
+            raise PimcError(rc, f"{what}: {buf.value.decode(errors='replace')}")
+
+    # ---- MirroredClass ----
+    def SetMode(self, mode):
+        assert mode in (OLDMODE, NEWMODE)
+        self.mode = mode
+
+    def set_path(self, path, copy=BOTH):
+        path = np.ascontiguousarray(path, dtype=np.float64)
+        assert path.shape == (self.S, self.N, 3), path.shape
+        self._check(_lib.pimc_set_path(self.h, copy, _dptr(path)), "set_path")
+
+    def get_path(self, copy=OLDMODE):
+        out = np.empty((self.S, self.N, 3))
+        self._check(_lib.pimc_get_path(self.h, copy, _dptr(out)), "get_path")
+        return out
+
+    # ---- pair actions ----
+    def pa_david_from_dm(self, dm_path, num_offdiag_terms=0):
+        self._check(_lib.pimc_pa_david_from_dm(self.h, 0, 0, dm_path.encode(), num_offdiag_terms), "pa_david_from_dm")
+
+    def pa_david(self, grid_type, grid_start, grid_end, ukj, dukj, tau_pos, num_offdiag_terms=0):
+        ukj = np.ascontiguousarray(ukj, dtype=np.float64)
+        dukj = np.ascontiguousarray(dukj, dtype=np.float64)
+        nt, ng, nc = ukj.shape
+        self._check(_lib.pimc_pa_david(self.h, 0, 0, grid_type, grid_start, grid_end, ng, nc, nt, _dptr(ukj),
+                                       _dptr(dukj), tau_pos, num_offdiag_terms), "pa_david")
+
+    def pa_tricubic(self, qgrid, ygrid, tgrid, smallest_beta, umat, dumat, pot_grid, pot_data):
+        umat = np.ascontiguousarray(umat, dtype=np.float64)
+        dumat = np.ascontiguousarray(dumat, dtype=np.float64)
+        pot = np.ascontiguousarray(pot_data, dtype=np.float64)
+        g = [np.array(x, dtype=np.float64) for x in (qgrid, ygrid, tgrid)]
+        self._check(_lib.pimc_pa_tricubic(self.h, 0, 0, _dptr(g[0]), _dptr(g[1]), _dptr(g[2]), umat.shape[0],
+                                          smallest_beta, _dptr(umat), _dptr(dumat), pot_grid[0], pot_grid[1],
+                                          int(pot_grid[2]), _dptr(pot)), "pa_tricubic")
+
+    # ---- actions ----
+    def single_action(self, action, copy, slice1, slice2, active, level, precision=FP64):
+        a = np.ascontiguousarray(active, dtype=np.int32)
+        out = C.c_double()
+        self._check(_lib.pimc_single_action(self.h, action, copy, slice1, slice2, _iptr(a), len(a), level,
+                                            precision, C.byref(out)), "single_action")
+        return out.value
+
+    def d_dbeta(self, action, slice1, slice2, level=0):
+        out = C.c_double()
+        self._check(_lib.pimc_d_dbeta(self.h, action, slice1, slice2, level, C.byref(out)), "d_dbeta")
+        return out.value
+
+    def AcceptCopy(self, slice1, slice2, active):
+        a = np.ascontiguousarray(active, dtype=np.int32)
+        self._check(_lib.pimc_accept_copy(self.h, slice1, slice2, _iptr(a), len(a)), "accept_copy")
+
+    def RejectCopy(self, slice1, slice2, active):
+        a = np.ascontiguousarray(active, dtype=np.int32)
+        self._check(_lib.pimc_reject_copy(self.h, slice1, slice2, _iptr(a), len(a)), "reject_copy")
+
+    def synchronize(self):
+        self._check(_lib.pimc_synchronize(self.h), "synchronize")
+
+
+class ActionBaseClass:
+    """ActionBaseClass (PIMC++/src/Actions/ActionBase.h:31-75) over the device."""
+
+    kind = None
+
+    def __init__(self, path_data: PathData, precision=FP64):
+        self.PathData = path_data
+        self.precision = precision
+
+    def SingleAction(self, slice1, slice2, activeParticles, level):
+        return self.PathData.single_action(self.kind, self.PathData.mode, slice1, slice2, activeParticles, level,
+                                           self.precision)
+
+    def Action(self, slice1, slice2, activeParticles, level):
+        return self.SingleAction(slice1, slice2, activeParticles, level)
+
+    def d_dBeta(self, slice1, slice2, level):
+        return self.PathData.d_dbeta(self.kind, slice1, slice2, level)
+
+
+class ShortRangeClass(ActionBaseClass):
+    """ShortRangeClass (PIMC++/src/Actions/ShortRangeClass.cc:191-355)."""
+    kind = ACTION_SHORTRANGE
+
+    def GetName(self):
+        return "ShortRange"
+
+
+class KineticClass(ActionBaseClass):
+    """KineticClass (PIMC++/src/Actions/KineticClass.cc:33-256)."""
+    kind = ACTION_KINETIC
+
+    def GetName(self):
+        return "Kinetic"
+
+
+class BisectionBlock:
+    """BisectionBlockClass::MakeMove on the device (BisectionBlock.cc:380-451).
+
+    One call of `MakeMoves(n_blocks)` runs n_blocks blocks of StepsPerBlock
+    moves each; the Local RNG stream is Philox-4x32-10 keyed by `seed`.
+    """
+
+    def __init__(self, path_data: PathData, num_levels, steps_per_block=1, shortrange_at_higher_levels=True,
+                 precision=FP64, shadow=False, cluster_ctas=0, threads_per_cta=0):
+        self.PathData = path_data
+        d = BisectionDesc()
+        d.num_levels = num_levels
+        d.steps_per_block = steps_per_block
+        d.shortrange_at_higher_levels = int(shortrange_at_higher_levels)
+        d.use_longrange = 0
+        d.precision = precision
+        d.shadow = int(shadow)
+        d.cluster_ctas = cluster_ctas
+        d.threads_per_cta = threads_per_cta
+        self.desc = d
+        self.steps_per_block = steps_per_block
+        path_data._check(_lib.pimc_bisection_setup(path_data.h, C.byref(d)), "bisection_setup")
+
+    def seed(self, seed):
+        self.PathData._check(_lib.pimc_rng_seed(self.PathData.h, C.c_uint64(seed)), "rng_seed")
+
+    def MakeMoves(self, n_blocks, trace=True):
+        st = BisectionStats()
+        rec = np.zeros(n_blocks * self.steps_per_block, dtype=MOVE_RECORD) if trace else None
+        ptr = rec.ctypes.data_as(_p) if trace else None
+        self.PathData._check(_lib.pimc_run_bisection(self.PathData.h, n_blocks, ptr, C.byref(st)), "run_bisection")
+        return rec, st.as_dict()
+
+    def launch_async(self, n_blocks):
+        self.PathData._check(_lib.pimc_run_bisection_async(self.PathData.h, n_blocks), "run_bisection_async")
+
+    def stats(self):
+        st = BisectionStats()
+        self.PathData._check(_lib.pimc_bisection_get_stats(self.PathData.h, C.byref(st)), "get_stats")
+        return st.as_dict()

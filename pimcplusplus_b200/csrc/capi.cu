@@ -1,0 +1,619 @@
+// C ABI of the B200 PIMC action library (include/pimc_b200.h).  Host-side
+// argument checks mirror the reference's asserts, but report a status code
+// instead of aborting; no C++ exception crosses the ABI.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "action_kernels.cuh"
+#include "bisection.cuh"
+#include "pimc_internal.h"
+
+using namespace pimc;
+
+namespace {
+
+int fail(pimc_context *c, int code, const std::string &msg) {
+  if (c) c->last_error = msg;
+  return code;
+}
+
+int cuda_fail(pimc_context *c, cudaError_t e, const char *where) {
+  return fail(c, PIMC_E_CUDA, std::string(where) + ": " + cudaGetErrorString(e));
+}
+
+#define CK(call)                                        \
+  do {                                                  \
+    cudaError_t e_ = (call);                            \
+    if (e_ != cudaSuccess) return cuda_fail(ctx, e_, #call); \
+  } while (0)
+
+template <typename T>
+int upload(pimc_context *ctx, const T *host, size_t n, const T **dev, size_t pad_bytes = 16) {
+  void *p = nullptr;
+  cudaError_t e = cudaMalloc(&p, n * sizeof(T) + pad_bytes);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaMalloc(table)");
+  ctx->owned.push_back(p);
+  e = cudaMemset(p, 0, n * sizeof(T) + pad_bytes);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaMemset(table)");
+  e = cudaMemcpy(p, host, n * sizeof(T), cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaMemcpy(table)");
+  *dev = static_cast<const T *>(p);
+  return PIMC_OK;
+}
+
+template <typename R>
+int upload_grid(pimc_context *ctx, const HostGrid &h, DGrid<R> &g) {
+  g.type = h.type;
+  g.n = h.n;
+  g.start = (R)h.start;
+  g.end = (R)h.end;
+  g.delta = (R)h.delta;
+  g.deltainv = (R)h.deltainv;
+  g.r0 = (R)h.r0;
+  g.log_spacing = (R)h.log_spacing;
+  g.x = nullptr;
+  if (h.type == PIMC_GRID_LOG) {
+    std::vector<R> x(h.x.begin(), h.x.end());
+    return upload(ctx, x.data(), x.size(), &g.x);
+  }
+  return PIMC_OK;
+}
+
+template <typename R>
+int upload_david(pimc_context *ctx, const DavidTables &t, DDavid<R> &d) {
+  int rc = upload_grid(ctx, t.grid, d.grid);
+  if (rc) return rc;
+  d.ncols = t.ncols;
+  d.num_tau = t.num_tau;
+  d.tau_pos = t.tau_pos;
+  d.num_terms = t.num_terms;
+  const size_t n = t.uy.size();
+  std::vector<R> buf(n);
+  const std::vector<double> *srcs[4] = {&t.uy, &t.ud2, &t.duy, &t.dud2};
+  const R **dsts[4] = {&d.uy, &d.ud2, &d.duy, &d.dud2};
+  for (int k = 0; k < 4; k++) {
+    for (size_t i = 0; i < n; i++) buf[i] = (R)(*srcs[k])[i];
+    if ((rc = upload(ctx, buf.data(), n, dsts[k]))) return rc;
+  }
+  // diagonal column (col 1) as (y, d2y) pairs, levels padded to an even count
+  const int np = t.grid.n;
+  d.diag_stride = (np + 1) & ~1;
+  std::vector<R> diag((size_t)t.num_tau * d.diag_stride * 2, (R)0);
+  for (int lev = 0; lev < t.num_tau; lev++)
+    for (int i = 0; i < np; i++) {
+      size_t src = ((size_t)lev * np + i) * t.ncols + 1;
+      diag[((size_t)lev * d.diag_stride + i) * 2] = (R)t.uy[src];
+      diag[((size_t)lev * d.diag_stride + i) * 2 + 1] = (R)t.ud2[src];
+    }
+  return upload(ctx, diag.data(), diag.size(), &d.diag);
+}
+
+int check_pair(pimc_context *ctx, int sp1, int sp2) {
+  if (!ctx) return PIMC_E_ARG;
+  if (sp1 < 0 || sp2 < 0 || sp1 >= ctx->num_species || sp2 >= ctx->num_species)
+    return fail(ctx, PIMC_E_ARG, "species index out of range");
+  if (ctx->num_species != 1) return fail(ctx, PIMC_E_ARG, "one species per context is supported");
+  return PIMC_OK;
+}
+
+int set_david(pimc_context *ctx, DavidTables &t) {
+  int rc;
+  if ((rc = upload_david<double>(ctx, t, ctx->pa.d64))) return rc;
+  if ((rc = upload_david<float>(ctx, t, ctx->pa.d32))) return rc;
+  ctx->pa.kind = PA_DAVID;
+  return PIMC_OK;
+}
+
+int check_active(pimc_context *ctx, const int *active, int n, ActiveList &out) {
+  if (n < 0 || n > kMaxActive) return fail(ctx, PIMC_E_ARG, "n_active out of range");
+  if (n > 0 && !active) return fail(ctx, PIMC_E_ARG, "active is null");
+  out.n = n;
+  for (int i = 0; i < n; i++) {
+    if (active[i] < 0 || active[i] >= ctx->sys.N) return fail(ctx, PIMC_E_ARG, "active particle out of range");
+    out.p[i] = active[i];
+  }
+  return PIMC_OK;
+}
+
+int finish_scalar(pimc_context *ctx, double *out) {
+  CK(cudaMemcpyAsync(ctx->h_out, ctx->d_out, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  *out = *ctx->h_out;
+  if (!std::isfinite(*out)) return fail(ctx, PIMC_E_NAN, "non-finite action");
+  return PIMC_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char *pimc_status_string(int status) {
+  switch (status) {
+    case PIMC_OK: return "ok";
+    case PIMC_E_ARG: return "invalid argument";
+    case PIMC_E_CUDA: return "CUDA error";
+    case PIMC_E_NAN: return "non-finite action";
+    case PIMC_E_INDEX: return "index out of range";
+    case PIMC_E_CAP: return "device loop cap reached";
+    case PIMC_E_FILE: return "file missing or malformed";
+    case PIMC_E_STATE: return "call out of order";
+    case PIMC_E_NOMEM: return "allocation failed";
+    case PIMC_E_STAGING: return "broken staging (|S| > 1e50)";
+    default: return "unknown status";
+  }
+}
+
+int pimc_version(void) { return 100; }
+
+int pimc_create(const pimc_system_desc *d, pimc_context **out) {
+  if (!d || !out) return PIMC_E_ARG;
+  *out = nullptr;
+  if (d->num_particles < 2 || d->num_time_slices < 2 || d->num_species < 1 || !d->species_of || !d->lambda)
+    return PIMC_E_ARG;
+  for (int i = 0; i < 3; i++)
+    if (!(d->box[i] > 0.0)) return PIMC_E_ARG;
+  if (!(d->tau > 0.0) || d->num_images < 0) return PIMC_E_ARG;
+  pimc_context *ctx = new (std::nothrow) pimc_context();
+  if (!ctx) return PIMC_E_NOMEM;
+  ctx->device = d->device;
+  ctx->num_species = d->num_species;
+  ctx->species_of.assign(d->species_of, d->species_of + d->num_particles);
+  ctx->lambda.assign(d->lambda, d->lambda + d->num_species);
+  for (int s : ctx->species_of)
+    if (s < 0 || s >= d->num_species) {
+      delete ctx;
+      return PIMC_E_ARG;
+    }
+  DevSystem &s = ctx->sys;
+  s.N = d->num_particles;
+  s.S = d->num_time_slices;
+  for (int i = 0; i < 3; i++) {
+    s.box[i] = d->box[i];
+    s.boxinv[i] = 1.0 / d->box[i];
+  }
+  s.tau = d->tau;
+  s.lambda = d->lambda[0];
+  s.num_images = d->num_images;
+  cudaError_t e = cudaSetDevice(d->device);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking);
+  ctx->path_elems = (size_t)s.S * s.N * 3;
+  for (int c = 0; c < 2 && e == cudaSuccess; c++) e = cudaMalloc(&ctx->d_path[c], ctx->path_elems * sizeof(double));
+  if (e == cudaSuccess) e = cudaMalloc(&ctx->d_partials, kPartialSlots * sizeof(double));
+  if (e == cudaSuccess) e = cudaMalloc(&ctx->d_counter, sizeof(unsigned int));
+  if (e == cudaSuccess) e = cudaMemset(ctx->d_counter, 0, sizeof(unsigned int));
+  if (e == cudaSuccess) e = cudaMalloc(&ctx->d_out, 4 * sizeof(double));
+  if (e == cudaSuccess) e = cudaMallocHost(&ctx->h_out, 4 * sizeof(double));
+  if (e == cudaSuccess) e = cudaMalloc(&ctx->d_chain, sizeof(ChainState));
+  if (e == cudaSuccess) e = cudaMemset(ctx->d_chain, 0, sizeof(ChainState));
+  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&ctx->sm_count, cudaDevAttrMultiProcessorCount, d->device);
+  if (e == cudaSuccess) e = cudaMemset(ctx->d_path[0], 0, ctx->path_elems * sizeof(double));
+  if (e == cudaSuccess) e = cudaMemset(ctx->d_path[1], 0, ctx->path_elems * sizeof(double));
+  if (e != cudaSuccess) {
+    pimc_destroy(ctx);
+    return PIMC_E_CUDA;
+  }
+  *out = ctx;
+  return PIMC_OK;
+}
+
+int pimc_destroy(pimc_context *ctx) {
+  if (!ctx) return PIMC_E_ARG;
+  cudaSetDevice(ctx->device);
+  if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  for (void *p : ctx->owned) cudaFree(p);
+  for (int c = 0; c < 2; c++) cudaFree(ctx->d_path[c]);
+  cudaFree(ctx->d_partials);
+  cudaFree(ctx->d_counter);
+  cudaFree(ctx->d_out);
+  if (ctx->h_out) cudaFreeHost(ctx->h_out);
+  cudaFree(ctx->d_chain);
+  cudaFree(ctx->d_trace);
+  if (ctx->stream) cudaStreamDestroy(ctx->stream);
+  delete ctx;
+  return PIMC_OK;
+}
+
+int pimc_last_error(pimc_context *ctx, char *buf, int len) {
+  if (!ctx || !buf || len <= 0) return PIMC_E_ARG;
+  std::snprintf(buf, (size_t)len, "%s", ctx->last_error.c_str());
+  return PIMC_OK;
+}
+
+int pimc_pa_david_from_dm(pimc_context *ctx, int sp1, int sp2, const char *dm_path, int num_offdiag_terms) {
+  int rc = check_pair(ctx, sp1, sp2);
+  if (rc) return rc;
+  if (!dm_path) return fail(ctx, PIMC_E_ARG, "dm_path is null");
+  if (num_offdiag_terms < 0) return fail(ctx, PIMC_E_ARG, "negative NumOffDiagonalTerms");
+  CK(cudaSetDevice(ctx->device));
+  DavidTables t;
+  std::string err;
+  rc = read_dm_file(dm_path, ctx->sys.tau, num_offdiag_terms, t, err);
+  if (rc) return fail(ctx, rc, err);
+  if (t.ncols < 2 || (num_offdiag_terms > 0 && (num_offdiag_terms + 1) * (num_offdiag_terms + 2) / 2 > t.ncols - 1))
+    return fail(ctx, PIMC_E_FILE, "fit has too few ukj columns for NumOffDiagonalTerms");
+  return set_david(ctx, t);
+}
+
+int pimc_dm_read_info(const char *dm_path, double desired_tau, int *num_grid, int *num_cols, int *num_tau,
+                      int *tau_pos, int *grid_type, double *grid_start, double *grid_end) {
+  if (!dm_path) return PIMC_E_ARG;
+  DavidTables t;
+  std::string err;
+  int rc = read_dm_file(dm_path, desired_tau, 0, t, err);
+  if (rc) return rc;
+  if (num_grid) *num_grid = t.grid.n;
+  if (num_cols) *num_cols = t.ncols;
+  if (num_tau) *num_tau = t.num_tau;
+  if (tau_pos) *tau_pos = t.tau_pos;
+  if (grid_type) *grid_type = t.grid.type;
+  if (grid_start) *grid_start = t.grid.start;
+  if (grid_end) *grid_end = t.grid.end;
+  return PIMC_OK;
+}
+
+int pimc_dm_read_tables(const char *dm_path, double desired_tau, double *ukj, double *ukj_d2, double *dukj,
+                        double *dukj_d2) {
+  if (!dm_path) return PIMC_E_ARG;
+  DavidTables t;
+  std::string err;
+  int rc = read_dm_file(dm_path, desired_tau, 0, t, err);
+  if (rc) return rc;
+  const size_t bytes = t.uy.size() * sizeof(double);
+  if (ukj) std::memcpy(ukj, t.uy.data(), bytes);
+  if (ukj_d2) std::memcpy(ukj_d2, t.ud2.data(), bytes);
+  if (dukj) std::memcpy(dukj, t.duy.data(), bytes);
+  if (dukj_d2) std::memcpy(dukj_d2, t.dud2.data(), bytes);
+  return PIMC_OK;
+}
+
+int pimc_pa_david(pimc_context *ctx, int sp1, int sp2, int grid_type, double grid_start, double grid_end, int num_grid,
+                  int num_cols, int num_tau, const double *ukj, const double *dukj, int tau_pos,
+                  int num_offdiag_terms) {
+  int rc = check_pair(ctx, sp1, sp2);
+  if (rc) return rc;
+  if (!ukj || !dukj || num_grid < 2 || num_cols < 2 || num_tau < 1 || tau_pos < 0 || tau_pos >= num_tau ||
+      num_offdiag_terms < 0 || (num_offdiag_terms + 1) * (num_offdiag_terms + 2) / 2 > num_cols - 1)
+    return fail(ctx, PIMC_E_ARG, "bad DavidPA table arguments");
+  if (!(grid_end > grid_start) || (grid_type == PIMC_GRID_LOG && !(grid_start > 0.0)))
+    return fail(ctx, PIMC_E_ARG, "bad DavidPA grid");
+  CK(cudaSetDevice(ctx->device));
+  DavidTables t;
+  if (grid_type == PIMC_GRID_LINEAR)
+    t.grid.init_linear(grid_start, grid_end, num_grid);
+  else if (grid_type == PIMC_GRID_LOG)
+    t.grid.init_log(grid_start, std::pow(grid_end / grid_start, 1.0 / (num_grid - 1.0)), num_grid);
+  else
+    return fail(ctx, PIMC_E_ARG, "bad grid type");
+  t.ncols = num_cols;
+  t.num_tau = num_tau;
+  t.tau_pos = tau_pos;
+  t.num_terms = num_offdiag_terms;
+  build_david(t, ukj, dukj);
+  return set_david(ctx, t);
+}
+
+int pimc_pa_tricubic(pimc_context *ctx, int sp1, int sp2, const double qgrid[3], const double ygrid[3],
+                     const double tgrid[3], int num_betas, double smallest_beta, const double *umat,
+                     const double *dumat, double pot_start, double pot_end, int pot_n, const double *pot_data) {
+  int rc = check_pair(ctx, sp1, sp2);
+  if (rc) return rc;
+  if (!qgrid || !ygrid || !tgrid || !umat || !dumat || !pot_data || num_betas < 1 || pot_n < 3 ||
+      !(pot_end > pot_start) || !(smallest_beta > 0.0))
+    return fail(ctx, PIMC_E_ARG, "bad tricubic arguments");
+  const double *gs[3] = {qgrid, ygrid, tgrid};
+  HostGrid hg[3];
+  for (int i = 0; i < 3; i++) {
+    int n = (int)gs[i][2];
+    if (n < 3 || !(gs[i][1] > gs[i][0])) return fail(ctx, PIMC_E_ARG, "bad tricubic grid");
+    hg[i].init_linear(gs[i][0], gs[i][1], n);
+  }
+  CK(cudaSetDevice(ctx->device));
+  const size_t nodes = (size_t)hg[0].n * hg[1].n * hg[2].n;
+  std::vector<double> F(nodes * 8 * num_betas), dF(nodes * 8 * num_betas);
+  for (int b = 0; b < num_betas; b++) {
+    tricubic_fill(hg[0], hg[1], hg[2], umat + b * nodes, F.data() + b * nodes * 8);
+    tricubic_fill(hg[0], hg[1], hg[2], dumat + b * nodes, dF.data() + b * nodes * 8);
+  }
+  HostGrid pg;
+  pg.init_linear(pot_start, pot_end, pot_n);
+  std::vector<double> pd2(pot_n);
+  spline_second_derivs(pg, pot_data, 1, 0, 5.0e30, 5.0e30, pd2.data());
+  DTricubic<double> &t64 = ctx->pa.t64;
+  DTricubic<float> &t32 = ctx->pa.t32;
+  t64.nq = t32.nq = hg[0].n;
+  t64.ny = t32.ny = hg[1].n;
+  t64.nt = t32.nt = hg[2].n;
+  t64.num_betas = t32.num_betas = num_betas;
+  upload_grid(ctx, hg[0], t64.qg);
+  upload_grid(ctx, hg[1], t64.yg);
+  upload_grid(ctx, hg[2], t64.tg);
+  upload_grid(ctx, hg[0], t32.qg);
+  upload_grid(ctx, hg[1], t32.yg);
+  upload_grid(ctx, hg[2], t32.tg);
+  t64.qmax = hg[0].end;
+  t32.qmax = (float)hg[0].end;
+  t64.smallest_beta = smallest_beta;
+  t32.smallest_beta = (float)smallest_beta;
+  if ((rc = upload(ctx, F.data(), F.size(), &t64.U))) return rc;
+  if ((rc = upload(ctx, dF.data(), dF.size(), &t64.dU))) return rc;
+  {
+    std::vector<float> f32(F.begin(), F.end());
+    if ((rc = upload(ctx, f32.data(), f32.size(), &t32.U))) return rc;
+    std::vector<float> df32(dF.begin(), dF.end());
+    if ((rc = upload(ctx, df32.data(), df32.size(), &t32.dU))) return rc;
+  }
+  upload_grid(ctx, pg, t64.pot_grid);
+  upload_grid(ctx, pg, t32.pot_grid);
+  if ((rc = upload(ctx, pot_data, (size_t)pot_n, &t64.pot_y))) return rc;
+  if ((rc = upload(ctx, pd2.data(), pd2.size(), &t64.pot_d2))) return rc;
+  {
+    std::vector<float> y32(pot_data, pot_data + pot_n), d32(pd2.begin(), pd2.end());
+    if ((rc = upload(ctx, y32.data(), y32.size(), &t32.pot_y))) return rc;
+    if ((rc = upload(ctx, d32.data(), d32.size(), &t32.pot_d2))) return rc;
+  }
+  ctx->pa.kind = PA_TRICUBIC;
+  return PIMC_OK;
+}
+
+int pimc_set_path(pimc_context *ctx, int copy, const double *path) {
+  if (!ctx || !path || copy < 0 || copy > 2) return fail(ctx, PIMC_E_ARG, "bad set_path arguments");
+  CK(cudaSetDevice(ctx->device));
+  for (int c = 0; c < 2; c++)
+    if (copy == PIMC_BOTH || copy == c)
+      CK(cudaMemcpyAsync(ctx->d_path[c], path, ctx->path_elems * sizeof(double), cudaMemcpyHostToDevice,
+                         ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  return PIMC_OK;
+}
+
+int pimc_get_path(pimc_context *ctx, int copy, double *path) {
+  if (!ctx || !path || copy < 0 || copy > 1) return fail(ctx, PIMC_E_ARG, "bad get_path arguments");
+  CK(cudaSetDevice(ctx->device));
+  CK(cudaMemcpyAsync(path, ctx->d_path[copy], ctx->path_elems * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  return PIMC_OK;
+}
+
+static int check_slices(pimc_context *ctx, int slice1, int slice2, int level, bool inclusive) {
+  if (level < 0 || level >= kMaxLevels) return fail(ctx, PIMC_E_ARG, "level out of range");
+  if (slice1 < 0 || slice2 < slice1 || slice2 >= ctx->sys.S) return fail(ctx, PIMC_E_ARG, "slice range out of range");
+  (void)inclusive;
+  return PIMC_OK;
+}
+
+int pimc_single_action(pimc_context *ctx, int action, int copy, int slice1, int slice2, const int *active,
+                       int n_active, int level, int precision, double *out) {
+  if (!ctx || !out) return PIMC_E_ARG;
+  if (copy != PIMC_OLD && copy != PIMC_NEW) return fail(ctx, PIMC_E_ARG, "copy must be OLD or NEW");
+  if (precision != PIMC_FP64 && precision != PIMC_MIXED) return fail(ctx, PIMC_E_ARG, "bad precision");
+  int rc = check_slices(ctx, slice1, slice2, level, action == PIMC_ACTION_LONGRANGE);
+  if (rc) return rc;
+  ActiveList act;
+  if ((rc = check_active(ctx, active, n_active, act))) return rc;
+  CK(cudaSetDevice(ctx->device));
+  const int skip = 1 << level;
+  const int nlinks = (slice2 - slice1 + skip - 1) / skip;
+  ReduceTarget t{ctx->stream, ctx->d_partials, ctx->d_counter, ctx->d_out};
+  const double *path = ctx->d_path[copy];
+  if (nlinks == 0 || n_active == 0) {
+    *out = 0.0;
+    return PIMC_OK;
+  }
+  if (slice1 + nlinks * skip > ctx->sys.S - 1 + skip && action != PIMC_ACTION_LONGRANGE)
+    return fail(ctx, PIMC_E_ARG, "link runs past the last slice");
+  if ((slice1 + (nlinks - 1) * skip + skip) >= ctx->sys.S) return fail(ctx, PIMC_E_ARG, "link runs past the last slice");
+  switch (action) {
+    case PIMC_ACTION_SHORTRANGE:
+      if (ctx->pa.kind == PA_NONE) return fail(ctx, PIMC_E_STATE, "no pair action set");
+      if (ctx->pa.kind == PA_DAVID && level + ctx->pa.d64.tau_pos >= ctx->pa.d64.num_tau)
+        return fail(ctx, PIMC_E_ARG, "level beyond the pair action's tau levels");
+      if (ctx->pa.kind == PA_TRICUBIC && level >= ctx->pa.t64.num_betas)
+        return fail(ctx, PIMC_E_ARG, "level beyond the pair action's beta levels");
+      CK(launch_sr_single(t, path, ctx->sys, ctx->pa, act, slice1, skip, nlinks, level, precision, ctx->sm_count));
+      break;
+    case PIMC_ACTION_KINETIC:
+      CK(launch_kin_single(t, path, ctx->sys, act, slice1, skip, nlinks, level, ctx->sm_count));
+      break;
+    default:
+      return fail(ctx, PIMC_E_ARG, "unsupported action");
+  }
+  return finish_scalar(ctx, out);
+}
+
+int pimc_d_dbeta(pimc_context *ctx, int action, int slice1, int slice2, int level, double *out) {
+  if (!ctx || !out) return PIMC_E_ARG;
+  int rc = check_slices(ctx, slice1, slice2, level, false);
+  if (rc) return rc;
+  CK(cudaSetDevice(ctx->device));
+  const int skip = 1 << level;
+  const int nlinks = (slice2 - slice1 + skip - 1) / skip;
+  if (nlinks == 0) {
+    *out = 0.0;
+    return PIMC_OK;
+  }
+  if ((slice1 + (nlinks - 1) * skip + skip) >= ctx->sys.S) return fail(ctx, PIMC_E_ARG, "link runs past the last slice");
+  ReduceTarget t{ctx->stream, ctx->d_partials, ctx->d_counter, ctx->d_out};
+  const double *path = ctx->d_path[PIMC_OLD];
+  switch (action) {
+    case PIMC_ACTION_SHORTRANGE:
+      if (ctx->pa.kind == PA_NONE) return fail(ctx, PIMC_E_STATE, "no pair action set");
+      if (ctx->pa.kind == PA_DAVID && level + ctx->pa.d64.tau_pos >= ctx->pa.d64.num_tau)
+        return fail(ctx, PIMC_E_ARG, "level beyond the pair action's tau levels");
+      CK(launch_sr_dbeta(t, path, ctx->sys, ctx->pa, slice1, skip, nlinks, level, ctx->sm_count));
+      break;
+    case PIMC_ACTION_KINETIC:
+      CK(launch_kin_dbeta(t, path, ctx->sys, slice1, skip, nlinks, level, ctx->sm_count));
+      break;
+    default:
+      return fail(ctx, PIMC_E_ARG, "unsupported action");
+  }
+  return finish_scalar(ctx, out);
+}
+
+int pimc_accept_copy(pimc_context *ctx, int slice1, int slice2, const int *active, int n_active) {
+  if (!ctx) return PIMC_E_ARG;
+  int rc = check_slices(ctx, slice1, slice2, 0, true);
+  if (rc) return rc;
+  ActiveList act;
+  if ((rc = check_active(ctx, active, n_active, act))) return rc;
+  if (n_active == 0) return PIMC_OK;
+  CK(cudaSetDevice(ctx->device));
+  CK(launch_accept(ctx->stream, ctx->d_path[0], ctx->d_path[1], ctx->sys, act, slice1, slice2));
+  CK(cudaStreamSynchronize(ctx->stream));
+  return PIMC_OK;
+}
+
+int pimc_reject_copy(pimc_context *ctx, int slice1, int slice2, const int *active, int n_active) {
+  if (!ctx) return PIMC_E_ARG;
+  int rc = check_slices(ctx, slice1, slice2, 0, true);
+  if (rc) return rc;
+  ActiveList act;
+  if ((rc = check_active(ctx, active, n_active, act))) return rc;
+  if (n_active == 0) return PIMC_OK;
+  CK(cudaSetDevice(ctx->device));
+  CK(launch_reject(ctx->stream, ctx->d_path[0], ctx->d_path[1], ctx->sys, act, slice1, slice2));
+  CK(cudaStreamSynchronize(ctx->stream));
+  return PIMC_OK;
+}
+
+// ---- bisection ----
+int pimc_bisection_setup(pimc_context *ctx, const pimc_bisection_desc *d) {
+  if (!ctx || !d) return PIMC_E_ARG;
+  if (ctx->pa.kind == PA_NONE) return fail(ctx, PIMC_E_STATE, "no pair action set");
+  if (d->num_levels < 1 || d->num_levels > 6) return fail(ctx, PIMC_E_ARG, "NumLevels must be 1..6");
+  if ((1 << d->num_levels) >= ctx->sys.S) return fail(ctx, PIMC_E_ARG, "not enough slices for NumLevels");
+  if (d->steps_per_block < 1) return fail(ctx, PIMC_E_ARG, "StepsPerBlock must be >= 1");
+  if (d->precision != PIMC_FP64 && d->precision != PIMC_MIXED) return fail(ctx, PIMC_E_ARG, "bad precision");
+  if (d->cluster_ctas < 0 || d->cluster_ctas > kMaxCluster) return fail(ctx, PIMC_E_ARG, "cluster_ctas 0..16");
+  if (d->threads_per_cta != 0 && (d->threads_per_cta < 64 || d->threads_per_cta > 512 || d->threads_per_cta % 32))
+    return fail(ctx, PIMC_E_ARG, "threads_per_cta must be a multiple of 32 in 64..512");
+  if (d->use_longrange) return fail(ctx, PIMC_E_ARG, "long range inside device moves is not available");
+  if (ctx->pa.kind == PA_DAVID && d->num_levels + ctx->pa.d64.tau_pos > ctx->pa.d64.num_tau)
+    return fail(ctx, PIMC_E_ARG, "pair action has fewer tau levels than NumLevels");
+  if (ctx->pa.kind == PA_TRICUBIC && d->num_levels > ctx->pa.t64.num_betas)
+    return fail(ctx, PIMC_E_ARG, "pair action has fewer beta levels than NumLevels");
+  CK(cudaSetDevice(ctx->device));
+  ctx->bis = *d;
+  if (ctx->bis.cluster_ctas == 0) ctx->bis.cluster_ctas = ctx->sys.N >= 256 ? 8 : 1;
+  if (ctx->bis.threads_per_cta == 0) ctx->bis.threads_per_cta = 256;
+  ChainState cs;
+  CK(cudaMemcpy(&cs, ctx->d_chain, sizeof(cs), cudaMemcpyDeviceToHost));
+  cs.moves = cs.accepted = cs.stages = cs.pair_evals = cs.flips = 0;
+  cs.status = 0;
+  CK(cudaMemcpy(ctx->d_chain, &cs, sizeof(cs), cudaMemcpyHostToDevice));
+  ctx->bis_ready = true;
+  return PIMC_OK;
+}
+
+int pimc_rng_seed(pimc_context *ctx, uint64_t seed) {
+  if (!ctx) return PIMC_E_ARG;
+  CK(cudaSetDevice(ctx->device));
+  ChainState cs;
+  CK(cudaMemcpy(&cs, ctx->d_chain, sizeof(cs), cudaMemcpyDeviceToHost));
+  cs.seed = seed;
+  cs.nlocal = 0;
+  cs.one_left = 0;
+  cs.x2 = 0.0;
+  CK(cudaMemcpy(ctx->d_chain, &cs, sizeof(cs), cudaMemcpyHostToDevice));
+  return PIMC_OK;
+}
+
+static int run_bisection(pimc_context *ctx, int n_blocks, pimc_move_record *device_trace, long long offset) {
+  BisectionArgs a;
+  a.path = ctx->d_path[PIMC_OLD];
+  a.sys = ctx->sys;
+  a.pa = ctx->pa;
+  a.chain = ctx->d_chain;
+  a.trace = device_trace;
+  a.trace_offset = offset;
+  a.num_levels = ctx->bis.num_levels;
+  a.steps_per_block = ctx->bis.steps_per_block;
+  a.n_blocks = n_blocks;
+  a.sr_higher = ctx->bis.shortrange_at_higher_levels;
+  CK(launch_bisection(a, ctx->bis.precision, ctx->bis.shadow, ctx->bis.cluster_ctas, ctx->bis.threads_per_cta,
+                      ctx->stream));
+  return PIMC_OK;
+}
+
+int pimc_run_bisection_async(pimc_context *ctx, int n_blocks) {
+  if (!ctx || n_blocks < 0) return PIMC_E_ARG;
+  if (!ctx->bis_ready) return fail(ctx, PIMC_E_STATE, "pimc_bisection_setup not called");
+  CK(cudaSetDevice(ctx->device));
+  return run_bisection(ctx, n_blocks, nullptr, 0);
+}
+
+int pimc_run_bisection(pimc_context *ctx, int n_blocks, pimc_move_record *trace, pimc_bisection_stats *stats) {
+  if (!ctx || n_blocks < 0) return PIMC_E_ARG;
+  if (!ctx->bis_ready) return fail(ctx, PIMC_E_STATE, "pimc_bisection_setup not called");
+  CK(cudaSetDevice(ctx->device));
+  const size_t nrec = (size_t)n_blocks * ctx->bis.steps_per_block;
+  if (trace && nrec > ctx->trace_cap) {
+    cudaFree(ctx->d_trace);
+    ctx->d_trace = nullptr;
+    ctx->trace_cap = 0;
+    CK(cudaMalloc(&ctx->d_trace, nrec * sizeof(pimc_move_record)));
+    ctx->trace_cap = nrec;
+  }
+  int rc = run_bisection(ctx, n_blocks, trace ? ctx->d_trace : nullptr, 0);
+  if (rc) return rc;
+  // The device moves advance OLD only; bring NEW back in sync (MirroredClass invariant).
+  CK(cudaMemcpyAsync(ctx->d_path[1], ctx->d_path[0], ctx->path_elems * sizeof(double), cudaMemcpyDeviceToDevice,
+                     ctx->stream));
+  if (trace && nrec)
+    CK(cudaMemcpyAsync(trace, ctx->d_trace, nrec * sizeof(pimc_move_record), cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  pimc_bisection_stats st;
+  rc = pimc_bisection_get_stats(ctx, &st);
+  if (rc) return rc;
+  if (stats) *stats = st;
+  if (st.status) return fail(ctx, st.status, std::string("device status: ") + pimc_status_string(st.status));
+  return PIMC_OK;
+}
+
+int pimc_bisection_get_stats(pimc_context *ctx, pimc_bisection_stats *stats) {
+  if (!ctx || !stats) return PIMC_E_ARG;
+  CK(cudaSetDevice(ctx->device));
+  ChainState cs;
+  CK(cudaMemcpyAsync(&cs, ctx->d_chain, sizeof(cs), cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  stats->moves = (int64_t)cs.moves;
+  stats->accepted = (int64_t)cs.accepted;
+  stats->stages_attempted = (int64_t)cs.stages;
+  stats->pair_evals = (int64_t)cs.pair_evals;
+  stats->flips = (int64_t)cs.flips;
+  stats->status = cs.status;
+  stats->pad = 0;
+  return PIMC_OK;
+}
+
+int pimc_synchronize(pimc_context *ctx) {
+  if (!ctx) return PIMC_E_ARG;
+  CK(cudaSetDevice(ctx->device));
+  CK(cudaStreamSynchronize(ctx->stream));
+  return PIMC_OK;
+}
+
+void *pimc_stream(pimc_context *ctx) { return ctx ? (void *)ctx->stream : nullptr; }
+
+// Long-range entry points are declared in the header; until the rho_k
+// kernels are linked in they report PIMC_E_STATE.
+int pimc_setup_kvecs(pimc_context *ctx, double, int *) { return fail(ctx, PIMC_E_STATE, "long range not built"); }
+int pimc_get_kvecs(pimc_context *ctx, double *) { return fail(ctx, PIMC_E_STATE, "long range not built"); }
+int pimc_set_longrange(pimc_context *ctx, int, const double *, const double *, const double *, const double *,
+                       const double *, const double *, const double *, const double *, int) {
+  return fail(ctx, PIMC_E_STATE, "long range not built");
+}
+int pimc_calc_rhok(pimc_context *ctx) { return fail(ctx, PIMC_E_STATE, "long range not built"); }
+int pimc_update_rhok(pimc_context *ctx, int, int, const int *, int, int) {
+  return fail(ctx, PIMC_E_STATE, "long range not built");
+}
+int pimc_get_rhok(pimc_context *ctx, int, double *) { return fail(ctx, PIMC_E_STATE, "long range not built"); }
+
+}  // extern "C"

@@ -1,0 +1,463 @@
+// Device-side restatement of the PIMC++ pair-action arithmetic, templated on
+// the evaluation precision R (double for the plain path, float for the mixed
+// path).  Wherever the result feeds a discrete choice (grid interval, image
+// index) the arithmetic uses explicitly rounded intrinsics so no fused
+// multiply-add changes the choice relative to the source-order evaluation.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdint.h>
+
+#include "pimc_internal.h"
+
+namespace pimc {
+
+// ---- explicitly rounded arithmetic (no contraction) ----
+__device__ __forceinline__ double rmul(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ double radd(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ double rsub(double a, double b) { return __dsub_rn(a, b); }
+__device__ __forceinline__ float rmul(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ float radd(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ float rsub(float a, float b) { return __fsub_rn(a, b); }
+__device__ __forceinline__ double rint_r(double a) { return rint(a); }
+__device__ __forceinline__ float rint_r(float a) { return rintf(a); }
+__device__ __forceinline__ double log_r(double a) { return log(a); }
+__device__ __forceinline__ float log_r(float a) { return logf(a); }
+__device__ __forceinline__ double floor_r(double a) { return floor(a); }
+__device__ __forceinline__ float floor_r(float a) { return floorf(a); }
+__device__ __forceinline__ double sqrt_r(double a) { return sqrt(a); }
+__device__ __forceinline__ float sqrt_r(float a) { return sqrtf(a); }
+__device__ __forceinline__ double fabs_r(double a) { return fabs(a); }
+__device__ __forceinline__ float fabs_r(float a) { return fabsf(a); }
+
+// ---- Grid (Common/Splines/Grid.h:69-136 LinearGrid, :519-575 LogGrid) ----
+// LinearGrid::ReverseMap = (int)nearbyint((r-Start)*deltainv - 0.5);
+// LogGrid::ReverseMap = (int)floor(log(r/r0)/log(Spacing)).
+template <typename R>
+__device__ __forceinline__ int reverse_map(const DGrid<R> &g, R r) {
+  if (g.type == PIMC_GRID_LINEAR) return (int)rint_r(rsub(rmul(rsub(r, g.start), g.deltainv), R(0.5)));
+  return (int)floor_r(log_r(r / g.r0) / g.log_spacing);
+}
+// Grid node i: LinearGrid stores Start + (double)i*delta (Grid.h:93-95).
+template <typename R>
+__device__ __forceinline__ R grid_x(const DGrid<R> &g, int i) {
+  if (g.type == PIMC_GRID_LINEAR) return radd(g.start, rmul((R)i, g.delta));
+  return g.x[i];
+}
+
+// Interval of a cubic spline evaluation with the clamps of
+// MultiCubicSpline::operator() (CubicSpline.h:485-501).
+template <typename R>
+struct SplineCell {
+  int low, hi;
+  R a, b, a3, b3, h26;
+};
+template <typename R>
+__device__ __forceinline__ SplineCell<R> spline_cell(const DGrid<R> &g, R x) {
+  SplineCell<R> c;
+  int hi = reverse_map(g, x) + 1;
+  int low = hi - 1;
+  if (low < 0) { low = 0; hi = 1; }
+  if (hi > (g.n - 1)) { hi = g.n - 1; low = hi - 1; }
+  R xl = grid_x(g, low), xh = grid_x(g, hi);
+  R h = xh - xl;
+  R hinv = R(1.0) / h;
+  c.a = (xh - x) * hinv;
+  c.b = (x - xl) * hinv;
+  c.a3 = c.a * c.a * c.a - c.a;
+  c.b3 = c.b * c.b * c.b - c.b;
+  c.h26 = h * h * R(0.1666666666666666666);
+  c.low = low;
+  c.hi = hi;
+  return c;
+}
+template <typename R>
+__device__ __forceinline__ R spline_apply(const SplineCell<R> &c, R yl, R yh, R dl, R dh) {
+  return c.a * yl + c.b * yh + (c.a3 * dl + c.b3 * dh) * c.h26;
+}
+// Column `col` of a [point][ncols] table pair.
+template <typename R>
+__device__ __forceinline__ R spline_col(const DGrid<R> &g, const R *__restrict__ y, const R *__restrict__ d2,
+                                        int ncols, int col, R x) {
+  SplineCell<R> c = spline_cell(g, x);
+  return spline_apply(c, __ldg(&y[c.low * ncols + col]), __ldg(&y[c.hi * ncols + col]),
+                      __ldg(&d2[c.low * ncols + col]), __ldg(&d2[c.hi * ncols + col]));
+}
+
+template <typename R>
+struct Pair2;
+template <>
+struct Pair2<double> { typedef double2 T; };
+template <>
+struct Pair2<float> { typedef float2 T; };
+
+// Column stored as interleaved (y, d2y) pairs, e.g. staged in shared memory.
+template <typename R>
+__device__ __forceinline__ R spline_pairs(const DGrid<R> &g, const typename Pair2<R>::T *tab, R x) {
+  SplineCell<R> c = spline_cell(g, x);
+  typename Pair2<R>::T lo = tab[c.low], hi = tab[c.hi];
+  return spline_apply(c, lo.x, hi.x, lo.y, hi.y);
+}
+
+// ---- DavidPAClass::calcUsqzFast (DavidPAClass.cc:468-511) ----
+// diag: column 1 of ukj(level+TauPos) as (y, d2y) pairs (global or shared).
+template <typename R>
+__device__ __forceinline__ R david_U(const DDavid<R> &d, const typename Pair2<R>::T *diag, R s, R q, R z,
+                                     int level) {
+  level = level + d.tau_pos;
+  const DGrid<R> &g = d.grid;
+  R rmin = g.start;
+  R r = q + R(0.5) * z;
+  R rprime = q - R(0.5) * z;
+  if (r > g.end) r = g.end;
+  if (rprime > g.end) rprime = g.end;
+  if ((rprime < rmin) || (r < rmin)) return spline_pairs(g, diag, rmin);
+  R U = R(0.5) * (spline_pairs(g, diag, r) + spline_pairs(g, diag, rprime));
+  if (d.num_terms > 0 && s > R(0) && q < g.end) {
+    const R *y = d.uy + (size_t)level * g.n * d.ncols;
+    const R *d2 = d.ud2 + (size_t)level * g.n * d.ncols;
+    SplineCell<R> c = spline_cell(g, q);
+    R zsquared = z * z;
+    R ssquared = s * s;
+    R ssquaredinverse = R(1.0) / ssquared;
+    R Sto2k = ssquared;
+    for (int k = 1; k <= d.num_terms; k++) {
+      R Zto2j = 1;
+      R currS = Sto2k;
+      for (int j = 0; j <= k; j++) {
+        int col = k * (k + 1) / 2 + j + 1;
+        R Ucof = spline_apply(c, __ldg(&y[c.low * d.ncols + col]), __ldg(&y[c.hi * d.ncols + col]),
+                              __ldg(&d2[c.low * d.ncols + col]), __ldg(&d2[c.hi * d.ncols + col]));
+        U += Ucof * Zto2j * currS;
+        Zto2j *= zsquared;
+        currS = currS * ssquaredinverse;
+      }
+      Sto2k = Sto2k * ssquared;
+    }
+  }
+  return U;
+}
+
+// ---- DavidPAClass::calcUsqz, dU output (DavidPAClass.cc:291-463) ----
+template <typename R>
+__device__ __forceinline__ R david_dU(const DDavid<R> &d, R s, R q, R z, int level) {
+  level = level + d.tau_pos;
+  const DGrid<R> &g = d.grid;
+  const R *uy = d.uy + (size_t)level * g.n * d.ncols;
+  const R *ud2 = d.ud2 + (size_t)level * g.n * d.ncols;
+  const R *dy = d.duy + (size_t)level * g.n * d.ncols;
+  const R *dd2 = d.dud2 + (size_t)level * g.n * d.ncols;
+  R rmin = g.start;
+  R r = q + R(0.5) * z;
+  R rprime = q - R(0.5) * z;
+  if (r > g.end) r = g.end;
+  if (rprime > g.end) rprime = g.end;
+  if (rprime < rmin) rprime = rmin;
+  if (r < rmin) r = rmin;
+  R V = R(0.5) * (spline_col(g, uy, ud2, d.ncols, 0, r) + spline_col(g, uy, ud2, d.ncols, 0, rprime));
+  R dU = R(0.5) * (spline_col(g, dy, dd2, d.ncols, 1, r) + spline_col(g, dy, dd2, d.ncols, 1, rprime));
+  dU += V;
+  if (d.num_terms > 0 && s > R(0) && q < g.end) {
+    SplineCell<R> c = spline_cell(g, q);
+    R zsquared = z * z;
+    R ssquared = s * s;
+    R ssquaredinverse = R(1.0) / ssquared;
+    R Sto2k = ssquared;
+    for (int k = 1; k <= d.num_terms; k++) {
+      R Zto2j = 1;
+      R currS = Sto2k;
+      for (int j = 0; j <= k; j++) {
+        int col = k * (k + 1) / 2 + j + 1;
+        R dUcof = spline_apply(c, __ldg(&dy[c.low * d.ncols + col]), __ldg(&dy[c.hi * d.ncols + col]),
+                               __ldg(&dd2[c.low * d.ncols + col]), __ldg(&dd2[c.hi * d.ncols + col]));
+        dU += dUcof * Zto2j * currS;
+        Zto2j *= zsquared;
+        currS = currS * ssquaredinverse;
+      }
+      Sto2k = Sto2k * ssquared;
+    }
+  }
+  return dU;
+}
+
+// ---- MyTricubicSpline::operator() (MyTricubicSpline.h:197-334) ----
+// Hermite basis p1, p2, q1, q2 (MyTricubicSpline.h:38-45).
+template <typename R>
+__device__ __forceinline__ void hermite4(R t, R h, R out[4]) {
+  R tm1 = t - R(1.0);
+  out[0] = tm1 * tm1 * (R(1.0) + R(2.0) * t);
+  out[1] = t * t * (R(3.0) - R(2.0) * t);
+  out[2] = h * (t * tm1 * tm1);
+  out[3] = h * (t * t * tm1);
+}
+
+template <typename R>
+struct Node8;
+template <>
+struct Node8<double> {
+  double v[8];
+  __device__ __forceinline__ void load(const double *p) {
+    const double2 *q = reinterpret_cast<const double2 *>(p);
+    double2 a = __ldg(q), b = __ldg(q + 1), c = __ldg(q + 2), d = __ldg(q + 3);
+    v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y; v[4] = c.x; v[5] = c.y; v[6] = d.x; v[7] = d.y;
+  }
+};
+template <>
+struct Node8<float> {
+  float v[8];
+  __device__ __forceinline__ void load(const float *p) {
+    const float4 *q = reinterpret_cast<const float4 *>(p);
+    float4 a = __ldg(q), b = __ldg(q + 1);
+    v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w; v[4] = b.x; v[5] = b.y; v[6] = b.z; v[7] = b.w;
+  }
+};
+
+// F: [nx][ny][nz][8] with components F, Fx, Fy, Fz, Fxy, Fxz, Fyz, Fxyz.
+template <typename R>
+__device__ __forceinline__ R tricubic_eval(const R *__restrict__ F, const DGrid<R> &gx, const DGrid<R> &gy,
+                                           const DGrid<R> &gz, R x, R y, R z) {
+  int ix = reverse_map(gx, x), iy = reverse_map(gy, y), iz = reverse_map(gz, z);
+  ix = max(0, ix); ix = min(ix, gx.n - 2);
+  iy = max(0, iy); iy = min(iy, gy.n - 2);
+  iz = max(0, iz); iz = min(iz, gz.n - 2);
+  R x0 = grid_x(gx, ix), y0 = grid_x(gy, iy), z0 = grid_x(gz, iz);
+  R h = grid_x(gx, ix + 1) - x0;
+  R k = grid_x(gy, iy + 1) - y0;
+  R l = grid_x(gz, iz + 1) - z0;
+  R a[4], b[4], c[4];
+  hermite4((x - x0) / h, h, a);
+  hermite4((y - y0) / k, k, b);
+  hermite4((z - z0) / l, l, c);
+  const size_t sy = (size_t)gz.n * 8, sx = (size_t)gy.n * sy;
+  const R *base = F + (size_t)ix * sx + (size_t)iy * sy + (size_t)iz * 8;
+  R val = R(0);
+#pragma unroll
+  for (int dx = 0; dx < 2; dx++) {
+#pragma unroll
+    for (int dy = 0; dy < 2; dy++) {
+      const R *p = base + dx * sx + dy * sy;
+      Node8<R> n0, n1;
+      n0.load(p);
+      n1.load(p + 8);
+      R A0 = a[dx], A1 = a[2 + dx], B0 = b[dy], B1 = b[2 + dy];
+      R C00 = c[0], C01 = c[2], C10 = c[1], C11 = c[3];  // (z-node, z-derivative)
+      // node (dz=0): C0 = c[0] value, c[2] derivative; node (dz=1): c[1], c[3]
+      R s00 = n0.v[0] * C00 + n0.v[3] * C01 + n1.v[0] * C10 + n1.v[3] * C11;  // F, Fz
+      R s01 = n0.v[2] * C00 + n0.v[6] * C01 + n1.v[2] * C10 + n1.v[6] * C11;  // Fy, Fyz
+      R s10 = n0.v[1] * C00 + n0.v[5] * C01 + n1.v[1] * C10 + n1.v[5] * C11;  // Fx, Fxz
+      R s11 = n0.v[4] * C00 + n0.v[7] * C01 + n1.v[4] * C10 + n1.v[7] * C11;  // Fxy, Fxyz
+      val += A0 * (B0 * s00 + B1 * s01) + A1 * (B0 * s10 + B1 * s11);
+    }
+  }
+  return val;
+}
+
+// SplinePot::V (Common/PH/SplinePot.cc:19-31) with no Vouter.
+template <typename R>
+__device__ __forceinline__ R pot_V(const DTricubic<R> &t, R r) {
+  if (r <= t.pot_grid.end) return spline_col(t.pot_grid, t.pot_y, t.pot_d2, 1, 0, r);
+  return R(0);
+}
+
+// ---- PAtricubicFitClass::U / dU (PAtricubicFit.cc:659-721) ----
+template <typename R, bool DERIV>
+__device__ __forceinline__ R tricubic_pa(const DTricubic<R> &t, R q, R z, R s2, int level) {
+  const DGrid<R> &qg = t.qg, &yg = t.yg, &tg = t.tg;
+  z = fabs_r(z);
+  R smax = R(2.0) * q;
+  R zmax = smax;
+  R s = sqrt_r(s2);
+  const R *F = (DERIV ? t.dU : t.U) + (size_t)level * t.nq * t.ny * t.nt * 8;
+  if ((q <= t.qmax) && (z < zmax) && (s < smax)) {
+    if (q == R(0)) return tricubic_eval(F, qg, yg, tg, R(0), R(0), R(0));
+    R y = z / zmax;
+    R tt = (s - z) / (smax - z);
+    return tricubic_eval(F, qg, yg, tg, q, y, tt);
+  }
+  R r = q + R(0.5) * z;
+  R rp = q - R(0.5) * z;
+  if (DERIV) return R(0.5) * (pot_V(t, r) + pot_V(t, rp));
+  R beta = t.smallest_beta;
+  for (int i = 0; i < level; i++) beta *= R(2.0);
+  return R(0.5) * beta * (pot_V(t, r) + pot_V(t, rp));
+}
+
+// ---- PathClass::DistDisp two-slice form (PathClass.h:696-746) ----
+// Positions of ptcl1 and ptcl2 at slices A and B; returns dispA = r2-r1 at A
+// wrapped to the minimum image and dispB at B taking the image consistent
+// with dispA.  Always FP64 (the path is FP64).
+__device__ __forceinline__ void dist_disp(const double a1[3], const double a2[3], const double b1[3],
+                                          const double b2[3], const DevSystem &s, double dA[3], double dB[3]) {
+#pragma unroll
+  for (int i = 0; i < 3; i++) {
+    double da = a2[i] - a1[i];
+    double db = b2[i] - b1[i];
+    double n = -rint(rmul(da, s.boxinv[i]));
+    da = radd(da, rmul(n, s.box[i]));
+    double m = rint(rmul(rsub(da, db), s.boxinv[i]));
+    db = radd(db, rmul(m, s.box[i]));
+    dA[i] = da;
+    dB[i] = db;
+  }
+}
+
+// PathClass::PutInBox (PathClass.h:897-921)
+__device__ __forceinline__ void put_in_box(double v[3], const DevSystem &s) {
+#pragma unroll
+  for (int i = 0; i < 3; i++) {
+    double n = -floor(radd(rmul(v[i], s.boxinv[i]), 0.5));
+    v[i] = radd(v[i], rmul(n, s.box[i]));
+  }
+}
+// PathClass::PutInBoxFast (PathClass.cc:1389-1407)
+__device__ __forceinline__ void put_in_box_fast(double v[3], const DevSystem &s) {
+#pragma unroll
+  for (int dim = 0; dim < 3; dim++) {
+    double halfBox = s.box[dim] / 2;
+    if (v[dim] > halfBox) v[dim] -= s.box[dim];
+    if (v[dim] < -halfBox) v[dim] += s.box[dim];
+  }
+}
+
+// Pair geometry of one link: q, z, s^2 as ShortRangeClass::SingleAction
+// forms them (ShortRangeClass.cc:217-220).
+template <typename R>
+struct LinkGeom {
+  R q, z, s2, s, rmag, rpmag;
+};
+template <typename R>
+__device__ __forceinline__ LinkGeom<R> link_geom(const double dA[3], const double dB[3]) {
+  LinkGeom<R> g;
+  R ax = (R)dA[0], ay = (R)dA[1], az = (R)dA[2];
+  R bx = (R)dB[0], by = (R)dB[1], bz = (R)dB[2];
+  R rmag = sqrt_r(ax * ax + ay * ay + az * az);
+  R rpmag = sqrt_r(bx * bx + by * by + bz * bz);
+  R d0 = ax - bx, d1 = ay - by, d2 = az - bz;
+  g.s2 = d0 * d0 + d1 * d1 + d2 * d2;
+  g.q = R(0.5) * (rmag + rpmag);
+  g.z = (rmag - rpmag);
+  g.s = sqrt_r(g.s2);
+  g.rmag = rmag;
+  g.rpmag = rpmag;
+  return g;
+}
+
+// U(q, z, s^2, level) of the pair action (ActionBaseClass's PA.U).
+template <typename R, int KIND>
+__device__ __forceinline__ R pa_U(const DevPA &pa, const typename Pair2<R>::T *diag, const LinkGeom<R> &g,
+                                  int level);
+template <>
+__device__ __forceinline__ double pa_U<double, PA_DAVID>(const DevPA &pa, const double2 *diag,
+                                                         const LinkGeom<double> &g, int level) {
+  return david_U<double>(pa.d64, diag, g.s, g.q, g.z, level);
+}
+template <>
+__device__ __forceinline__ float pa_U<float, PA_DAVID>(const DevPA &pa, const float2 *diag,
+                                                       const LinkGeom<float> &g, int level) {
+  return david_U<float>(pa.d32, diag, g.s, g.q, g.z, level);
+}
+template <>
+__device__ __forceinline__ double pa_U<double, PA_TRICUBIC>(const DevPA &pa, const double2 *,
+                                                            const LinkGeom<double> &g, int level) {
+  const DTricubic<double> &t = pa.t64;
+  return tricubic_pa<double, false>(t, g.q, g.z, g.s2, level);
+}
+template <>
+__device__ __forceinline__ float pa_U<float, PA_TRICUBIC>(const DevPA &pa, const float2 *,
+                                                          const LinkGeom<float> &g, int level) {
+  const DTricubic<float> &t = pa.t32;
+  return tricubic_pa<float, false>(t, g.q, g.z, g.s2, level);
+}
+
+template <typename R>
+__device__ __forceinline__ const DDavid<R> &david_of(const DevPA &pa);
+template <>
+__device__ __forceinline__ const DDavid<double> &david_of<double>(const DevPA &pa) { return pa.d64; }
+template <>
+__device__ __forceinline__ const DDavid<float> &david_of<float>(const DevPA &pa) { return pa.d32; }
+
+// dU (energy estimator), FP64 only.
+template <int KIND>
+__device__ __forceinline__ double pa_dU(const DevPA &pa, const LinkGeom<double> &g, int level);
+template <>
+__device__ __forceinline__ double pa_dU<PA_DAVID>(const DevPA &pa, const LinkGeom<double> &g, int level) {
+  return david_dU<double>(pa.d64, g.s, g.q, g.z, level);
+}
+template <>
+__device__ __forceinline__ double pa_dU<PA_TRICUBIC>(const DevPA &pa, const LinkGeom<double> &g, int level) {
+  const DTricubic<double> &t = pa.t64;
+  return tricubic_pa<double, true>(t, g.q, g.z, g.s2, level);
+}
+
+// ---- KineticClass::SingleAction link term (KineticClass.cc:45-78) ----
+// vel = Velocity(slice, slice+skip): the PutInBox'ed link vector.
+__device__ __forceinline__ double kinetic_link(const double vel[3], double four_lambda_tau_inv, int num_images,
+                                               const DevSystem &s) {
+  double GaussProd = 1.0;
+  for (int dim = 0; dim < 3; dim++) {
+    double GaussSum = 0.0;
+    for (int image = -num_images; image <= num_images; image++) {
+      double dist = vel[dim] + (double)image * s.box[dim];
+      GaussSum += exp(-dist * dist * four_lambda_tau_inv);
+    }
+    GaussProd *= GaussSum;
+  }
+  return -log(GaussProd);
+}
+
+// ---- Philox-4x32-10 (Salmon et al., SC'11): the Local/Common/World streams ----
+__device__ __forceinline__ void philox4x32_10(uint32_t c[4], uint32_t k0, uint32_t k1) {
+  const uint32_t M0 = 0xD2511F53u, M1 = 0xCD9E8D57u;
+  const uint32_t W0 = 0x9E3779B9u, W1 = 0xBB67AE85u;
+#pragma unroll
+  for (int r = 0; r < 10; ++r) {
+    uint32_t hi0 = __umulhi(M0, c[0]), lo0 = M0 * c[0];
+    uint32_t hi1 = __umulhi(M1, c[2]), lo1 = M1 * c[2];
+    uint32_t n0 = hi1 ^ c[1] ^ k0;
+    uint32_t n2 = hi0 ^ c[3] ^ k1;
+    c[0] = n0; c[1] = lo1; c[2] = n2; c[3] = lo0;
+    k0 += W0; k1 += W1;
+  }
+}
+// Element `index` of stream `stream`: two 53-bit doubles per Philox block.
+__device__ __forceinline__ double philox_uniform(uint64_t seed, uint32_t stream, uint64_t index) {
+  uint64_t block = index >> 1;
+  uint32_t c[4] = {(uint32_t)block, (uint32_t)(block >> 32), stream, 0x50494D43u};
+  philox4x32_10(c, (uint32_t)seed, (uint32_t)(seed >> 32));
+  int h = (int)(index & 1);
+  uint32_t a = (h ? c[2] : c[0]) >> 5, b = (h ? c[3] : c[1]) >> 6;
+  return ((double)a * 67108864.0 + (double)b) * (1.0 / 9007199254740992.0);
+}
+
+// RandomClass on one thread: Local(), LocalInt(), LocalGaussian() with the
+// polar-method pair cache (Common/Random/Random.h:33-49,156-180).
+struct DevRandom {
+  uint64_t seed, n;
+  int one_left;
+  double x2;
+  __device__ __forceinline__ double Local() { return philox_uniform(seed, 0u, n++); }
+  __device__ __forceinline__ int LocalInt(int max) { return (int)floor(Local() * max); }
+  __device__ __forceinline__ double LocalGaussian(double sigma) {
+    double X1;
+    if (one_left) {
+      X1 = x2;
+      one_left = 0;
+    } else {
+      double V1, V2, S;
+      int guard = 0;
+      do {
+        V1 = 2.0 * Local() - 1.0;
+        V2 = 2.0 * Local() - 1.0;
+        S = V1 * V1 + V2 * V2;
+      } while (S >= 1.0 && ++guard < 1000000);
+      double temp = sqrt((-2.0 * log(S)) / S);
+      X1 = V1 * temp;
+      x2 = V2 * temp;
+      one_left = 1;
+    }
+    return X1 * sigma;
+  }
+};
+
+}  // namespace pimc

@@ -1,0 +1,146 @@
+// Internal types of the B200 PIMC action library: host-side tables, the
+// device descriptors handed to kernels by value, and the context.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+#include <vector>
+
+#include "../../include/pimc_b200.h"
+
+namespace pimc {
+
+constexpr int kMaxLevels = 8;        // bisection levels a move may use (2^8 slices)
+constexpr int kMaxWindow = (1 << 6) + 1;  // slices of a move window held in shared memory (NumLevels <= 6)
+constexpr int kMaxCluster = 16;
+constexpr int kMaxActive = 64;       // active particles of one SingleAction call
+constexpr int kPartialSlots = 8192;  // per-block partial sums of the reduction kernels
+
+// ---------------------------------------------------------------------------
+// Host tables (FP64, built once on the host like the reference's setup).
+// ---------------------------------------------------------------------------
+struct HostGrid {
+  int type = PIMC_GRID_LINEAR;
+  int n = 0;
+  double start = 0, end = 0, delta = 0, deltainv = 0, r0 = 0, spacing = 1, log_spacing = 0;
+  std::vector<double> x;
+  void init_linear(double s, double e, int num);
+  void init_log(double r0_, double spacing_, int num);
+};
+
+// Natural/clamped cubic-spline second derivatives over columns (Numerical
+// Recipes tridiagonal solve).  y, d2y row-major [point][column].
+void spline_second_derivs(const HostGrid &g, const double *y, int ncols, int col, double start_deriv,
+                          double end_deriv, double *d2y);
+// First-derivative tricubic coefficient fill of 8 components per node.
+void tricubic_fill(const HostGrid &gx, const HostGrid &gy, const HostGrid &gz, const double *values,
+                   double *F);
+
+struct DavidTables {
+  HostGrid grid;
+  int ncols = 0, num_tau = 0, tau_pos = 0, num_terms = 0;
+  std::vector<double> uy, ud2, duy, dud2;  // [tau][point][col]
+};
+int read_dm_file(const char *path, double desired_tau, int num_terms, DavidTables &out, std::string &err);
+void build_david(DavidTables &t, const double *ukj, const double *dukj);
+
+// ---------------------------------------------------------------------------
+// Device descriptors (passed to kernels by value).
+// ---------------------------------------------------------------------------
+template <typename R>
+struct DGrid {
+  int type, n;
+  R start, end, delta, deltainv, r0, log_spacing;
+  const R *x;  // node coordinates [n]
+};
+
+// DavidPAClass tables for one species pair, one precision.
+template <typename R>
+struct DDavid {
+  DGrid<R> grid;
+  int ncols, num_tau, tau_pos, num_terms;
+  const R *uy, *ud2;    // ukj  [tau][point][col]
+  const R *duy, *dud2;  // dukj [tau][point][col]
+  const R *diag;        // column 1 of ukj as (y, d2y) pairs [tau][diag_stride][2]
+  int diag_stride;      // points per level of diag, rounded up to an even count
+};
+
+// PAtricubicFitClass tables for one species pair, one precision.
+template <typename R>
+struct DTricubic {
+  int nq, ny, nt, num_betas;
+  DGrid<R> qg, yg, tg;       // linear q, y, t grids
+  R qmax;                    // qgrid End
+  R smallest_beta;
+  const R *U;   // [beta][nq][ny][nt][8]
+  const R *dU;  // same
+  DGrid<R> pot_grid;
+  const R *pot_y, *pot_d2;  // SplinePot natural cubic spline
+};
+
+enum PAKind : int { PA_NONE = 0, PA_DAVID = 1, PA_TRICUBIC = 2 };
+
+struct DevPA {
+  int kind;
+  DDavid<double> d64;
+  DDavid<float> d32;
+  DTricubic<double> t64;
+  DTricubic<float> t32;
+};
+
+struct DevSystem {
+  int N, S;  // particles, path rows
+  double box[3], boxinv[3];
+  double tau, lambda;
+  int num_images;
+};
+
+// Per-chain device state of the bisection driver.
+struct ChainState {
+  uint64_t seed;
+  uint64_t nlocal;     // position in the Local stream
+  int32_t one_left;    // LocalGaussian cache flag (Random.h:159-160)
+  int32_t status;
+  double x2;           // cached second Gaussian
+  unsigned long long moves, accepted, stages, pair_evals, flips;
+};
+
+struct DeviceBuffer {
+  void *p = nullptr;
+  size_t bytes = 0;
+};
+
+}  // namespace pimc
+
+struct pimc_context {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  pimc::DevSystem sys{};
+  std::vector<int> species_of;
+  std::vector<double> lambda;
+  int num_species = 1;
+  double *d_path[2] = {nullptr, nullptr};
+  size_t path_elems = 0;
+  // pair action (single species pair)
+  pimc::DevPA pa{};
+  std::vector<void *> owned;  // device allocations of the tables
+  // reduction scratch
+  double *d_partials = nullptr;
+  unsigned int *d_counter = nullptr;
+  double *d_out = nullptr;
+  double *h_out = nullptr;  // pinned
+  int *d_active = nullptr;
+  // bisection
+  pimc_bisection_desc bis{};
+  bool bis_ready = false;
+  pimc::ChainState *d_chain = nullptr;
+  pimc_move_record *d_trace = nullptr;
+  size_t trace_cap = 0;
+  int sm_count = 0;
+  // long range
+  int num_k = 0;
+  double kcutoff = 0;
+  std::string last_error;
+};
