@@ -70,6 +70,7 @@ def lib():
         "oracle_system_set_mode": (None, [p, i]),
         "oracle_init_random_fixed": (i, [p, u64, d]),
         "oracle_shortrange_single": (d, [p, i, i, ip, i, i]),
+        "oracle_shortrange_single_abs": (d, [p, i, i, ip, i, i]),
         "oracle_shortrange_dbeta": (d, [p, i, i, i]),
         "oracle_kinetic_single": (d, [p, i, i, ip, i, i]),
         "oracle_kinetic_dbeta": (d, [p, i, i, i]),
@@ -235,6 +236,11 @@ class System:
         a = np.ascontiguousarray(active, dtype=np.int32)
         self.set_mode(copy)
         return lib().oracle_shortrange_single(self.h, s1, s2, _ip(a), len(a), level)
+
+    def shortrange_single_abs(self, s1, s2, active, level, copy=0):
+        a = np.ascontiguousarray(active, dtype=np.int32)
+        self.set_mode(copy)
+        return lib().oracle_shortrange_single_abs(self.h, s1, s2, _ip(a), len(a), level)
 
     def shortrange_dbeta(self, s1, s2, level=0):
         self.set_mode(0)

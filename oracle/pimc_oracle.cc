@@ -801,7 +801,8 @@ struct OracleSystem {
   }
 
   // ShortRangeClass::SingleAction (ShortRangeClass.cc:191-236)
-  double ShortRangeSingle(int slice1, int slice2, const int *changed, int nchanged, int level) {
+  double ShortRangeSingle(int slice1, int slice2, const int *changed, int nchanged, int level,
+                          bool absolute = false) {
     double TotalU = 0.0;
     std::vector<char> DoPtcl(N, 1);
     int skip = 1 << level;
@@ -820,7 +821,7 @@ struct OracleSystem {
           double z = (rmag - rpmag);
           double U = pa->U(q, z, s2, level);
           if (pa->IsLongRange() && UseLongRange) U -= 0.5 * (Ulong(level, rmag) + Ulong(level, rpmag));
-          TotalU += U;
+          TotalU += absolute ? fabs(U) : U;
         }
       }
     }
@@ -1227,6 +1228,9 @@ int oracle_init_random_fixed(OracleSystem *s, uint64_t seed, double radius) {
 
 double oracle_shortrange_single(OracleSystem *s, int slice1, int slice2, const int *active, int n, int level) {
   return s->ShortRangeSingle(slice1, slice2, active, n, level);
+}
+double oracle_shortrange_single_abs(OracleSystem *s, int slice1, int slice2, const int *active, int n, int level) {
+  return s->ShortRangeSingle(slice1, slice2, active, n, level, true);
 }
 double oracle_shortrange_dbeta(OracleSystem *s, int slice1, int slice2, int level) {
   return s->ShortRangeDBeta(slice1, slice2, level);

@@ -79,6 +79,9 @@ int oracle_init_random_fixed(OracleSystem *s, uint64_t seed, double radius);
 
 double oracle_shortrange_single(OracleSystem *s, int slice1, int slice2, const int *active,
                                 int n_active, int level);
+/* Sum of |U| over the same terms: the scale of the summation error. */
+double oracle_shortrange_single_abs(OracleSystem *s, int slice1, int slice2, const int *active,
+                                    int n_active, int level);
 double oracle_shortrange_dbeta(OracleSystem *s, int slice1, int slice2, int level);
 double oracle_kinetic_single(OracleSystem *s, int slice1, int slice2, const int *active,
                              int n_active, int level);
