@@ -234,21 +234,32 @@ def run_ours(args):
     n, slices, L = cfg["N"], cfg["M"] + 1, cfg["levels"]
     start = initial_path(n, slices, box, 17 + rank, 0.45 * 2.556)
 
-    def make(precision, shadow=False, cl=args.cluster, threads=args.threads):
+    def make(precision, shadow=False, cl=args.cluster, threads=args.threads, schedule=None):
+        schedule = P.WINDOWS if (schedule if schedule is not None else args.schedule) == "windows" else P.SEQUENTIAL
         d = P.PathData(n, slices, box, tau, 6.0596, 0, device=local)
         d.pa_tricubic(qg, yg, tg, tau, umat, dumat, pg, pot)
         d.set_path(start)
-        bb = P.BisectionBlock(d, L, 1, precision=precision, shadow=shadow, cluster_ctas=cl, threads_per_cta=threads)
+        bb = P.BisectionBlock(d, L, args.steps_per_block, precision=precision, shadow=shadow, cluster_ctas=cl,
+                              threads_per_cta=threads, schedule=schedule)
         bb.seed(1000 + rank)
         return d, bb
 
+    # blocks per step: the windows schedule runs one round (one launch) per block
+    def blocks_for(schedule):
+        per = ((slices - 1) >> L) if schedule == "windows" else 1
+        return max(1, args.moves // (args.steps_per_block * per))
+
+    blocks = blocks_for(args.schedule)
+
     flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=f"cuda:{local}")
 
-    def timed(precision):
-        d, bb = make(precision)
+    def timed(precision, schedule=None, steps=None):
+        steps = steps or args.steps
+        d, bb = make(precision, schedule=schedule)
+        nb = blocks_for(schedule or args.schedule)
         stream = torch.cuda.ExternalStream(P.lib().pimc_stream(d.h), device=f"cuda:{local}")
         for _ in range(args.warmup):
-            bb.launch_async(args.moves)
+            bb.launch_async(nb)
         d.synchronize()
         s0 = bb.stats()
         times = []
@@ -258,13 +269,13 @@ def run_ours(args):
         if dist:
             dist.barrier()
         torch.cuda.synchronize()
-        for _ in range(args.steps):
+        for _ in range(steps):
             with torch.cuda.stream(stream):
                 flush.zero_()  # L2 flush between steps, outside the timed events
                 e0 = torch.cuda.Event(enable_timing=True)
                 e1 = torch.cuda.Event(enable_timing=True)
                 e0.record(stream)
-                bb.launch_async(args.moves)
+                bb.launch_async(nb)
                 e1.record(stream)
             e1.synchronize()
             times.append(e0.elapsed_time(e1))
@@ -295,11 +306,14 @@ def run_ours(args):
     ms32, st32, clocks = timed(P.MIXED)
     ms64, st64 = agg(ms64, st64)
     ms32, st32 = agg(ms32, st32)
+    other = "sequential" if args.schedule == "windows" else "windows"
+    ms_o, st_o, _ = timed(P.MIXED, schedule=other, steps=2)
+    ms_o, st_o = agg(ms_o, st_o)
 
     # dS accuracy of the mixed path: mixed decisions with the FP64 terms alongside
-    d, bb = make(P.MIXED, shadow=True)
-    bb.MakeMoves(200, trace=False)
-    rec, sh = bb.MakeMoves(args.accuracy_moves, trace=True)
+    d, bb = make(P.MIXED, shadow=True, schedule="sequential")
+    bb.MakeMoves(200 // args.steps_per_block, trace=False)
+    rec, sh = bb.MakeMoves(max(1, args.accuracy_moves // args.steps_per_block), trace=True)
     d.close()
     m = rec["dS_shadow"] != 0.0
     rel = np.abs(rec["dS"][m] - rec["dS_shadow"][m]) / np.abs(rec["dS_shadow"][m])
@@ -310,14 +324,14 @@ def run_ours(args):
     host = start.copy()
     for _ in range(2):
         d.set_path(host)
-        bb.MakeMoves(args.moves, trace=False)
+        bb.MakeMoves(blocks, trace=False)
         host = d.get_path(P.OLDMODE)
     e2e_t, e2e_evals = 0.0, 0
     for _ in range(args.steps):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         d.set_path(host)
-        _, st = bb.MakeMoves(args.moves, trace=False)
+        _, st = bb.MakeMoves(blocks, trace=False)
         host = d.get_path(P.OLDMODE)
         e2e_t += time.perf_counter() - t0
     e2e_evals = bb.stats()["pair_evals"]
@@ -349,8 +363,9 @@ def run_ours(args):
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms32 / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32 pair terms / f64 sums", "data": "synthetic",
-            "config": {"workload": W_NAME, "moves_per_step": args.moves, "cluster_ctas": args.cluster,
-                       "threads_per_cta": args.threads,
+            "config": {"workload": W_NAME, "moves_per_step": st32["moves"] // world // args.steps,
+                       "schedule": args.schedule, "steps_per_block": args.steps_per_block,
+                       "cluster_ctas": args.cluster, "threads_per_cta": args.threads,
                        "l2": "flushed between steps by a 256 MiB write outside the timed events",
                        "parallelism": f"replicas x{world}"},
             "moves_per_s": st32["moves"] / (ms32 / 1000.0),
@@ -358,13 +373,15 @@ def run_ours(args):
             "fp64": {"pair_evals_per_s": value64, "moves_per_s": st64["moves"] / (ms64 / 1000.0),
                      "accepted_moves_per_s": st64["accepted"] / (ms64 / 1000.0), "ms_per_step": ms64 / args.steps},
             "mixed_over_fp64": value / value64 if value64 else None,
+            other: {"pair_evals_per_s": st_o["pair_evals"] / (ms_o / 1000.0),
+                    "moves_per_s": st_o["moves"] / (ms_o / 1000.0), "precision": "mixed"},
             "dS_relerr": {"median": float(np.median(rel)) if rel.size else None,
                           "p99": float(np.quantile(rel, 0.99)) if rel.size else None,
                           "max": float(np.max(rel)) if rel.size else None, "stages": int(rel.size),
                           "flip_rate": flip_rate},
             "e2e": {"value": e2e_evals_timed / e2e_t if e2e_t else None, "unit": UNIT,
                     "h2d_bytes_per_step": path_bytes, "d2h_bytes_per_step": path_bytes + 48},
-            "gpu_launches": args.steps * 2,
+            "gpu_launches": args.steps * 2 * nb_launches(args.schedule, blocks),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
                          "bytes_per_eval": BYTES_PER_EVAL["mixed"],
@@ -380,6 +397,11 @@ def run_ours(args):
         dist.destroy_process_group()
 
 
+def nb_launches(schedule, blocks):
+    """Bisection-kernel launches per timed step (FP64 + mixed counted by the caller)."""
+    return blocks if schedule == "windows" else 1
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -387,6 +409,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--moves", type=int, default=2048)
+    ap.add_argument("--schedule", default="windows", choices=["windows", "sequential"])
+    ap.add_argument("--steps-per-block", type=int, default=8)
     ap.add_argument("--cluster", type=int, default=8)
     ap.add_argument("--threads", type=int, default=256)
     ap.add_argument("--accuracy-moves", type=int, default=1000)

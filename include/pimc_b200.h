@@ -163,6 +163,14 @@ int pimc_get_rhok(pimc_context *ctx, int copy, double *out /* [slices][num_k][2]
 
 /* ---- device-resident bisection moves (BisectionBlockClass::MakeMove) ---- */
 
+/* Move schedules.  SEQUENTIAL is the reference's: one move at a time, the
+ * window start drawn from the Local stream (ChooseTimeSlices).  WINDOWS runs
+ * one round per block: a Common-stream offset o in [0, 2^L) and concurrent
+ * BisectionBlocks on the disjoint windows [o + w 2^L, o + (w+1) 2^L], each
+ * with its own Local stream (PIMC++'s time-slice parallelism on one GPU). */
+#define PIMC_SCHEDULE_SEQUENTIAL 0
+#define PIMC_SCHEDULE_WINDOWS 1
+
 typedef struct pimc_bisection_desc {
   int num_levels;                   /* Move{NumLevels} */
   int steps_per_block;              /* Move{StepsPerBlock} */
@@ -172,6 +180,7 @@ typedef struct pimc_bisection_desc {
   int shadow;                       /* also evaluate the other precision, for dS error */
   int cluster_ctas;                 /* CTAs cooperating on one chain (1..16), 0 = auto */
   int threads_per_cta;              /* 0 = auto */
+  int schedule;                     /* PIMC_SCHEDULE_SEQUENTIAL or PIMC_SCHEDULE_WINDOWS */
 } pimc_bisection_desc;
 
 /* One move: the fields the accept trace is compared on. */
@@ -195,11 +204,16 @@ typedef struct pimc_bisection_stats {
 } pimc_bisection_stats;
 
 int pimc_bisection_setup(pimc_context *ctx, const pimc_bisection_desc *desc);
-/* Seeds the Local stream of the chain (Philox-4x32-10 key; counter reset). */
+/* Seeds the chain's streams (Philox-4x32-10 key; counters reset): the Local
+ * stream of the sequential schedule and the per-window streams. */
 int pimc_rng_seed(pimc_context *ctx, uint64_t seed);
-/* Runs n_blocks BisectionBlock moves on the device (OLD copy is the state;
- * NEW is brought back in sync afterwards).  trace: n_blocks*steps_per_block
- * records or NULL.  stats: accumulated since the last pimc_bisection_setup. */
+/* Window slots per round of the WINDOWS schedule: floor((slices-1) / 2^L). */
+int pimc_bisection_windows(pimc_context *ctx, int *windows);
+/* Runs n_blocks BisectionBlocks on the device (OLD copy is the state; NEW is
+ * brought back in sync afterwards).  SEQUENTIAL: n_blocks*steps_per_block
+ * moves.  WINDOWS: n_blocks rounds of windows*steps_per_block moves; the
+ * trace slots of windows that do not fit a round have slice1 = -1.
+ * trace: that many records or NULL.  stats: accumulated since setup. */
 int pimc_run_bisection(pimc_context *ctx, int n_blocks, pimc_move_record *trace,
                        pimc_bisection_stats *stats);
 /* Enqueues n_blocks moves on the context stream without synchronising or

@@ -87,6 +87,7 @@ def lib():
         "oracle_rng_seed": (None, [p, u64]),
         "oracle_run_bisection": (i, [p, i, C.POINTER(MoveRecord)]),
         "oracle_rng_position": (u64, [p]),
+        "oracle_run_windows": (i, [p, i, C.POINTER(MoveRecord)]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
@@ -297,6 +298,7 @@ class System:
     def bisection_config(self, num_levels, steps_per_block=1, shortrange_at_higher_levels=True,
                          use_longrange=False):
         self.steps_per_block = steps_per_block
+        self.num_levels = num_levels
         lib().oracle_bisection_config(self.h, num_levels, steps_per_block, int(shortrange_at_higher_levels),
                                       int(use_longrange))
 
@@ -307,6 +309,12 @@ class System:
         n = n_blocks * self.steps_per_block
         recs = (MoveRecord * n)()
         lib().oracle_run_bisection(self.h, n_blocks, recs)
+        return recs
+
+    def run_windows(self, n_rounds):
+        w = min((self.S - 1) >> self.num_levels, 64)
+        recs = (MoveRecord * (n_rounds * w * self.steps_per_block))()
+        lib().oracle_run_windows(self.h, n_rounds, recs)
         return recs
 
     def rng_position(self):

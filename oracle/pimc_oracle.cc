@@ -7,6 +7,7 @@
 
 #include "pimc_oracle.h"
 
+#include <algorithm>
 #include <cmath>
 #include <complex>
 #include <cstdio>
@@ -54,10 +55,11 @@ enum { STREAM_LOCAL = 0, STREAM_COMMON = 1, STREAM_WORLD = 2 };
 // RandomClass semantics (Common/Random/Random.h:33-49,156-180,268-273).
 struct Random {
   uint64_t seed = 0;
+  uint32_t stream = STREAM_LOCAL;  // Philox stream of Local()
   uint64_t nlocal = 0, nworld = 0;
   bool one_left = false;  // the static polar-method cache, Random.h:159-160
   double x2 = 0.0;
-  double Local() { return philox_uniform(seed, STREAM_LOCAL, nlocal++); }
+  double Local() { return philox_uniform(seed, stream, nlocal++); }
   double World() { return philox_uniform(seed, STREAM_WORLD, nworld++); }
   int LocalInt(int max) { return (int)floor(Local() * max); }
   double LocalGaussian(double sigma) {
@@ -746,6 +748,8 @@ struct OracleSystem {
   int mode = 0;                 // ActiveCopy (MirroredClass.cc:19): 0 OLD, 1 NEW
   OraclePA *pa = nullptr;
   Random rng;
+  std::vector<Random> wrng;       // per-window Local streams of the concurrent schedule
+  uint64_t rounds = 0;            // Common-stream index of the next round
   // bisection
   int NumLevels = 1, StepsPerBlock = 1, SRHigher = 1, UseLongRange = 0;
   // long range
@@ -1163,6 +1167,32 @@ struct OracleSystem {
   }
   // BisectionBlockClass::MakeMove (BisectionBlock.cc:380-451) with
   // ChooseTimeSlices (:310-378), no reference slice.
+  // Concurrent-window schedule (the CUDA library's PIMC_SCHEDULE_WINDOWS),
+  // replayed sequentially: round r draws o = floor(Common() * 2^L) at
+  // Common-stream index r and runs one block per window [o + w 2^L, ...],
+  // window w drawing from its own Local stream.  The windows commute, so the
+  // order here is immaterial.
+  void MakeRound(OracleMoveRecord *recs) {
+    const int span = 1 << NumLevels;
+    const int W = std::min((NumSlices - 1) >> NumLevels, 64);
+    const int o = (int)floor(philox_uniform(rng.seed, STREAM_COMMON, rounds) * span);
+    rounds++;
+    for (int w = 0; w < W; w++) {
+      OracleMoveRecord *r = recs + (size_t)w * StepsPerBlock;
+      const int slice1 = o + w * span;
+      if (slice1 + span > NumSlices - 1) {
+        for (int st = 0; st < StepsPerBlock; st++) {
+          memset(&r[st], 0, sizeof(OracleMoveRecord));
+          r[st].slice1 = -1;
+          r[st].ptcl = -1;
+        }
+        continue;
+      }
+      std::swap(rng, wrng[w]);
+      for (int st = 0; st < StepsPerBlock; st++) MakeMove(slice1, slice1 + span, &r[st]);
+      std::swap(rng, wrng[w]);
+    }
+  }
   void MakeBlock(OracleMoveRecord *recs) {
     int sliceSep = 1 << NumLevels;
     int numLeft = NumSlices - sliceSep;
@@ -1290,8 +1320,20 @@ void oracle_bisection_config(OracleSystem *s, int num_levels, int steps_per_bloc
 }
 void oracle_rng_seed(OracleSystem *s, uint64_t seed) {
   s->rng.seed = seed;
+  s->rng.stream = STREAM_LOCAL;
   s->rng.nlocal = 0;
   s->rng.one_left = false;
+  s->wrng.assign(64, Random());
+  for (int w = 0; w < 64; w++) {
+    s->wrng[w].seed = seed;
+    s->wrng[w].stream = 0x100u + (uint32_t)w;
+  }
+  s->rounds = 0;
+}
+int oracle_run_windows(OracleSystem *s, int n_rounds, OracleMoveRecord *records) {
+  const int W = std::min((s->NumSlices - 1) >> s->NumLevels, 64);
+  for (int r = 0; r < n_rounds; r++) s->MakeRound(records + (size_t)r * W * s->StepsPerBlock);
+  return W;
 }
 int oracle_run_bisection(OracleSystem *s, int n_blocks, OracleMoveRecord *records) {
   for (int b = 0; b < n_blocks; b++) s->MakeBlock(records + (size_t)b * s->StepsPerBlock);

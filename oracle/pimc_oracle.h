@@ -117,6 +117,10 @@ void oracle_bisection_config(OracleSystem *s, int num_levels, int steps_per_bloc
 void oracle_rng_seed(OracleSystem *s, uint64_t seed);
 /* Runs n_blocks BisectionBlock moves; fills n_blocks*steps_per_block records. */
 int oracle_run_bisection(OracleSystem *s, int n_blocks, OracleMoveRecord *records);
+/* Concurrent-window schedule replayed sequentially: n_rounds rounds, each
+ * windows*steps_per_block records (slice1 = -1 for a window that does not
+ * fit); returns windows = floor((slices-1)/2^L). */
+int oracle_run_windows(OracleSystem *s, int n_rounds, OracleMoveRecord *records);
 uint64_t oracle_rng_position(OracleSystem *s);
 
 #ifdef __cplusplus

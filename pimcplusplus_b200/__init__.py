@@ -33,6 +33,7 @@ OLDMODE, NEWMODE, BOTH = 0, 1, 2
 FP64, MIXED = 0, 1
 ACTION_SHORTRANGE, ACTION_KINETIC, ACTION_LONGRANGE = 0, 1, 2
 GRID_LINEAR, GRID_LOG = 0, 1
+SEQUENTIAL, WINDOWS = 0, 1
 
 STATUS = {
     0: "ok", 1: "invalid argument", 2: "CUDA error", 3: "non-finite action", 4: "index out of range",
@@ -71,6 +72,7 @@ class BisectionDesc(C.Structure):
         ("shadow", C.c_int),
         ("cluster_ctas", C.c_int),
         ("threads_per_cta", C.c_int),
+        ("schedule", C.c_int),
     ]
 
 
@@ -121,6 +123,7 @@ _SIGS = {
     "pimc_get_rhok": (_i, [_p, _i, _dp]),
     "pimc_bisection_setup": (_i, [_p, C.POINTER(BisectionDesc)]),
     "pimc_rng_seed": (_i, [_p, C.c_uint64]),
+    "pimc_bisection_windows": (_i, [_p, _ip]),
     "pimc_run_bisection": (_i, [_p, _i, _p, C.POINTER(BisectionStats)]),
     "pimc_run_bisection_async": (_i, [_p, _i]),
     "pimc_bisection_get_stats": (_i, [_p, C.POINTER(BisectionStats)]),
@@ -320,7 +323,7 @@ class BisectionBlock:
     """
 
     def __init__(self, path_data: PathData, num_levels, steps_per_block=1, shortrange_at_higher_levels=True,
-                 precision=FP64, shadow=False, cluster_ctas=0, threads_per_cta=0):
+                 precision=FP64, shadow=False, cluster_ctas=0, threads_per_cta=0, schedule=SEQUENTIAL):
         self.PathData = path_data
         d = BisectionDesc()
         d.num_levels = num_levels
@@ -331,16 +334,20 @@ class BisectionBlock:
         d.shadow = int(shadow)
         d.cluster_ctas = cluster_ctas
         d.threads_per_cta = threads_per_cta
+        d.schedule = schedule
         self.desc = d
         self.steps_per_block = steps_per_block
         path_data._check(_lib.pimc_bisection_setup(path_data.h, C.byref(d)), "bisection_setup")
+        w = C.c_int()
+        path_data._check(_lib.pimc_bisection_windows(path_data.h, C.byref(w)), "bisection_windows")
+        self.windows = w.value
 
     def seed(self, seed):
         self.PathData._check(_lib.pimc_rng_seed(self.PathData.h, C.c_uint64(seed)), "rng_seed")
 
     def MakeMoves(self, n_blocks, trace=True):
         st = BisectionStats()
-        rec = np.zeros(n_blocks * self.steps_per_block, dtype=MOVE_RECORD) if trace else None
+        rec = np.zeros(n_blocks * self.windows * self.steps_per_block, dtype=MOVE_RECORD) if trace else None
         ptr = rec.ctypes.data_as(_p) if trace else None
         self.PathData._check(_lib.pimc_run_bisection(self.PathData.h, n_blocks, ptr, C.byref(st)), "run_bisection")
         return rec, st.as_dict()

@@ -190,8 +190,8 @@ int pimc_create(const pimc_system_desc *d, pimc_context **out) {
   if (e == cudaSuccess) e = cudaMemset(ctx->d_counter, 0, sizeof(unsigned int));
   if (e == cudaSuccess) e = cudaMalloc(&ctx->d_out, 4 * sizeof(double));
   if (e == cudaSuccess) e = cudaMallocHost(&ctx->h_out, 4 * sizeof(double));
-  if (e == cudaSuccess) e = cudaMalloc(&ctx->d_chain, sizeof(ChainState));
-  if (e == cudaSuccess) e = cudaMemset(ctx->d_chain, 0, sizeof(ChainState));
+  if (e == cudaSuccess) e = cudaMalloc(&ctx->d_chain, kMaxWindows * sizeof(ChainState));
+  if (e == cudaSuccess) e = cudaMemset(ctx->d_chain, 0, kMaxWindows * sizeof(ChainState));
   if (e == cudaSuccess) e = cudaDeviceGetAttribute(&ctx->sm_count, cudaDevAttrMultiProcessorCount, d->device);
   if (e == cudaSuccess) e = cudaMemset(ctx->d_path[0], 0, ctx->path_elems * sizeof(double));
   if (e == cudaSuccess) e = cudaMemset(ctx->d_path[1], 0, ctx->path_elems * sizeof(double));
@@ -484,6 +484,11 @@ int pimc_reject_copy(pimc_context *ctx, int slice1, int slice2, const int *activ
 }
 
 // ---- bisection ----
+static int window_slots(const pimc_context *ctx, int num_levels) {
+  int w = (ctx->sys.S - 1) >> num_levels;
+  return std::max(0, std::min(w, kMaxWindows));
+}
+
 int pimc_bisection_setup(pimc_context *ctx, const pimc_bisection_desc *d) {
   if (!ctx || !d) return PIMC_E_ARG;
   if (ctx->pa.kind == PA_NONE) return fail(ctx, PIMC_E_STATE, "no pair action set");
@@ -494,6 +499,10 @@ int pimc_bisection_setup(pimc_context *ctx, const pimc_bisection_desc *d) {
   if (d->cluster_ctas < 0 || d->cluster_ctas > kMaxCluster) return fail(ctx, PIMC_E_ARG, "cluster_ctas 0..16");
   if (d->threads_per_cta != 0 && (d->threads_per_cta < 64 || d->threads_per_cta > 512 || d->threads_per_cta % 32))
     return fail(ctx, PIMC_E_ARG, "threads_per_cta must be a multiple of 32 in 64..512");
+  if (d->schedule != PIMC_SCHEDULE_SEQUENTIAL && d->schedule != PIMC_SCHEDULE_WINDOWS)
+    return fail(ctx, PIMC_E_ARG, "bad schedule");
+  if (d->schedule == PIMC_SCHEDULE_WINDOWS && window_slots(ctx, d->num_levels) < 1)
+    return fail(ctx, PIMC_E_ARG, "no window fits");
   if (d->use_longrange) return fail(ctx, PIMC_E_ARG, "long range inside device moves is not available");
   if (ctx->pa.kind == PA_DAVID && d->num_levels + ctx->pa.d64.tau_pos > ctx->pa.d64.num_tau)
     return fail(ctx, PIMC_E_ARG, "pair action has fewer tau levels than NumLevels");
@@ -503,11 +512,13 @@ int pimc_bisection_setup(pimc_context *ctx, const pimc_bisection_desc *d) {
   ctx->bis = *d;
   if (ctx->bis.cluster_ctas == 0) ctx->bis.cluster_ctas = ctx->sys.N >= 256 ? 8 : 1;
   if (ctx->bis.threads_per_cta == 0) ctx->bis.threads_per_cta = 256;
-  ChainState cs;
-  CK(cudaMemcpy(&cs, ctx->d_chain, sizeof(cs), cudaMemcpyDeviceToHost));
-  cs.moves = cs.accepted = cs.stages = cs.pair_evals = cs.flips = 0;
-  cs.status = 0;
-  CK(cudaMemcpy(ctx->d_chain, &cs, sizeof(cs), cudaMemcpyHostToDevice));
+  std::vector<ChainState> cs(kMaxWindows);
+  CK(cudaMemcpy(cs.data(), ctx->d_chain, cs.size() * sizeof(ChainState), cudaMemcpyDeviceToHost));
+  for (auto &c : cs) {
+    c.moves = c.accepted = c.stages = c.pair_evals = c.flips = 0;
+    c.status = 0;
+  }
+  CK(cudaMemcpy(ctx->d_chain, cs.data(), cs.size() * sizeof(ChainState), cudaMemcpyHostToDevice));
   ctx->bis_ready = true;
   return PIMC_OK;
 }
@@ -515,30 +526,61 @@ int pimc_bisection_setup(pimc_context *ctx, const pimc_bisection_desc *d) {
 int pimc_rng_seed(pimc_context *ctx, uint64_t seed) {
   if (!ctx) return PIMC_E_ARG;
   CK(cudaSetDevice(ctx->device));
-  ChainState cs;
-  CK(cudaMemcpy(&cs, ctx->d_chain, sizeof(cs), cudaMemcpyDeviceToHost));
-  cs.seed = seed;
-  cs.nlocal = 0;
-  cs.one_left = 0;
-  cs.x2 = 0.0;
-  CK(cudaMemcpy(ctx->d_chain, &cs, sizeof(cs), cudaMemcpyHostToDevice));
+  std::vector<ChainState> cs(kMaxWindows);
+  CK(cudaMemcpy(cs.data(), ctx->d_chain, cs.size() * sizeof(ChainState), cudaMemcpyDeviceToHost));
+  for (int w = 0; w < kMaxWindows; w++) {
+    cs[w].seed = seed;
+    cs[w].nlocal = 0;
+    cs[w].stream = w == 0 && ctx->bis.schedule == PIMC_SCHEDULE_SEQUENTIAL ? kStreamLocal : kStreamWindow0 + w;
+    cs[w].one_left = 0;
+    cs[w].x2 = 0.0;
+  }
+  // stream ids are fixed by the schedule at seeding time; window 0 of the
+  // concurrent schedule uses kStreamWindow0, the sequential chain kStreamLocal
+  cs[0].stream = ctx->bis.schedule == PIMC_SCHEDULE_WINDOWS ? kStreamWindow0 : kStreamLocal;
+  ctx->rounds = 0;
+  CK(cudaMemcpy(ctx->d_chain, cs.data(), cs.size() * sizeof(ChainState), cudaMemcpyHostToDevice));
   return PIMC_OK;
 }
 
-static int run_bisection(pimc_context *ctx, int n_blocks, pimc_move_record *device_trace, long long offset) {
+int pimc_bisection_windows(pimc_context *ctx, int *windows) {
+  if (!ctx || !windows) return PIMC_E_ARG;
+  if (!ctx->bis_ready) return fail(ctx, PIMC_E_STATE, "pimc_bisection_setup not called");
+  *windows = ctx->bis.schedule == PIMC_SCHEDULE_WINDOWS ? window_slots(ctx, ctx->bis.num_levels) : 1;
+  return PIMC_OK;
+}
+
+static size_t records_for(const pimc_context *ctx, int n_blocks) {
+  size_t per = ctx->bis.schedule == PIMC_SCHEDULE_WINDOWS ? (size_t)window_slots(ctx, ctx->bis.num_levels) : 1;
+  return (size_t)n_blocks * per * ctx->bis.steps_per_block;
+}
+
+static int run_bisection(pimc_context *ctx, int n_blocks, pimc_move_record *device_trace) {
   BisectionArgs a;
   a.path = ctx->d_path[PIMC_OLD];
   a.sys = ctx->sys;
   a.pa = ctx->pa;
-  a.chain = ctx->d_chain;
+  a.chains = ctx->d_chain;
   a.trace = device_trace;
-  a.trace_offset = offset;
+  a.trace_offset = 0;
   a.num_levels = ctx->bis.num_levels;
   a.steps_per_block = ctx->bis.steps_per_block;
   a.n_blocks = n_blocks;
   a.sr_higher = ctx->bis.shortrange_at_higher_levels;
-  CK(launch_bisection(a, ctx->bis.precision, ctx->bis.shadow, ctx->bis.cluster_ctas, ctx->bis.threads_per_cta,
-                      ctx->stream));
+  a.concurrent = ctx->bis.schedule == PIMC_SCHEDULE_WINDOWS;
+  a.round = ctx->rounds;
+  const int cl = ctx->bis.cluster_ctas, thr = ctx->bis.threads_per_cta;
+  if (!a.concurrent) {
+    CK(launch_bisection(a, ctx->bis.precision, ctx->bis.shadow, cl, 1, thr, ctx->stream));
+    return PIMC_OK;
+  }
+  const int W = window_slots(ctx, ctx->bis.num_levels);
+  for (int r = 0; r < n_blocks; r++) {
+    a.round = ctx->rounds + r;
+    a.trace_offset = (long long)r * W * ctx->bis.steps_per_block;
+    CK(launch_bisection(a, ctx->bis.precision, ctx->bis.shadow, cl, W, thr, ctx->stream));
+  }
+  ctx->rounds += n_blocks;
   return PIMC_OK;
 }
 
@@ -546,14 +588,14 @@ int pimc_run_bisection_async(pimc_context *ctx, int n_blocks) {
   if (!ctx || n_blocks < 0) return PIMC_E_ARG;
   if (!ctx->bis_ready) return fail(ctx, PIMC_E_STATE, "pimc_bisection_setup not called");
   CK(cudaSetDevice(ctx->device));
-  return run_bisection(ctx, n_blocks, nullptr, 0);
+  return run_bisection(ctx, n_blocks, nullptr);
 }
 
 int pimc_run_bisection(pimc_context *ctx, int n_blocks, pimc_move_record *trace, pimc_bisection_stats *stats) {
   if (!ctx || n_blocks < 0) return PIMC_E_ARG;
   if (!ctx->bis_ready) return fail(ctx, PIMC_E_STATE, "pimc_bisection_setup not called");
   CK(cudaSetDevice(ctx->device));
-  const size_t nrec = (size_t)n_blocks * ctx->bis.steps_per_block;
+  const size_t nrec = records_for(ctx, n_blocks);
   if (trace && nrec > ctx->trace_cap) {
     cudaFree(ctx->d_trace);
     ctx->d_trace = nullptr;
@@ -561,7 +603,7 @@ int pimc_run_bisection(pimc_context *ctx, int n_blocks, pimc_move_record *trace,
     CK(cudaMalloc(&ctx->d_trace, nrec * sizeof(pimc_move_record)));
     ctx->trace_cap = nrec;
   }
-  int rc = run_bisection(ctx, n_blocks, trace ? ctx->d_trace : nullptr, 0);
+  int rc = run_bisection(ctx, n_blocks, trace ? ctx->d_trace : nullptr);
   if (rc) return rc;
   // The device moves advance OLD only; bring NEW back in sync (MirroredClass invariant).
   CK(cudaMemcpyAsync(ctx->d_path[1], ctx->d_path[0], ctx->path_elems * sizeof(double), cudaMemcpyDeviceToDevice,
@@ -580,16 +622,18 @@ int pimc_run_bisection(pimc_context *ctx, int n_blocks, pimc_move_record *trace,
 int pimc_bisection_get_stats(pimc_context *ctx, pimc_bisection_stats *stats) {
   if (!ctx || !stats) return PIMC_E_ARG;
   CK(cudaSetDevice(ctx->device));
-  ChainState cs;
-  CK(cudaMemcpyAsync(&cs, ctx->d_chain, sizeof(cs), cudaMemcpyDeviceToHost, ctx->stream));
+  std::vector<ChainState> cs(kMaxWindows);
+  CK(cudaMemcpyAsync(cs.data(), ctx->d_chain, cs.size() * sizeof(ChainState), cudaMemcpyDeviceToHost, ctx->stream));
   CK(cudaStreamSynchronize(ctx->stream));
-  stats->moves = (int64_t)cs.moves;
-  stats->accepted = (int64_t)cs.accepted;
-  stats->stages_attempted = (int64_t)cs.stages;
-  stats->pair_evals = (int64_t)cs.pair_evals;
-  stats->flips = (int64_t)cs.flips;
-  stats->status = cs.status;
-  stats->pad = 0;
+  std::memset(stats, 0, sizeof(*stats));
+  for (const auto &c : cs) {
+    stats->moves += (int64_t)c.moves;
+    stats->accepted += (int64_t)c.accepted;
+    stats->stages_attempted += (int64_t)c.stages;
+    stats->pair_evals += (int64_t)c.pair_evals;
+    stats->flips += (int64_t)c.flips;
+    if (c.status && !stats->status) stats->status = c.status;
+  }
   return PIMC_OK;
 }
 

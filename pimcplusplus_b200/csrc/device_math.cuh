@@ -430,34 +430,64 @@ __device__ __forceinline__ double philox_uniform(uint64_t seed, uint32_t stream,
   return ((double)a * 67108864.0 + (double)b) * (1.0 / 9007199254740992.0);
 }
 
-// RandomClass on one thread: Local(), LocalInt(), LocalGaussian() with the
-// polar-method pair cache (Common/Random/Random.h:33-49,156-180).
+// RandomClass (Common/Random/Random.h:33-49,156-180): Local(), LocalInt(),
+// LocalGaussian() with the polar-method pair cache.  Every lane of a warp
+// holds the same copy and draws the same values (warp-uniform state).
 struct DevRandom {
   uint64_t seed, n;
+  uint32_t stream;
   int one_left;
   double x2;
-  __device__ __forceinline__ double Local() { return philox_uniform(seed, 0u, n++); }
+  __device__ __forceinline__ double Local() { return philox_uniform(seed, stream, n++); }
   __device__ __forceinline__ int LocalInt(int max) { return (int)floor(Local() * max); }
-  __device__ __forceinline__ double LocalGaussian(double sigma) {
-    double X1;
-    if (one_left) {
-      X1 = x2;
-      one_left = 0;
-    } else {
-      double V1, V2, S;
-      int guard = 0;
-      do {
-        V1 = 2.0 * Local() - 1.0;
-        V2 = 2.0 * Local() - 1.0;
-        S = V1 * V1 + V2 * V2;
-      } while (S >= 1.0 && ++guard < 1000000);
-      double temp = sqrt((-2.0 * log(S)) / S);
-      X1 = V1 * temp;
-      x2 = V2 * temp;
-      one_left = 1;
-    }
-    return X1 * sigma;
-  }
 };
+
+// G unit Gaussians in stream order into out[0..G-1], drawn by one full warp.
+// Sequentially, LocalGaussian returns the cached X2 if one is left, else
+// draws uniform pairs (V1, V2) until S = V1^2 + V2^2 < 1 and returns
+// X1 = V1 t, caching X2 = V2 t, t = sqrt(-2 ln S / S).  Here lane j tests the
+// candidate pair at stream offset 2j; a ballot orders the accepted pairs, so
+// the values, the cache and the stream position come out exactly as the
+// sequential loop leaves them.  Bounded: at most 4096 rounds of 32 pairs.
+__device__ __forceinline__ void warp_gaussians(DevRandom &rng, int G, double *out, int lane) {
+  int k = 0;
+  if (G > 0 && rng.one_left) {
+    if (lane == 0) out[0] = rng.x2;
+    rng.one_left = 0;
+    k = 1;
+  }
+  for (int guard = 0; k < G && guard < 4096; guard++) {
+    const int need = (G - k + 1) >> 1;
+    const uint64_t base = rng.n + 2ull * (uint64_t)lane;
+    const double V1 = 2.0 * philox_uniform(rng.seed, rng.stream, base) - 1.0;
+    const double V2 = 2.0 * philox_uniform(rng.seed, rng.stream, base + 1) - 1.0;
+    const double S = V1 * V1 + V2 * V2;
+    const bool acc = !(S >= 1.0);
+    const unsigned m = __ballot_sync(0xffffffffu, acc);
+    const int before = __popc(m & ((1u << lane) - 1u));
+    const int navail = __popc(m);
+    const double temp = sqrt((-2.0 * log(S)) / S);
+    const double X1 = V1 * temp, X2 = V2 * temp;
+    if (acc && before < need) {
+      const int idx = k + 2 * before;
+      out[idx] = X1;
+      if (idx + 1 < G) out[idx + 1] = X2;
+    }
+    if (navail >= need) {
+      const unsigned lastm = __ballot_sync(0xffffffffu, acc && before == need - 1);
+      const int p = __ffs(lastm) - 1;
+      const double x2p = __shfl_sync(0xffffffffu, X2, p);
+      if ((G - k) & 1) {
+        rng.x2 = x2p;
+        rng.one_left = 1;
+      }
+      rng.n += 2ull * (uint64_t)(p + 1);
+      k = G;
+    } else {
+      rng.n += 64;
+      k += 2 * navail;
+    }
+  }
+}
 
 }  // namespace pimc

@@ -97,13 +97,20 @@ struct DevSystem {
   int num_images;
 };
 
-// Per-chain device state of the bisection driver.
+constexpr int kMaxWindows = 64;      // concurrent slice windows of one chain
+constexpr uint32_t kStreamLocal = 0, kStreamCommon = 1, kStreamWorld = 2;
+constexpr uint32_t kStreamWindow0 = 0x100;  // Local stream of window w is kStreamWindow0 + w
+
+// Device state of one Local RNG stream and its move counters: the chain in
+// the sequential schedule, or one slice window in the concurrent schedule.
 struct ChainState {
   uint64_t seed;
-  uint64_t nlocal;     // position in the Local stream
+  uint64_t nlocal;     // position in the stream
+  uint32_t stream;     // Philox stream id
   int32_t one_left;    // LocalGaussian cache flag (Random.h:159-160)
-  int32_t status;
   double x2;           // cached second Gaussian
+  int32_t status;
+  int32_t pad;
   unsigned long long moves, accepted, stages, pair_evals, flips;
 };
 
@@ -135,7 +142,8 @@ struct pimc_context {
   // bisection
   pimc_bisection_desc bis{};
   bool bis_ready = false;
-  pimc::ChainState *d_chain = nullptr;
+  pimc::ChainState *d_chain = nullptr;  // kMaxWindows states
+  unsigned long long rounds = 0;         // concurrent-window rounds run so far
   pimc_move_record *d_trace = nullptr;
   size_t trace_cap = 0;
   int sm_count = 0;

@@ -247,3 +247,60 @@ def test_bisection_mixed_shadow_dS_error(tmp_path):
     rel = np.abs(rec["dS"][mask] - rec["dS_shadow"][mask]) / np.maximum(np.abs(rec["dS_shadow"][mask]), 1e-3)
     assert np.median(rel) < 1e-5
     assert stats["flips"] <= 0.01 * stats["stages_attempted"] + 1
+
+
+def compare_window_traces(ref, got, stats, tol=1e-9):
+    assert len(ref) == len(got)
+    n_moves = 0
+    for i, (r, g) in enumerate(zip(ref, got)):
+        assert (r.slice1, r.ptcl, r.accepted, r.stages_passed) == (
+            int(g["slice1"]), int(g["ptcl"]), int(g["accepted"]), int(g["stages_passed"])), i
+        if r.slice1 >= 0:
+            n_moves += 1
+        for k in range(8):
+            assert abs(r.dS[k] - g["dS"][k]) <= tol * max(1.0, abs(r.dS[k])), (i, k, r.dS[k], g["dS"][k])
+    assert stats["moves"] == n_moves
+    assert stats["status"] == 0
+
+
+@pytest.mark.parametrize("cluster", [1, 2])
+def test_bisection_trace_windows_david(tmp_path, cluster):
+    """Concurrent-window schedule (time-slice parallel) against the oracle's
+    sequential replay of the same rounds."""
+    cfg, tau, box, dm = lj_case(tmp_path)
+    n, slices = cfg["N"], cfg["M"] + 1
+    o = O.System(n, slices, box, tau, W.HE4_LAMBDA, 0)
+    o.set_pa(O.PairAction.from_dm(dm, tau, 0))
+    o.init_random_fixed(37, 0.45 * W.LJ_SIGMA)
+    d = P.PathData(n, slices, box, tau, W.HE4_LAMBDA, 0)
+    d.set_path(o.get_path(0))
+    d.pa_david_from_dm(dm, 0)
+    o.bisection_config(3, 2)
+    o.rng_seed(41)
+    ref = o.run_windows(60)
+    bb = P.BisectionBlock(d, 3, 2, cluster_ctas=cluster, threads_per_cta=128, schedule=P.WINDOWS)
+    assert bb.windows == 5
+    bb.seed(41)
+    got, stats = bb.MakeMoves(60)
+    compare_window_traces(ref, got, stats)
+    assert np.max(np.abs(d.get_path(P.OLDMODE) - o.get_path(0))) < 1e-9
+
+
+def test_bisection_trace_windows_tricubic():
+    cfg, tau, box, tabs = tricubic_case()
+    qg, yg, tg, umat, dumat, pg, pot = tabs
+    n, slices = cfg["N"], cfg["M"] + 1
+    o = O.System(n, slices, box, tau, W.HE4_LAMBDA, 0)
+    o.set_pa(O.PairAction.tricubic(qg, yg, tg, tau, umat, dumat, pg, pot))
+    o.init_random_fixed(43, 0.45 * W.LJ_SIGMA)
+    d = P.PathData(n, slices, box, tau, W.HE4_LAMBDA, 0)
+    d.set_path(o.get_path(0))
+    d.pa_tricubic(qg, yg, tg, tau, umat, dumat, pg, pot)
+    o.bisection_config(3, 1)
+    o.rng_seed(47)
+    ref = o.run_windows(50)
+    bb = P.BisectionBlock(d, 3, 1, cluster_ctas=4, threads_per_cta=256, schedule=P.WINDOWS, precision=P.FP64)
+    bb.seed(47)
+    got, stats = bb.MakeMoves(50)
+    compare_window_traces(ref, got, stats)
+    assert np.max(np.abs(d.get_path(P.OLDMODE) - o.get_path(0))) < 1e-9
