@@ -6,20 +6,22 @@
 //    particle's OLD and NEW window positions live in shared memory, so NEW
 //    never touches HBM; an accepted move writes the window back once.
 //  * A slice window is worked by one thread-block cluster of CL CTAs
-//    (CL = 1..16).  Warp 0 of every CTA replays the same Philox stream
-//    (slice, particle, Gaussians, acceptance), so sampled positions and
-//    decisions are identical in every CTA without communication.  Only the
-//    stage action sums cross CTAs: lane r of warp 0 writes this CTA's
-//    (S_old, S_new) partial into CTA r's shared memory (DSMEM) and after one
-//    cluster barrier every CTA adds the partials in rank order — the same
+//    (CL = 1..16).  The sampler warp (the last warp) of every CTA replays the
+//    same Philox stream (slice, particle, Gaussians, acceptance), so sampled
+//    positions and decisions are identical in every CTA without
+//    communication.  Only the stage action sums cross CTAs: warp 0 writes
+//    this CTA's partials into every peer's shared memory (DSMEM) and after
+//    one cluster barrier every CTA adds the partials in rank order — the same
 //    bits everywhere.
 //  * Gaussians come from a warp-parallel polar method that reproduces the
 //    sequential draw order exactly (warp_gaussians); the per-midpoint work
 //    of a level runs one midpoint per lane.
-//  * Partners x links of a stage are split over the cluster's threads; each
-//    item evaluates the pair action for the OLD and the NEW position of the
-//    moved particle against the same partner (partners are identical in
-//    both copies), accumulated in FP64.
+//  * Partners x links of a stage are split over the cluster's threads and
+//    accumulated in FP64.  Partners are identical in the OLD and NEW copies,
+//    so only the moved particle differs; the OLD action of every level is
+//    evaluated in the first stage of a move (the OLD path is fixed for the
+//    whole move) and each stage then evaluates only its NEW action, while
+//    the sampler warp draws the next level speculatively.
 //  * Two schedules.  Sequential: one window at a time, slice1 drawn from the
 //    Local stream exactly as ChooseTimeSlices does (BisectionBlock.cc:362-374).
 //    Concurrent windows: one launch is one round; the round draws an offset o
@@ -130,17 +132,82 @@ __device__ double sample_level_warp(double (*w_old)[3], double (*w_new)[3], doub
 
 }  // namespace
 
+// Pair-action sum of one stage level over this CTA's share of the
+// (partner, link) items, on the window copy `w` (OLD or NEW), plus the
+// moved particle's kinetic links on cluster rank 0.  Returns the sum in the
+// evaluation precision R and, with SHADOW, in the other precision.
+template <int KIND, typename R, bool SHADOW>
+__device__ __forceinline__ double2 level_sum(const BisectionArgs &a, const double (*w)[3],
+                                             const typename Pair2<R>::T *dg, const void *dgs, int lv, int slice1,
+                                             int ptcl, unsigned rank, unsigned CL, int etid, int ethreads) {
+  typedef typename std::conditional<std::is_same<R, double>::value, float, double>::type RS;
+  const DevSystem &sys = a.sys;
+  const int N = sys.N;
+  const int span = 1 << a.num_levels;
+  const int skip = 1 << lv;
+  const int nlinks = span >> lv;
+  double acc = 0.0, acc2 = 0.0;
+  if (rank == 0 && sys.lambda != 0.0) {  // KineticClass::SingleAction on the moved particle
+    const double levelTau = sys.tau * (1 << lv);
+    const double F = 1.0 / (4.0 * sys.lambda * levelTau);
+    for (int k = etid; k < nlinks; k += ethreads) {
+      double v[3];
+      for (int i = 0; i < 3; i++) v[i] = w[k * skip + skip][i] - w[k * skip][i];
+      put_in_box(v, sys);
+      const double kin = kinetic_link(v, F, sys.num_images, sys);
+      acc += kin;
+      acc2 += kin;
+    }
+  }
+  if (lv == 0 || a.sr_higher) {  // ShortRangeClass::SingleAction over partners x links
+    const int np = N - 1;
+    const long long total = (long long)np * nlinks;
+    const long long chunk = (total + CL - 1) / CL;
+    const long long beg = chunk * rank;
+    const long long end = min(total, beg + chunk);
+    const double *path = a.path;
+    for (long long it = beg + etid; it < end; it += ethreads) {
+      const int link = (int)(it / np);
+      const int j = (int)(it - (long long)link * np);
+      const int p2 = j < ptcl ? j : j + 1;
+      const int r0 = link * skip;
+      const double *pa_ = path + ((size_t)(slice1 + r0) * N + p2) * 3;
+      const double *pb_ = path + ((size_t)(slice1 + r0 + skip) * N + p2) * 3;
+      const double a2[3] = {__ldg(pa_), __ldg(pa_ + 1), __ldg(pa_ + 2)};
+      const double b2[3] = {__ldg(pb_), __ldg(pb_ + 1), __ldg(pb_ + 2)};
+      double dA[3], dB[3];
+      dist_disp(w[r0], a2, w[r0 + skip], b2, sys, dA, dB);
+      acc += (double)pa_U<R, KIND>(a.pa, dg, link_geom<R>(dA, dB), lv);
+      if (SHADOW)
+        acc2 += (double)pa_U<RS, KIND>(a.pa, reinterpret_cast<const typename Pair2<RS>::T *>(dgs),
+                                       link_geom<RS>(dA, dB), lv);
+    }
+  }
+  return make_double2(acc, acc2);
+}
+
 // KIND: pair-action type; R: precision of the pair terms; SHADOW: also
 // evaluate the pair terms in the other precision for the dS error.
+//
+// Per move: the sampler warp (the last warp, owner of the RNG stream) picks
+// the particle and samples the top level; the first stage then evaluates the
+// OLD action of every level at once (the OLD path is fixed for the whole
+// move) together with the NEW action of the top level.  While the other
+// warps evaluate stage l, the sampler speculatively samples level l-1 from
+// the stream position that follows stage l's acceptance draw; the draw
+// order is therefore exactly the reference's, and the speculative state is
+// committed only if stage l accepts.
 template <int KIND, typename R, bool SHADOW>
 __global__ void __launch_bounds__(512, 1) bisection_kernel(BisectionArgs a) {
   typedef typename Pair2<R>::T P2;
   typedef typename std::conditional<std::is_same<R, double>::value, float, double>::type RS;  // shadow precision
   typedef typename Pair2<RS>::T P2S;
+  constexpr int NV = 2 * kMaxLevels + 2;  // reduced values: S_old[levels], S_new, and their shadows
   __shared__ double w_old[kMaxWindow][3], w_new[kMaxWindow][3];
   __shared__ double gbuf[3 * 32];
-  __shared__ double sh_red[16][4];
-  __shared__ double xchg[2][kMaxCluster][4];
+  __shared__ double sh_red[16][NV];
+  __shared__ double xchg[2][kMaxCluster][NV];
+  __shared__ double s_logsr[kMaxLevels], s_logu[kMaxLevels], s_sold[kMaxLevels], s_sold2[kMaxLevels];
   __shared__ int s_ctl[4];  // slice1, ptcl, stage accepted, status
   __shared__ __align__(8) uint64_t s_bar;
   extern __shared__ __align__(16) unsigned char dyn[];
@@ -152,12 +219,16 @@ __global__ void __launch_bounds__(512, 1) bisection_kernel(BisectionArgs a) {
   const int tid = threadIdx.x;
   const int lane = tid & 31, warp = tid >> 5;
   const int nwarps = blockDim.x >> 5;
+  const int sampler = nwarps - 1;
+  const int ethreads = (nwarps - 1) * 32;  // evaluating threads: every warp but the sampler
   const DevSystem &sys = a.sys;
   const int N = sys.N;
   const int L = a.num_levels;
   const int span = 1 << L;
   ChainState *cs = a.chains + (a.concurrent ? window : 0);
   const bool lead = (rank == 0 && tid == 0);
+  const int iL = L;                       // slot of S_new
+  const int iS = SHADOW ? L + 1 : 0;      // first shadow slot (S_old shadows, then S_new shadow)
 
   // ---- stage the diagonal DavidPA columns into shared memory (bulk TMA) ----
   // Each level's column is diag_stride pairs long, padded so every level and
@@ -205,7 +276,7 @@ __global__ void __launch_bounds__(512, 1) bisection_kernel(BisectionArgs a) {
     if (SHADOW) diag_smem_s = reinterpret_cast<const P2S *>(dyn + bytes);
   }
 
-  // ---- RNG state: every lane of warp 0 of every CTA holds the same copy ----
+  // ---- RNG state: every lane of the sampler warp of every CTA holds the same copy ----
   DevRandom rng;
   rng.seed = cs->seed;
   rng.n = cs->nlocal;
@@ -238,11 +309,12 @@ __global__ void __launch_bounds__(512, 1) bisection_kernel(BisectionArgs a) {
   if (KIND == PA_DAVID) cluster.sync();  // every CTA has read xchg[1]
   const int numLeft = sys.S - span;
   const int n_blocks = a.concurrent ? 1 : a.n_blocks;
+  if (tid == 0) s_ctl[3] = 0;
 
   for (int blk = 0; blk < n_blocks; blk++) {
     for (int step = 0; step < a.steps_per_block; step++) {
       // ChooseTimeSlices (BisectionBlock.cc:362-374), ChooseParticle (NoPermuteClass.cc:61-68)
-      if (warp == 0) {
+      if (warp == sampler) {
         if (!a.concurrent && step == 0) slice1 = rng.LocalInt(numLeft);
         const int p = rng.LocalInt(N);
         if (lane == 0) {
@@ -258,8 +330,14 @@ __global__ void __launch_bounds__(512, 1) bisection_kernel(BisectionArgs a) {
         for (int i = 0; i < 3; i++) w_old[rel][i] = w_new[rel][i] = p[i];
       }
       __syncthreads();
-      double logsr = 0.0;  // meaningful in warp 0
-      if (warp == 0) logsr = sample_level_warp(w_old, w_new, gbuf, L, L - 1, sys, rng, lane);
+      if (warp == sampler) {
+        const double lsr = sample_level_warp(w_old, w_new, gbuf, L, L - 1, sys, rng, lane);
+        const double lu = log(rng.Local());
+        if (lane == 0) {
+          s_logsr[L - 1] = lsr;
+          s_logu[L - 1] = lu;
+        }
+      }
       __syncthreads();
 
       double prevDS = 0.0, prevDS_s = 0.0;
@@ -274,114 +352,89 @@ __global__ void __launch_bounds__(512, 1) bisection_kernel(BisectionArgs a) {
       int si = 0;
       for (int level = L - 1; level >= 0; level--, si++) {
         // ---- LocalStageClass::Attempt (StageClass.cc:49-95) ----
-        const int skip = 1 << level;
-        const int nlinks = span >> level;
-        double so = 0.0, sn = 0.0, so2 = 0.0, sn2 = 0.0;
-        // Kinetic (KineticClass::SingleAction) on the moved particle, CTA 0 only.
-        if (rank == 0 && tid < nlinks && sys.lambda != 0.0) {
-          const double levelTau = sys.tau * (1 << level);
-          const double F = 1.0 / (4.0 * sys.lambda * levelTau);
-          const int r0 = tid * skip;
-          double vo[3], vn[3];
-          for (int i = 0; i < 3; i++) {
-            vo[i] = w_old[r0 + skip][i] - w_old[r0][i];
-            vn[i] = w_new[r0 + skip][i] - w_new[r0][i];
+        const bool first = (level == L - 1);
+        DevRandom spec = rng;
+        if (warp != sampler) {
+          const P2 *dgb = diag_smem;
+          const P2S *dgsb = diag_smem_s;
+          const size_t st = KIND == PA_DAVID ? (size_t)david_of<R>(a.pa).diag_stride : 0;
+          const size_t sts = (KIND == PA_DAVID && SHADOW) ? (size_t)david_of<RS>(a.pa).diag_stride : 0;
+          if (first)
+            for (int lv = 0; lv < L; lv++) {
+              const double2 v = level_sum<KIND, R, SHADOW>(a, w_old, dgb ? dgb + lv * st : nullptr,
+                                                           dgsb ? dgsb + lv * sts : nullptr, lv, slice1, ptcl, rank,
+                                                           CL, tid, ethreads);
+              const double o1 = warp_sum(v.x);
+              const double o2 = SHADOW ? warp_sum(v.y) : 0.0;
+              if (lane == 0) {
+                sh_red[warp][lv] = o1;
+                if (SHADOW) sh_red[warp][iS + lv] = o2;
+              }
+            }
+          const double2 v = level_sum<KIND, R, SHADOW>(a, w_new, dgb ? dgb + level * st : nullptr,
+                                                       dgsb ? dgsb + level * sts : nullptr, level, slice1, ptcl, rank,
+                                                       CL, tid, ethreads);
+          const double n1 = warp_sum(v.x);
+          const double n2 = SHADOW ? warp_sum(v.y) : 0.0;
+          if (lane == 0) {
+            sh_red[warp][iL] = n1;
+            if (SHADOW) sh_red[warp][iS + L] = n2;
           }
-          put_in_box(vo, sys);
-          put_in_box(vn, sys);
-          const double ko = kinetic_link(vo, F, sys.num_images, sys), kn = kinetic_link(vn, F, sys.num_images, sys);
-          so += ko;
-          sn += kn;
-          if (SHADOW) {
-            so2 += ko;
-            sn2 += kn;
-          }
-        }
-        // ShortRange (ShortRangeClass::SingleAction) over partners x links.
-        if (level == 0 || a.sr_higher) {
-          const int np = N - 1;
-          const long long total = (long long)np * nlinks;
-          const long long chunk = (total + CL - 1) / CL;
-          const long long beg = chunk * rank;
-          const long long end = min(total, beg + chunk);
-          const P2 *dg = nullptr;
-          const P2S *dgs = nullptr;
-          if (KIND == PA_DAVID) {
-            dg = diag_smem + (size_t)level * david_of<R>(a.pa).diag_stride;
-            if (SHADOW) dgs = diag_smem_s + (size_t)level * david_of<RS>(a.pa).diag_stride;
-          }
-          for (long long it = beg + tid; it < end; it += blockDim.x) {
-            const int link = (int)(it / np);
-            const int j = (int)(it - (long long)link * np);
-            const int p2 = j < ptcl ? j : j + 1;
-            const int r0 = link * skip;
-            const double *pa_ = path + ((size_t)(slice1 + r0) * N + p2) * 3;
-            const double *pb_ = path + ((size_t)(slice1 + r0 + skip) * N + p2) * 3;
-            const double a2[3] = {__ldg(pa_), __ldg(pa_ + 1), __ldg(pa_ + 2)};
-            const double b2[3] = {__ldg(pb_), __ldg(pb_ + 1), __ldg(pb_ + 2)};
-            double dAo[3], dBo[3], dAn[3], dBn[3];
-            dist_disp(w_old[r0], a2, w_old[r0 + skip], b2, sys, dAo, dBo);
-            dist_disp(w_new[r0], a2, w_new[r0 + skip], b2, sys, dAn, dBn);
-            const LinkGeom<R> go = link_geom<R>(dAo, dBo);
-            const LinkGeom<R> gn = link_geom<R>(dAn, dBn);
-            so += (double)pa_U<R, KIND>(a.pa, dg, go, level);
-            sn += (double)pa_U<R, KIND>(a.pa, dg, gn, level);
-            if (SHADOW) {
-              so2 += (double)pa_U<RS, KIND>(a.pa, dgs, link_geom<RS>(dAo, dBo), level);
-              sn2 += (double)pa_U<RS, KIND>(a.pa, dgs, link_geom<RS>(dAn, dBn), level);
+        } else {
+          // speculative sampling of the next level (BisectionStage::Sample of stage level-1)
+          if (level > 0) {
+            const double lsr = sample_level_warp(w_old, w_new, gbuf, L, level - 1, sys, spec, lane);
+            const double lu = log(spec.Local());
+            if (lane == 0) {
+              s_logsr[level - 1] = lsr;
+              s_logu[level - 1] = lu;
             }
           }
-          if (lead) pair_evals += 2ull * (unsigned long long)total;
+          if (lane < NV) sh_red[warp][lane] = 0.0;
         }
-        // ---- reduce: warps -> CTA (warp 0) -> cluster (DSMEM, rank order) ----
-        so = warp_sum(so);
-        sn = warp_sum(sn);
-        if (SHADOW) {
-          so2 = warp_sum(so2);
-          sn2 = warp_sum(sn2);
-        }
-        if (lane == 0) {
-          sh_red[warp][0] = so;
-          sh_red[warp][1] = sn;
-          sh_red[warp][2] = so2;
-          sh_red[warp][3] = sn2;
-        }
+        // Counted as the reference performs them: OLD + NEW of the stage's
+        // links; the OLD terms of later levels evaluated ahead are not counted.
+        if (lead && (level == 0 || a.sr_higher)) pair_evals += 2ull * (unsigned long long)(N - 1) * (span >> level);
         __syncthreads();
+        // ---- reduce: warps -> CTA (warp 0) -> cluster (DSMEM, rank order) ----
         const int par = xc & 1;
         xc++;
+        const int nv = first ? (SHADOW ? 2 * L + 2 : L + 1) : 0;
         if (warp == 0) {
-          double v[4] = {0.0, 0.0, 0.0, 0.0};
-          for (int w = 0; w < nwarps; w++)
-            for (int c = 0; c < 4; c++) v[c] += sh_red[w][c];
-          so = v[0];
-          sn = v[1];
-          so2 = v[2];
-          sn2 = v[3];
-          if (CL > 1 && lane < (int)CL) {
-            double *dst = cluster.map_shared_rank(&xchg[par][rank][0], lane);
-            dst[0] = so;
-            dst[1] = sn;
-            dst[2] = so2;
-            dst[3] = sn2;
+          // slots that carry data this stage: all on the first stage, else S_new (+ shadow)
+          double v = 0.0;
+          const int slot = lane < nv ? lane : (lane == 0 ? iL : (SHADOW && lane == 1 ? iS + L : -1));
+          if (slot >= 0)
+            for (int w = 0; w < nwarps; w++) v += sh_red[w][slot];
+          if (CL > 1) {
+            if (slot >= 0)
+              for (unsigned r = 0; r < CL; r++) cluster.map_shared_rank(&xchg[par][rank][0], r)[slot] = v;
+          } else if (slot >= 0) {
+            xchg[par][0][slot] = v;
           }
         }
-        if (CL > 1) {
+        if (CL > 1)
           cluster.sync();
-          if (warp == 0) {
-            so = sn = so2 = sn2 = 0.0;
-            for (unsigned r = 0; r < CL; r++) {
-              so += xchg[par][r][0];
-              sn += xchg[par][r][1];
-              so2 += xchg[par][r][2];
-              sn2 += xchg[par][r][3];
-            }
-          }
-        }
-        // ---- Metropolis test (identical in every CTA), then sample the next level ----
+        else
+          __syncwarp();
         if (warp == 0) {
+          const int slot = lane < nv ? lane : (lane == 0 ? iL : (SHADOW && lane == 1 ? iS + L : -1));
+          double v = 0.0;
+          if (slot >= 0)
+            for (unsigned r = 0; r < CL; r++) v += xchg[par][r][slot];
+          if (first) {
+            if (lane < L) s_sold[lane] = v;
+            if (SHADOW && lane >= iS && lane < iS + L) s_sold2[lane - iS] = v;
+          }
+          const double sn = __shfl_sync(0xffffffffu, v, first ? iL : 0);
+          const double sn2 = SHADOW ? __shfl_sync(0xffffffffu, v, first ? iS + L : 1) : 0.0;
+          __syncwarp();
+          // ---- Metropolis test, identical in every CTA ----
+          const double so = s_sold[level];
           const double currActionChange = sn - so;
+          const double logsr = s_logsr[level];
           const double logAcceptProb = logsr - currActionChange + prevDS;
-          const double logu = log(rng.Local());
+          const double logu = s_logu[level];
           bool toAccept = logAcceptProb >= logu;
           if (toAccept && (fabs(sn) > 1e50 || fabs(so) > 1e50)) {  // StageClass.cc:74-85
             toAccept = false;
@@ -389,18 +442,14 @@ __global__ void __launch_bounds__(512, 1) bisection_kernel(BisectionArgs a) {
           }
           if (!isfinite(currActionChange)) status = PIMC_E_NAN;
           if (SHADOW) {
-            const double dss = sn2 - so2;
+            const double dss = sn2 - s_sold2[level];
             const bool other = (logsr - dss + prevDS_s) >= logu;
             if (other != toAccept && lead) flips++;
             prevDS_s = dss;
+            if (lead && si < 8) rec.dS_shadow[si] = dss;
           }
           prevDS = currActionChange;
-          if (lead && si < 8) {
-            rec.dS[si] = currActionChange;
-            if (SHADOW) rec.dS_shadow[si] = sn2 - so2;
-          }
-          if (toAccept && level > 0 && status == 0)
-            logsr = sample_level_warp(w_old, w_new, gbuf, L, level - 1, sys, rng, lane);
+          if (lead && si < 8) rec.dS[si] = currActionChange;
           if (lane == 0) {
             s_ctl[2] = toAccept ? 1 : 0;
             s_ctl[3] = status;
@@ -412,6 +461,7 @@ __global__ void __launch_bounds__(512, 1) bisection_kernel(BisectionArgs a) {
           acc_all = false;
           break;
         }
+        if (warp == sampler) rng = spec;  // commit the speculative draws of the next level
         passed++;
       }
       // ---- AcceptCopy (PathClass.cc:797-863); a rejected move left HBM untouched ----
@@ -445,10 +495,12 @@ __global__ void __launch_bounds__(512, 1) bisection_kernel(BisectionArgs a) {
     }
     if (s_ctl[3] != 0) break;
   }
-  if (lead) {
+  if (warp == sampler && lane == 0 && rank == 0) {
     cs->nlocal = rng.n;
     cs->one_left = rng.one_left;
     cs->x2 = rng.x2;
+  }
+  if (lead) {
     cs->moves += moves;
     cs->accepted += accepted;
     cs->stages += stages;
