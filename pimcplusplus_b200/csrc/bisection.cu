@@ -18,10 +18,9 @@
 //    of a level runs one midpoint per lane.
 //  * Partners x links of a stage are split over the cluster's threads and
 //    accumulated in FP64.  Partners are identical in the OLD and NEW copies,
-//    so only the moved particle differs; the OLD action of every level is
-//    evaluated in the first stage of a move (the OLD path is fixed for the
-//    whole move) and each stage then evaluates only its NEW action, while
-//    the sampler warp draws the next level speculatively.
+//    so each item reads its partner once and evaluates the pair action for
+//    the OLD and the NEW position of the moved particle, while the sampler
+//    warp draws the next level speculatively.
 //  * Two schedules.  Sequential: one window at a time, slice1 drawn from the
 //    Local stream exactly as ChooseTimeSlices does (BisectionBlock.cc:362-374).
 //    Concurrent windows: one launch is one round; the round draws an offset o
@@ -132,82 +131,92 @@ __device__ double sample_level_warp(double (*w_old)[3], double (*w_new)[3], doub
 
 }  // namespace
 
-// Pair-action sum of one stage level over this CTA's share of the
-// (partner, link) items, on the window copy `w` (OLD or NEW), plus the
-// moved particle's kinetic links on cluster rank 0.  Returns the sum in the
-// evaluation precision R and, with SHADOW, in the other precision.
+// OLD and NEW action sums of one stage level over this CTA's share of the
+// (partner, link) items, plus the moved particle's kinetic links on cluster
+// rank 0.  Partner positions are read once and serve both copies.  Returns
+// (S_old, S_new) in the evaluation precision R and, with SHADOW, the same in
+// the other precision.
 template <int KIND, typename R, bool SHADOW>
-__device__ __forceinline__ double2 level_sum(const BisectionArgs &a, const double (*w)[3],
-                                             const typename Pair2<R>::T *dg, const void *dgs, int lv, int slice1,
-                                             int ptcl, unsigned rank, unsigned CL, int etid, int ethreads) {
+__device__ __forceinline__ double4 stage_sums(const BisectionArgs &a, const double (*w_old)[3],
+                                              const double (*w_new)[3], const typename Pair2<R>::T *dg,
+                                              const void *dgs, int lv, int slice1, int ptcl, unsigned rank,
+                                              unsigned CL, int etid, int ethreads) {
   typedef typename std::conditional<std::is_same<R, double>::value, float, double>::type RS;
+  typedef typename Pair2<RS>::T P2S;
   const DevSystem &sys = a.sys;
   const int N = sys.N;
   const int span = 1 << a.num_levels;
   const int skip = 1 << lv;
   const int nlinks = span >> lv;
-  double acc = 0.0, acc2 = 0.0;
+  double so = 0.0, sn = 0.0, so2 = 0.0, sn2 = 0.0;
   if (rank == 0 && sys.lambda != 0.0) {  // KineticClass::SingleAction on the moved particle
     const double levelTau = sys.tau * (1 << lv);
     const double F = 1.0 / (4.0 * sys.lambda * levelTau);
     for (int k = etid; k < nlinks; k += ethreads) {
-      double v[3];
-      for (int i = 0; i < 3; i++) v[i] = w[k * skip + skip][i] - w[k * skip][i];
-      put_in_box(v, sys);
-      const double kin = kinetic_link(v, F, sys.num_images, sys);
-      acc += kin;
-      acc2 += kin;
+      double vo[3], vn[3];
+      for (int i = 0; i < 3; i++) {
+        vo[i] = w_old[k * skip + skip][i] - w_old[k * skip][i];
+        vn[i] = w_new[k * skip + skip][i] - w_new[k * skip][i];
+      }
+      put_in_box(vo, sys);
+      put_in_box(vn, sys);
+      const double ko = kinetic_link(vo, F, sys.num_images, sys), kn = kinetic_link(vn, F, sys.num_images, sys);
+      so += ko;
+      sn += kn;
+      so2 += ko;
+      sn2 += kn;
     }
   }
   if (lv == 0 || a.sr_higher) {  // ShortRangeClass::SingleAction over partners x links
     const int np = N - 1;
-    const long long total = (long long)np * nlinks;
-    const long long chunk = (total + CL - 1) / CL;
-    const long long beg = chunk * rank;
-    const long long end = min(total, beg + chunk);
+    const int total = np * nlinks;  // < 2^31: N <= 2^20, 2^L <= 64 (host-checked)
+    const int chunk = (total + (int)CL - 1) / (int)CL;
+    const int beg = chunk * (int)rank;
+    const int end = min(total, beg + chunk);
     const double *path = a.path;
-    for (long long it = beg + etid; it < end; it += ethreads) {
-      const int link = (int)(it / np);
-      const int j = (int)(it - (long long)link * np);
+    for (int it = beg + etid; it < end; it += ethreads) {
+      const int link = it / np;
+      const int j = it - link * np;
       const int p2 = j < ptcl ? j : j + 1;
       const int r0 = link * skip;
       const double *pa_ = path + ((size_t)(slice1 + r0) * N + p2) * 3;
       const double *pb_ = path + ((size_t)(slice1 + r0 + skip) * N + p2) * 3;
       const double a2[3] = {__ldg(pa_), __ldg(pa_ + 1), __ldg(pa_ + 2)};
       const double b2[3] = {__ldg(pb_), __ldg(pb_ + 1), __ldg(pb_ + 2)};
-      double dA[3], dB[3];
-      dist_disp(w[r0], a2, w[r0 + skip], b2, sys, dA, dB);
-      acc += (double)pa_U<R, KIND>(a.pa, dg, link_geom<R>(dA, dB), lv);
-      if (SHADOW)
-        acc2 += (double)pa_U<RS, KIND>(a.pa, reinterpret_cast<const typename Pair2<RS>::T *>(dgs),
-                                       link_geom<RS>(dA, dB), lv);
+      double dAo[3], dBo[3], dAn[3], dBn[3];
+      dist_disp(w_old[r0], a2, w_old[r0 + skip], b2, sys, dAo, dBo);
+      dist_disp(w_new[r0], a2, w_new[r0 + skip], b2, sys, dAn, dBn);
+      so += (double)pa_U<R, KIND>(a.pa, dg, link_geom<R>(dAo, dBo), lv);
+      sn += (double)pa_U<R, KIND>(a.pa, dg, link_geom<R>(dAn, dBn), lv);
+      if (SHADOW) {
+        const P2S *d2 = reinterpret_cast<const P2S *>(dgs);
+        so2 += (double)pa_U<RS, KIND>(a.pa, d2, link_geom<RS>(dAo, dBo), lv);
+        sn2 += (double)pa_U<RS, KIND>(a.pa, d2, link_geom<RS>(dAn, dBn), lv);
+      }
     }
   }
-  return make_double2(acc, acc2);
+  return make_double4(so, sn, so2, sn2);
 }
 
 // KIND: pair-action type; R: precision of the pair terms; SHADOW: also
 // evaluate the pair terms in the other precision for the dS error.
 //
 // Per move: the sampler warp (the last warp, owner of the RNG stream) picks
-// the particle and samples the top level; the first stage then evaluates the
-// OLD action of every level at once (the OLD path is fixed for the whole
-// move) together with the NEW action of the top level.  While the other
-// warps evaluate stage l, the sampler speculatively samples level l-1 from
-// the stream position that follows stage l's acceptance draw; the draw
-// order is therefore exactly the reference's, and the speculative state is
-// committed only if stage l accepts.
+// the particle and samples the top level.  While the other warps evaluate
+// the OLD and NEW action of stage l, the sampler speculatively samples level
+// l-1 from the stream position that follows stage l's acceptance draw; the
+// draw order is therefore exactly the reference's, and the speculative
+// state is committed only if stage l accepts.
 template <int KIND, typename R, bool SHADOW>
 __global__ void __launch_bounds__(512, 1) bisection_kernel(BisectionArgs a) {
   typedef typename Pair2<R>::T P2;
   typedef typename std::conditional<std::is_same<R, double>::value, float, double>::type RS;  // shadow precision
   typedef typename Pair2<RS>::T P2S;
-  constexpr int NV = 2 * kMaxLevels + 2;  // reduced values: S_old[levels], S_new, and their shadows
   __shared__ double w_old[kMaxWindow][3], w_new[kMaxWindow][3];
   __shared__ double gbuf[3 * 32];
-  __shared__ double sh_red[16][NV];
-  __shared__ double xchg[2][kMaxCluster][NV];
-  __shared__ double s_logsr[kMaxLevels], s_logu[kMaxLevels], s_sold[kMaxLevels], s_sold2[kMaxLevels];
+  __shared__ double sh_red[16][4];  // per warp: S_old, S_new, and their shadows
+  __shared__ double xchg[2][kMaxCluster][4];
+  __shared__ double s_logsr[kMaxLevels], s_logu[kMaxLevels];
   __shared__ int s_ctl[4];  // slice1, ptcl, stage accepted, status
   __shared__ __align__(8) uint64_t s_bar;
   extern __shared__ __align__(16) unsigned char dyn[];
@@ -227,8 +236,6 @@ __global__ void __launch_bounds__(512, 1) bisection_kernel(BisectionArgs a) {
   const int span = 1 << L;
   ChainState *cs = a.chains + (a.concurrent ? window : 0);
   const bool lead = (rank == 0 && tid == 0);
-  const int iL = L;                       // slot of S_new
-  const int iS = SHADOW ? L + 1 : 0;      // first shadow slot (S_old shadows, then S_new shadow)
 
   // ---- stage the diagonal DavidPA columns into shared memory (bulk TMA) ----
   // Each level's column is diag_stride pairs long, padded so every level and
@@ -352,33 +359,20 @@ __global__ void __launch_bounds__(512, 1) bisection_kernel(BisectionArgs a) {
       int si = 0;
       for (int level = L - 1; level >= 0; level--, si++) {
         // ---- LocalStageClass::Attempt (StageClass.cc:49-95) ----
-        const bool first = (level == L - 1);
         DevRandom spec = rng;
         if (warp != sampler) {
-          const P2 *dgb = diag_smem;
-          const P2S *dgsb = diag_smem_s;
           const size_t st = KIND == PA_DAVID ? (size_t)david_of<R>(a.pa).diag_stride : 0;
           const size_t sts = (KIND == PA_DAVID && SHADOW) ? (size_t)david_of<RS>(a.pa).diag_stride : 0;
-          if (first)
-            for (int lv = 0; lv < L; lv++) {
-              const double2 v = level_sum<KIND, R, SHADOW>(a, w_old, dgb ? dgb + lv * st : nullptr,
-                                                           dgsb ? dgsb + lv * sts : nullptr, lv, slice1, ptcl, rank,
-                                                           CL, tid, ethreads);
-              const double o1 = warp_sum(v.x);
-              const double o2 = SHADOW ? warp_sum(v.y) : 0.0;
-              if (lane == 0) {
-                sh_red[warp][lv] = o1;
-                if (SHADOW) sh_red[warp][iS + lv] = o2;
-              }
-            }
-          const double2 v = level_sum<KIND, R, SHADOW>(a, w_new, dgb ? dgb + level * st : nullptr,
-                                                       dgsb ? dgsb + level * sts : nullptr, level, slice1, ptcl, rank,
-                                                       CL, tid, ethreads);
-          const double n1 = warp_sum(v.x);
-          const double n2 = SHADOW ? warp_sum(v.y) : 0.0;
+          const double4 v = stage_sums<KIND, R, SHADOW>(a, w_old, w_new, diag_smem ? diag_smem + level * st : nullptr,
+                                                        diag_smem_s ? diag_smem_s + level * sts : nullptr, level,
+                                                        slice1, ptcl, rank, CL, tid, ethreads);
+          const double o1 = warp_sum(v.x), n1 = warp_sum(v.y);
+          const double o2 = SHADOW ? warp_sum(v.z) : 0.0, n2 = SHADOW ? warp_sum(v.w) : 0.0;
           if (lane == 0) {
-            sh_red[warp][iL] = n1;
-            if (SHADOW) sh_red[warp][iS + L] = n2;
+            sh_red[warp][0] = o1;
+            sh_red[warp][1] = n1;
+            sh_red[warp][2] = o2;
+            sh_red[warp][3] = n2;
           }
         } else {
           // speculative sampling of the next level (BisectionStage::Sample of stage level-1)
@@ -390,7 +384,7 @@ __global__ void __launch_bounds__(512, 1) bisection_kernel(BisectionArgs a) {
               s_logu[level - 1] = lu;
             }
           }
-          if (lane < NV) sh_red[warp][lane] = 0.0;
+          if (lane < 4) sh_red[warp][lane] = 0.0;
         }
         // Counted as the reference performs them: OLD + NEW of the stage's
         // links; the OLD terms of later levels evaluated ahead are not counted.
@@ -399,38 +393,27 @@ __global__ void __launch_bounds__(512, 1) bisection_kernel(BisectionArgs a) {
         // ---- reduce: warps -> CTA (warp 0) -> cluster (DSMEM, rank order) ----
         const int par = xc & 1;
         xc++;
-        const int nv = first ? (SHADOW ? 2 * L + 2 : L + 1) : 0;
-        if (warp == 0) {
-          // slots that carry data this stage: all on the first stage, else S_new (+ shadow)
+        if (warp == 0 && lane < 4) {
           double v = 0.0;
-          const int slot = lane < nv ? lane : (lane == 0 ? iL : (SHADOW && lane == 1 ? iS + L : -1));
-          if (slot >= 0)
-            for (int w = 0; w < nwarps; w++) v += sh_red[w][slot];
-          if (CL > 1) {
-            if (slot >= 0)
-              for (unsigned r = 0; r < CL; r++) cluster.map_shared_rank(&xchg[par][rank][0], r)[slot] = v;
-          } else if (slot >= 0) {
-            xchg[par][0][slot] = v;
-          }
+          for (int w = 0; w < nwarps; w++) v += sh_red[w][lane];
+          if (CL > 1)
+            for (unsigned r = 0; r < CL; r++) cluster.map_shared_rank(&xchg[par][rank][0], r)[lane] = v;
+          else
+            xchg[par][0][lane] = v;
         }
         if (CL > 1)
           cluster.sync();
         else
           __syncwarp();
         if (warp == 0) {
-          const int slot = lane < nv ? lane : (lane == 0 ? iL : (SHADOW && lane == 1 ? iS + L : -1));
           double v = 0.0;
-          if (slot >= 0)
-            for (unsigned r = 0; r < CL; r++) v += xchg[par][r][slot];
-          if (first) {
-            if (lane < L) s_sold[lane] = v;
-            if (SHADOW && lane >= iS && lane < iS + L) s_sold2[lane - iS] = v;
-          }
-          const double sn = __shfl_sync(0xffffffffu, v, first ? iL : 0);
-          const double sn2 = SHADOW ? __shfl_sync(0xffffffffu, v, first ? iS + L : 1) : 0.0;
-          __syncwarp();
+          if (lane < 4)
+            for (unsigned r = 0; r < CL; r++) v += xchg[par][r][lane];
+          const double so = __shfl_sync(0xffffffffu, v, 0);
+          const double sn = __shfl_sync(0xffffffffu, v, 1);
+          const double so2 = __shfl_sync(0xffffffffu, v, 2);
+          const double sn2 = __shfl_sync(0xffffffffu, v, 3);
           // ---- Metropolis test, identical in every CTA ----
-          const double so = s_sold[level];
           const double currActionChange = sn - so;
           const double logsr = s_logsr[level];
           const double logAcceptProb = logsr - currActionChange + prevDS;
@@ -442,7 +425,7 @@ __global__ void __launch_bounds__(512, 1) bisection_kernel(BisectionArgs a) {
           }
           if (!isfinite(currActionChange)) status = PIMC_E_NAN;
           if (SHADOW) {
-            const double dss = sn2 - s_sold2[level];
+            const double dss = sn2 - so2;
             const bool other = (logsr - dss + prevDS_s) >= logu;
             if (other != toAccept && lead) flips++;
             prevDS_s = dss;

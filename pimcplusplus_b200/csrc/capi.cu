@@ -495,6 +495,7 @@ int pimc_bisection_setup(pimc_context *ctx, const pimc_bisection_desc *d) {
   if (d->num_levels < 1 || d->num_levels > 6) return fail(ctx, PIMC_E_ARG, "NumLevels must be 1..6");
   if ((1 << d->num_levels) >= ctx->sys.S) return fail(ctx, PIMC_E_ARG, "not enough slices for NumLevels");
   if (d->steps_per_block < 1) return fail(ctx, PIMC_E_ARG, "StepsPerBlock must be >= 1");
+  if (ctx->sys.N > (1 << 20)) return fail(ctx, PIMC_E_ARG, "device moves support up to 2^20 particles");
   if (d->precision != PIMC_FP64 && d->precision != PIMC_MIXED) return fail(ctx, PIMC_E_ARG, "bad precision");
   if (d->cluster_ctas < 0 || d->cluster_ctas > kMaxCluster) return fail(ctx, PIMC_E_ARG, "cluster_ctas 0..16");
   if (d->threads_per_cta != 0 && (d->threads_per_cta < 64 || d->threads_per_cta > 512 || d->threads_per_cta % 32))
