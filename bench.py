@@ -252,6 +252,9 @@ def run_ours(args):
     blocks = blocks_for(args.schedule)
 
     flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=f"cuda:{local}")
+    _d, _bb = make(P.MIXED)
+    occupancy = _bb.occupancy()
+    _d.close()
 
     def timed(precision, schedule=None, steps=None):
         steps = steps or args.steps
@@ -366,6 +369,7 @@ def run_ours(args):
             "config": {"workload": W_NAME, "moves_per_step": st32["moves"] // world // args.steps,
                        "schedule": args.schedule, "steps_per_block": args.steps_per_block,
                        "cluster_ctas": args.cluster, "threads_per_cta": args.threads,
+                       "resident_clusters": occupancy, "windows": (slices - 1) >> L,
                        "l2": "flushed between steps by a 256 MiB write outside the timed events",
                        "parallelism": f"replicas x{world}"},
             "moves_per_s": st32["moves"] / (ms32 / 1000.0),

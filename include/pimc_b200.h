@@ -220,6 +220,9 @@ int pimc_run_bisection(pimc_context *ctx, int n_blocks, pimc_move_record *trace,
  * copying anything back (for timing); pimc_bisection_stats reads the totals. */
 int pimc_run_bisection_async(pimc_context *ctx, int n_blocks);
 int pimc_bisection_get_stats(pimc_context *ctx, pimc_bisection_stats *stats);
+/* Clusters of the configured shape that can be resident at once (window
+ * clusters beyond this run in a second wave). */
+int pimc_bisection_occupancy(pimc_context *ctx, int *max_active_clusters);
 int pimc_synchronize(pimc_context *ctx);
 /* The CUDA stream of the context (cudaStream_t as void*). */
 void *pimc_stream(pimc_context *ctx);

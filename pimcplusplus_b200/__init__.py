@@ -127,6 +127,7 @@ _SIGS = {
     "pimc_run_bisection": (_i, [_p, _i, _p, C.POINTER(BisectionStats)]),
     "pimc_run_bisection_async": (_i, [_p, _i]),
     "pimc_bisection_get_stats": (_i, [_p, C.POINTER(BisectionStats)]),
+    "pimc_bisection_occupancy": (_i, [_p, _ip]),
     "pimc_synchronize": (_i, [_p]),
     "pimc_stream": (_p, [_p]),
 }
@@ -354,6 +355,12 @@ class BisectionBlock:
 
     def launch_async(self, n_blocks):
         self.PathData._check(_lib.pimc_run_bisection_async(self.PathData.h, n_blocks), "run_bisection_async")
+
+    def occupancy(self):
+        """Clusters of this launch shape that fit on the device at once."""
+        v = C.c_int()
+        self.PathData._check(_lib.pimc_bisection_occupancy(self.PathData.h, C.byref(v)), "occupancy")
+        return v.value
 
     def stats(self):
         st = BisectionStats()

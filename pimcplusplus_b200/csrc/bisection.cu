@@ -518,6 +518,45 @@ static cudaError_t launch_t(const BisectionArgs &a, int cl, int clusters, int th
   return cudaLaunchKernelEx(&cfg, kfn, a);
 }
 
+template <int KIND, typename R, bool SHADOW>
+static cudaError_t occupancy_t(int cl, int threads, size_t dyn, int *max_clusters) {
+  auto kfn = bisection_kernel<KIND, R, SHADOW>;
+  cudaError_t e = cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn);
+  if (e != cudaSuccess) return e;
+  if (cl > 8) {
+    e = cudaFuncSetAttribute(kfn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+    if (e != cudaSuccess) return e;
+  }
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(cl, 1, 1);
+  cfg.blockDim = dim3(threads, 1, 1);
+  cfg.dynamicSmemBytes = dyn;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = cl;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaOccupancyMaxActiveClusters(max_clusters, kfn, &cfg);
+}
+
+cudaError_t bisection_occupancy(const BisectionArgs &a, int precision, int shadow, int cl, int threads,
+                                int *max_clusters) {
+  const size_t dyn = bisection_dyn_smem(a, precision, shadow);
+  const bool mixed = precision == PIMC_MIXED;
+  if (a.pa.kind == PA_DAVID) {
+    if (mixed) return shadow ? occupancy_t<PA_DAVID, float, true>(cl, threads, dyn, max_clusters)
+                             : occupancy_t<PA_DAVID, float, false>(cl, threads, dyn, max_clusters);
+    return shadow ? occupancy_t<PA_DAVID, double, true>(cl, threads, dyn, max_clusters)
+                  : occupancy_t<PA_DAVID, double, false>(cl, threads, dyn, max_clusters);
+  }
+  if (mixed) return shadow ? occupancy_t<PA_TRICUBIC, float, true>(cl, threads, dyn, max_clusters)
+                           : occupancy_t<PA_TRICUBIC, float, false>(cl, threads, dyn, max_clusters);
+  return shadow ? occupancy_t<PA_TRICUBIC, double, true>(cl, threads, dyn, max_clusters)
+                : occupancy_t<PA_TRICUBIC, double, false>(cl, threads, dyn, max_clusters);
+}
+
 size_t bisection_dyn_smem(const BisectionArgs &a, int precision, int shadow) {
   if (a.pa.kind != PA_DAVID) return 0;
   const size_t b64 = (size_t)a.num_levels * a.pa.d64.diag_stride * sizeof(double2);

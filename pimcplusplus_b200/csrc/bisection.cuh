@@ -19,6 +19,8 @@ struct BisectionArgs {
   unsigned long long round;   // Common-stream index of this round (concurrent)
 };
 
+cudaError_t bisection_occupancy(const BisectionArgs &a, int precision, int shadow, int cluster_ctas, int threads,
+                                int *max_clusters);
 size_t bisection_dyn_smem(const BisectionArgs &a, int precision, int shadow);
 cudaError_t launch_bisection(const BisectionArgs &a, int precision, int shadow, int cluster_ctas, int clusters,
                              int threads, cudaStream_t st);

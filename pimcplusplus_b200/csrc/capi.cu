@@ -638,6 +638,18 @@ int pimc_bisection_get_stats(pimc_context *ctx, pimc_bisection_stats *stats) {
   return PIMC_OK;
 }
 
+int pimc_bisection_occupancy(pimc_context *ctx, int *max_active_clusters) {
+  if (!ctx || !max_active_clusters) return PIMC_E_ARG;
+  if (!ctx->bis_ready) return fail(ctx, PIMC_E_STATE, "pimc_bisection_setup not called");
+  CK(cudaSetDevice(ctx->device));
+  BisectionArgs a{};
+  a.pa = ctx->pa;
+  a.num_levels = ctx->bis.num_levels;
+  CK(bisection_occupancy(a, ctx->bis.precision, ctx->bis.shadow, ctx->bis.cluster_ctas, ctx->bis.threads_per_cta,
+                         max_active_clusters));
+  return PIMC_OK;
+}
+
 int pimc_synchronize(pimc_context *ctx) {
   if (!ctx) return PIMC_E_ARG;
   CK(cudaSetDevice(ctx->device));
