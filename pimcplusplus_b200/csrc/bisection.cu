@@ -107,20 +107,35 @@ __device__ double sample_level_warp(double (*w_old)[3], double (*w_new)[3], doub
     for (int i = 0; i < 3; i++) rbar[i] = w_new[rel][i] + 0.5 * rdiff[i];
     for (int i = 0; i < 3; i++) Delta[i] = gbuf[3 * lane + i] * sigma;
     put_in_box(Delta, s);
-    double GaussProd = 1.0, GaussProdOld = 1.0;
+    // log of the image-summed Gaussian transition densities (BisectionStage.cc:241-256).
+    // Without images, log(prod_d exp(-x_d)) = -sum_d x_d up to rounding while no
+    // factor underflows; otherwise the reference's product is formed.
+    bool direct = s.num_images == 0;
+    double eo[3], en[3];
     for (int dim = 0; dim < 3; dim++) {
-      double GaussSum = 0.0, GaussSumOld = 0.0;
-      for (int image = -s.num_images; image <= s.num_images; image++) {
-        double dist = Delta[dim] + (double)image * s.box[dim];
-        double distOld = DeltaOld[dim] + (double)image * s.box[dim];
-        GaussSum += exp(-0.5 * dist * dist / sigma2);
-        GaussSumOld += exp(-0.5 * distOld * distOld / sigma2);
-      }
-      GaussProd *= GaussSum;
-      GaussProdOld *= GaussSumOld;
+      en[dim] = 0.5 * Delta[dim] * Delta[dim] / sigma2;
+      eo[dim] = 0.5 * DeltaOld[dim] * DeltaOld[dim] / sigma2;
+      direct = direct && en[dim] < 700.0 && eo[dim] < 700.0;
     }
-    lo = log(GaussProdOld);
-    ln = log(GaussProd);
+    if (direct) {
+      lo = -(eo[0] + eo[1] + eo[2]);
+      ln = -(en[0] + en[1] + en[2]);
+    } else {
+      double GaussProd = 1.0, GaussProdOld = 1.0;
+      for (int dim = 0; dim < 3; dim++) {
+        double GaussSum = 0.0, GaussSumOld = 0.0;
+        for (int image = -s.num_images; image <= s.num_images; image++) {
+          double dist = Delta[dim] + (double)image * s.box[dim];
+          double distOld = DeltaOld[dim] + (double)image * s.box[dim];
+          GaussSum += exp(-0.5 * dist * dist / sigma2);
+          GaussSumOld += exp(-0.5 * distOld * distOld / sigma2);
+        }
+        GaussProd *= GaussSum;
+        GaussProdOld *= GaussSumOld;
+      }
+      lo = log(GaussProdOld);
+      ln = log(GaussProd);
+    }
     for (int i = 0; i < 3; i++) w_new[mid][i] = rbar[i] + Delta[i];
   }
   lo = warp_sum(lo);
@@ -174,24 +189,41 @@ __device__ __forceinline__ double4 stage_sums(const BisectionArgs &a, const doub
     const int beg = chunk * (int)rank;
     const int end = min(total, beg + chunk);
     const double *path = a.path;
-    for (int it = beg + etid; it < end; it += ethreads) {
-      const int link = it / np;
-      const int j = it - link * np;
-      const int p2 = j < ptcl ? j : j + 1;
-      const int r0 = link * skip;
-      const double *pa_ = path + ((size_t)(slice1 + r0) * N + p2) * 3;
-      const double *pb_ = path + ((size_t)(slice1 + r0 + skip) * N + p2) * 3;
-      const double a2[3] = {__ldg(pa_), __ldg(pa_ + 1), __ldg(pa_ + 2)};
-      const double b2[3] = {__ldg(pb_), __ldg(pb_ + 1), __ldg(pb_ + 2)};
-      double dAo[3], dBo[3], dAn[3], dBn[3];
-      dist_disp(w_old[r0], a2, w_old[r0 + skip], b2, sys, dAo, dBo);
-      dist_disp(w_new[r0], a2, w_new[r0 + skip], b2, sys, dAn, dBn);
-      so += (double)pa_U<R, KIND>(a.pa, dg, link_geom<R>(dAo, dBo), lv);
-      sn += (double)pa_U<R, KIND>(a.pa, dg, link_geom<R>(dAn, dBn), lv);
-      if (SHADOW) {
-        const P2S *d2 = reinterpret_cast<const P2S *>(dgs);
-        so2 += (double)pa_U<RS, KIND>(a.pa, d2, link_geom<RS>(dAo, dBo), lv);
-        sn2 += (double)pa_U<RS, KIND>(a.pa, d2, link_geom<RS>(dAn, dBn), lv);
+    // Two items per pass so a thread's partner and table loads overlap.
+    for (int it0 = beg + etid; it0 < end; it0 += 2 * ethreads) {
+      double a2[2][3], b2[2][3];
+      int r0s[2];
+      bool live[2];
+#pragma unroll
+      for (int u = 0; u < 2; u++) {
+        const int it = it0 + u * ethreads;
+        live[u] = it < end;
+        const int itc = live[u] ? it : it0;
+        const int link = itc / np;
+        const int j = itc - link * np;
+        const int p2 = j < ptcl ? j : j + 1;
+        r0s[u] = link * skip;
+        const double *pa_ = path + ((size_t)(slice1 + r0s[u]) * N + p2) * 3;
+        const double *pb_ = path + ((size_t)(slice1 + r0s[u] + skip) * N + p2) * 3;
+        for (int i = 0; i < 3; i++) {
+          a2[u][i] = __ldg(pa_ + i);
+          b2[u][i] = __ldg(pb_ + i);
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < 2; u++) {
+        if (!live[u]) continue;
+        const int r0 = r0s[u];
+        double dAo[3], dBo[3], dAn[3], dBn[3];
+        dist_disp(w_old[r0], a2[u], w_old[r0 + skip], b2[u], sys, dAo, dBo);
+        dist_disp(w_new[r0], a2[u], w_new[r0 + skip], b2[u], sys, dAn, dBn);
+        so += (double)pa_U<R, KIND>(a.pa, dg, link_geom<R>(dAo, dBo), lv);
+        sn += (double)pa_U<R, KIND>(a.pa, dg, link_geom<R>(dAn, dBn), lv);
+        if (SHADOW) {
+          const P2S *d2 = reinterpret_cast<const P2S *>(dgs);
+          so2 += (double)pa_U<RS, KIND>(a.pa, d2, link_geom<RS>(dAo, dBo), lv);
+          sn2 += (double)pa_U<RS, KIND>(a.pa, d2, link_geom<RS>(dAn, dBn), lv);
+        }
       }
     }
   }

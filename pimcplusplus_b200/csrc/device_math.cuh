@@ -394,6 +394,13 @@ __device__ __forceinline__ double pa_dU<PA_TRICUBIC>(const DevPA &pa, const Link
 // vel = Velocity(slice, slice+skip): the PutInBox'ed link vector.
 __device__ __forceinline__ double kinetic_link(const double vel[3], double four_lambda_tau_inv, int num_images,
                                                const DevSystem &s) {
+  if (num_images == 0) {
+    // -log(prod_d exp(-v_d^2 F)) = sum_d v_d^2 F, exact up to rounding while
+    // no factor underflows (the reference would then return +inf).
+    const double e0 = vel[0] * vel[0] * four_lambda_tau_inv, e1 = vel[1] * vel[1] * four_lambda_tau_inv,
+                 e2 = vel[2] * vel[2] * four_lambda_tau_inv;
+    if (e0 < 700.0 && e1 < 700.0 && e2 < 700.0) return e0 + e1 + e2;
+  }
   double GaussProd = 1.0;
   for (int dim = 0; dim < 3; dim++) {
     double GaussSum = 0.0;
@@ -458,9 +465,25 @@ __device__ __forceinline__ void warp_gaussians(DevRandom &rng, int G, double *ou
   }
   for (int guard = 0; k < G && guard < 4096; guard++) {
     const int need = (G - k + 1) >> 1;
-    const uint64_t base = rng.n + 2ull * (uint64_t)lane;
-    const double V1 = 2.0 * philox_uniform(rng.seed, rng.stream, base) - 1.0;
-    const double V2 = 2.0 * philox_uniform(rng.seed, rng.stream, base + 1) - 1.0;
+    // Candidate pair j uses uniforms n+2j and n+2j+1.  Lane j computes the
+    // Philox block holding uniform n+2j (two uniforms per block); when n is
+    // odd the second uniform is the first half of the next lane's block.
+    const uint64_t b0 = (rng.n >> 1) + (uint64_t)lane;
+    uint32_t c[4] = {(uint32_t)b0, (uint32_t)(b0 >> 32), rng.stream, 0x50494D43u};
+    philox4x32_10(c, (uint32_t)rng.seed, (uint32_t)(rng.seed >> 32));
+    const double h0 = ((double)(c[0] >> 5) * 67108864.0 + (double)(c[1] >> 6)) * (1.0 / 9007199254740992.0);
+    const double h1 = ((double)(c[2] >> 5) * 67108864.0 + (double)(c[3] >> 6)) * (1.0 / 9007199254740992.0);
+    double u1, u2;
+    if ((rng.n & 1) == 0) {
+      u1 = h0;
+      u2 = h1;
+    } else {
+      u1 = h1;
+      u2 = __shfl_down_sync(0xffffffffu, h0, 1);
+      if (lane == 31) u2 = philox_uniform(rng.seed, rng.stream, rng.n + 2ull * 31 + 1);
+    }
+    const double V1 = 2.0 * u1 - 1.0;
+    const double V2 = 2.0 * u2 - 1.0;
     const double S = V1 * V1 + V2 * V2;
     const bool acc = !(S >= 1.0);
     const unsigned m = __ballot_sync(0xffffffffu, acc);
