@@ -205,9 +205,10 @@ __device__ __forceinline__ double4 stage_sums(const BisectionArgs &a, const doub
         r0s[u] = link * skip;
         const double *pa_ = path + ((size_t)(slice1 + r0s[u]) * N + p2) * 3;
         const double *pb_ = path + ((size_t)(slice1 + r0s[u] + skip) * N + p2) * 3;
+        // L2-coherent loads: other CTAs write accepted windows during the launch.
         for (int i = 0; i < 3; i++) {
-          a2[u][i] = __ldg(pa_ + i);
-          b2[u][i] = __ldg(pb_ + i);
+          a2[u][i] = __ldcg(pa_ + i);
+          b2[u][i] = __ldcg(pb_ + i);
         }
       }
 #pragma unroll
@@ -366,7 +367,7 @@ __global__ void __launch_bounds__(512, 1) bisection_kernel(BisectionArgs a) {
       const int ptcl = s_ctl[1];
       for (int rel = tid; rel <= span; rel += blockDim.x) {
         const double *p = path + ((size_t)(slice1 + rel) * N + ptcl) * 3;
-        for (int i = 0; i < 3; i++) w_old[rel][i] = w_new[rel][i] = p[i];
+        for (int i = 0; i < 3; i++) w_old[rel][i] = w_new[rel][i] = __ldcg(p + i);
       }
       __syncthreads();
       if (warp == sampler) {

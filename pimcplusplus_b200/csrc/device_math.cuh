@@ -253,34 +253,48 @@ __device__ __forceinline__ R tricubic_eval(const R *__restrict__ F, const DGrid<
   return val;
 }
 
-// SplinePot::V (Common/PH/SplinePot.cc:19-31) with no Vouter.
+// SplinePot::V (Common/PH/SplinePot.cc:19-31) with no Vouter: the natural
+// cubic spline up to the grid end, zero beyond.  Branch-free: the spline is
+// evaluated at min(r, End) and the result selected.
 template <typename R>
 __device__ __forceinline__ R pot_V(const DTricubic<R> &t, R r) {
-  if (r <= t.pot_grid.end) return spline_col(t.pot_grid, t.pot_y, t.pot_d2, 1, 0, r);
-  return R(0);
+  const R v = spline_col(t.pot_grid, t.pot_y, t.pot_d2, 1, 0, r <= t.pot_grid.end ? r : t.pot_grid.end);
+  return r <= t.pot_grid.end ? v : R(0);
 }
 
 // ---- PAtricubicFitClass::U / dU (PAtricubicFit.cc:659-721) ----
+// Inside the fitted region (q <= qmax, z < 2q, s < 2q) the tricubic spline at
+// (q, z/2q, (s-z)/(2q-z)) (at (0,0,0) when q == 0); outside it the primitive
+// action 1/2 beta_l (V(r) + V(r')) (dU: 1/2 (V(r) + V(r'))).  Both candidates
+// are evaluated unconditionally and one is selected, so a warp never splits
+// between the two branches and every table load of the item issues in one
+// phase; out-of-region lanes read the (0,0,0) cell, which coalesces.
 template <typename R, bool DERIV>
 __device__ __forceinline__ R tricubic_pa(const DTricubic<R> &t, R q, R z, R s2, int level) {
   const DGrid<R> &qg = t.qg, &yg = t.yg, &tg = t.tg;
   z = fabs_r(z);
-  R smax = R(2.0) * q;
-  R zmax = smax;
-  R s = sqrt_r(s2);
+  const R smax = R(2.0) * q;
+  const R zmax = smax;
+  const R s = sqrt_r(s2);
+  const bool inside = (q <= t.qmax) && (z < zmax) && (s < smax);
+  const bool nonzero = inside && q != R(0);
+  const R xq = nonzero ? q : R(0);
+  const R xy = nonzero ? z / zmax : R(0);
+  const R xt = nonzero ? (s - z) / (smax - z) : R(0);
   const R *F = (DERIV ? t.dU : t.U) + (size_t)level * t.nq * t.ny * t.nt * 8;
-  if ((q <= t.qmax) && (z < zmax) && (s < smax)) {
-    if (q == R(0)) return tricubic_eval(F, qg, yg, tg, R(0), R(0), R(0));
-    R y = z / zmax;
-    R tt = (s - z) / (smax - z);
-    return tricubic_eval(F, qg, yg, tg, q, y, tt);
+  const R tri = tricubic_eval(F, qg, yg, tg, xq, xy, xt);
+  const R r = q + R(0.5) * z;
+  const R rp = q - R(0.5) * z;
+  const R vsum = pot_V(t, r) + pot_V(t, rp);
+  R prim;
+  if (DERIV) {
+    prim = R(0.5) * vsum;
+  } else {
+    R beta = t.smallest_beta;
+    for (int i = 0; i < level; i++) beta *= R(2.0);
+    prim = R(0.5) * beta * vsum;
   }
-  R r = q + R(0.5) * z;
-  R rp = q - R(0.5) * z;
-  if (DERIV) return R(0.5) * (pot_V(t, r) + pot_V(t, rp));
-  R beta = t.smallest_beta;
-  for (int i = 0; i < level; i++) beta *= R(2.0);
-  return R(0.5) * beta * (pot_V(t, r) + pot_V(t, rp));
+  return inside ? tri : prim;
 }
 
 // ---- PathClass::DistDisp two-slice form (PathClass.h:696-746) ----
