@@ -189,41 +189,80 @@ __device__ __forceinline__ double4 stage_sums(const BisectionArgs &a, const doub
     const int beg = chunk * (int)rank;
     const int end = min(total, beg + chunk);
     const double *path = a.path;
-    // Two items per pass so a thread's partner and table loads overlap.
-    for (int it0 = beg + etid; it0 < end; it0 += 2 * ethreads) {
-      double a2[2][3], b2[2][3];
-      int r0s[2];
-      bool live[2];
+    const int items = max(0, end - beg);
+    // Team size: when this CTA has fewer items than threads, T lanes share an
+    // item — the OLD and the NEW copy on different lanes and, for the tricubic
+    // fit, the four (x,y) node pairs split over the rest — which shortens the
+    // dependent chain of each lane.  T = 1 keeps one lane per item.
+    int T = 1;
+    const int tmax = KIND == PA_TRICUBIC ? 8 : 2;
+    while (T < tmax && items * T * 2 <= ethreads) T *= 2;
+    if (T == 1) {
+      // Two items per pass so a thread's partner and table loads overlap.
+      for (int it0 = beg + etid; it0 < end; it0 += 2 * ethreads) {
+        double a2[2][3], b2[2][3];
+        int r0s[2];
+        bool live[2];
 #pragma unroll
-      for (int u = 0; u < 2; u++) {
-        const int it = it0 + u * ethreads;
-        live[u] = it < end;
-        const int itc = live[u] ? it : it0;
-        const int link = itc / np;
-        const int j = itc - link * np;
-        const int p2 = j < ptcl ? j : j + 1;
-        r0s[u] = link * skip;
-        const double *pa_ = path + ((size_t)(slice1 + r0s[u]) * N + p2) * 3;
-        const double *pb_ = path + ((size_t)(slice1 + r0s[u] + skip) * N + p2) * 3;
-        // L2-coherent loads: other CTAs write accepted windows during the launch.
-        for (int i = 0; i < 3; i++) {
-          a2[u][i] = __ldcg(pa_ + i);
-          b2[u][i] = __ldcg(pb_ + i);
+        for (int u = 0; u < 2; u++) {
+          const int it = it0 + u * ethreads;
+          live[u] = it < end;
+          const int itc = live[u] ? it : it0;
+          const int link = itc / np;
+          const int j = itc - link * np;
+          const int p2 = j < ptcl ? j : j + 1;
+          r0s[u] = link * skip;
+          const double *pa_ = path + ((size_t)(slice1 + r0s[u]) * N + p2) * 3;
+          const double *pb_ = path + ((size_t)(slice1 + r0s[u] + skip) * N + p2) * 3;
+          // L2-coherent loads: other CTAs write accepted windows during the launch.
+          for (int i = 0; i < 3; i++) {
+            a2[u][i] = __ldcg(pa_ + i);
+            b2[u][i] = __ldcg(pb_ + i);
+          }
+        }
+#pragma unroll
+        for (int u = 0; u < 2; u++) {
+          if (!live[u]) continue;
+          const int r0 = r0s[u];
+          double dAo[3], dBo[3], dAn[3], dBn[3];
+          dist_disp(w_old[r0], a2[u], w_old[r0 + skip], b2[u], sys, dAo, dBo);
+          dist_disp(w_new[r0], a2[u], w_new[r0 + skip], b2[u], sys, dAn, dBn);
+          so += (double)pa_U<R, KIND>(a.pa, dg, link_geom<R>(dAo, dBo), lv);
+          sn += (double)pa_U<R, KIND>(a.pa, dg, link_geom<R>(dAn, dBn), lv);
+          if (SHADOW) {
+            const P2S *d2 = reinterpret_cast<const P2S *>(dgs);
+            so2 += (double)pa_U<RS, KIND>(a.pa, d2, link_geom<RS>(dAo, dBo), lv);
+            sn2 += (double)pa_U<RS, KIND>(a.pa, d2, link_geom<RS>(dAn, dBn), lv);
+          }
         }
       }
-#pragma unroll
-      for (int u = 0; u < 2; u++) {
-        if (!live[u]) continue;
-        const int r0 = r0s[u];
-        double dAo[3], dBo[3], dAn[3], dBn[3];
-        dist_disp(w_old[r0], a2[u], w_old[r0 + skip], b2[u], sys, dAo, dBo);
-        dist_disp(w_new[r0], a2[u], w_new[r0 + skip], b2[u], sys, dAn, dBn);
-        so += (double)pa_U<R, KIND>(a.pa, dg, link_geom<R>(dAo, dBo), lv);
-        sn += (double)pa_U<R, KIND>(a.pa, dg, link_geom<R>(dAn, dBn), lv);
-        if (SHADOW) {
-          const P2S *d2 = reinterpret_cast<const P2S *>(dgs);
-          so2 += (double)pa_U<RS, KIND>(a.pa, d2, link_geom<RS>(dAo, dBo), lv);
-          sn2 += (double)pa_U<RS, KIND>(a.pa, d2, link_geom<RS>(dAn, dBn), lv);
+    } else {
+      const int member = etid % T, team = etid / T, nteams = ethreads / T;
+      const bool is_new = (member & 1) != 0;
+      const int nparts = T >> 1, part = member >> 1;
+      const double(*w)[3] = is_new ? w_new : w_old;
+      for (int it = beg + team; it < end; it += nteams) {
+        const int link = it / np;
+        const int j = it - link * np;
+        const int p2 = j < ptcl ? j : j + 1;
+        const int r0 = link * skip;
+        const double *pa_ = path + ((size_t)(slice1 + r0) * N + p2) * 3;
+        const double *pb_ = path + ((size_t)(slice1 + r0 + skip) * N + p2) * 3;
+        const double a2[3] = {__ldcg(pa_), __ldcg(pa_ + 1), __ldcg(pa_ + 2)};
+        const double b2[3] = {__ldcg(pb_), __ldcg(pb_ + 1), __ldcg(pb_ + 2)};
+        double dA[3], dB[3];
+        dist_disp(w[r0], a2, w[r0 + skip], b2, sys, dA, dB);
+        const double v = (double)pa_U_part<R, KIND>(a.pa, dg, link_geom<R>(dA, dB), lv, part, nparts);
+        double v2 = 0.0;
+        if (SHADOW)
+          v2 = (double)pa_U_part<RS, KIND>(a.pa, reinterpret_cast<const P2S *>(dgs), link_geom<RS>(dA, dB), lv,
+                                           part, nparts);
+        if (is_new) {
+          sn += v;
+          sn2 += v2;
+        } else {
+          so += v;
+          so2 += v2;
         }
       }
     }

@@ -61,8 +61,11 @@ __device__ __forceinline__ SplineCell<R> spline_cell(const DGrid<R> &g, R x) {
   if (low < 0) { low = 0; hi = 1; }
   if (hi > (g.n - 1)) { hi = g.n - 1; low = hi - 1; }
   R xl = grid_x(g, low), xh = grid_x(g, hi);
-  R h = xh - xl;
-  R hinv = R(1.0) / h;
+  // A linear grid's cell width is delta (X(hi) - X(low) differs from it by
+  // one rounding at most), so its inverse is the precomputed deltainv.
+  const bool lin = g.type == PIMC_GRID_LINEAR;
+  R h = lin ? g.delta : xh - xl;
+  R hinv = lin ? g.deltainv : R(1.0) / h;
   c.a = (xh - x) * hinv;
   c.b = (x - xl) * hinv;
   c.a3 = c.a * c.a * c.a - c.a;
@@ -214,41 +217,38 @@ struct Node8<float> {
 };
 
 // F: [nx][ny][nz][8] with components F, Fx, Fy, Fz, Fxy, Fxz, Fyz, Fxyz.
+// The cell's (x-node, y-node) pairs k = 2 dx + dy in [k0, k1) are summed, so
+// lanes of a team can split one evaluation; [0, 4) is the whole spline.  The
+// grids are linear: the cell widths are delta and u = (x - x0) deltainv.
 template <typename R>
 __device__ __forceinline__ R tricubic_eval(const R *__restrict__ F, const DGrid<R> &gx, const DGrid<R> &gy,
-                                           const DGrid<R> &gz, R x, R y, R z) {
+                                           const DGrid<R> &gz, R x, R y, R z, int k0 = 0, int k1 = 4) {
   int ix = reverse_map(gx, x), iy = reverse_map(gy, y), iz = reverse_map(gz, z);
   ix = max(0, ix); ix = min(ix, gx.n - 2);
   iy = max(0, iy); iy = min(iy, gy.n - 2);
   iz = max(0, iz); iz = min(iz, gz.n - 2);
-  R x0 = grid_x(gx, ix), y0 = grid_x(gy, iy), z0 = grid_x(gz, iz);
-  R h = grid_x(gx, ix + 1) - x0;
-  R k = grid_x(gy, iy + 1) - y0;
-  R l = grid_x(gz, iz + 1) - z0;
   R a[4], b[4], c[4];
-  hermite4((x - x0) / h, h, a);
-  hermite4((y - y0) / k, k, b);
-  hermite4((z - z0) / l, l, c);
+  hermite4((x - grid_x(gx, ix)) * gx.deltainv, gx.delta, a);
+  hermite4((y - grid_x(gy, iy)) * gy.deltainv, gy.delta, b);
+  hermite4((z - grid_x(gz, iz)) * gz.deltainv, gz.delta, c);
   const size_t sy = (size_t)gz.n * 8, sx = (size_t)gy.n * sy;
   const R *base = F + (size_t)ix * sx + (size_t)iy * sy + (size_t)iz * 8;
   R val = R(0);
 #pragma unroll
-  for (int dx = 0; dx < 2; dx++) {
-#pragma unroll
-    for (int dy = 0; dy < 2; dy++) {
-      const R *p = base + dx * sx + dy * sy;
-      Node8<R> n0, n1;
-      n0.load(p);
-      n1.load(p + 8);
-      R A0 = a[dx], A1 = a[2 + dx], B0 = b[dy], B1 = b[2 + dy];
-      R C00 = c[0], C01 = c[2], C10 = c[1], C11 = c[3];  // (z-node, z-derivative)
-      // node (dz=0): C0 = c[0] value, c[2] derivative; node (dz=1): c[1], c[3]
-      R s00 = n0.v[0] * C00 + n0.v[3] * C01 + n1.v[0] * C10 + n1.v[3] * C11;  // F, Fz
-      R s01 = n0.v[2] * C00 + n0.v[6] * C01 + n1.v[2] * C10 + n1.v[6] * C11;  // Fy, Fyz
-      R s10 = n0.v[1] * C00 + n0.v[5] * C01 + n1.v[1] * C10 + n1.v[5] * C11;  // Fx, Fxz
-      R s11 = n0.v[4] * C00 + n0.v[7] * C01 + n1.v[4] * C10 + n1.v[7] * C11;  // Fxy, Fxyz
-      val += A0 * (B0 * s00 + B1 * s01) + A1 * (B0 * s10 + B1 * s11);
-    }
+  for (int k = 0; k < 4; k++) {
+    if (k < k0 || k >= k1) continue;
+    const int dx = k >> 1, dy = k & 1;
+    const R *p = base + dx * sx + dy * sy;
+    Node8<R> n0, n1;
+    n0.load(p);
+    n1.load(p + 8);
+    const R A0 = a[dx], A1 = a[2 + dx], B0 = b[dy], B1 = b[2 + dy];
+    const R C00 = c[0], C01 = c[2], C10 = c[1], C11 = c[3];  // (z-node, z-derivative)
+    const R s00 = n0.v[0] * C00 + n0.v[3] * C01 + n1.v[0] * C10 + n1.v[3] * C11;  // F, Fz
+    const R s01 = n0.v[2] * C00 + n0.v[6] * C01 + n1.v[2] * C10 + n1.v[6] * C11;  // Fy, Fyz
+    const R s10 = n0.v[1] * C00 + n0.v[5] * C01 + n1.v[1] * C10 + n1.v[5] * C11;  // Fx, Fxz
+    const R s11 = n0.v[4] * C00 + n0.v[7] * C01 + n1.v[4] * C10 + n1.v[7] * C11;  // Fxy, Fxyz
+    val += A0 * (B0 * s00 + B1 * s01) + A1 * (B0 * s10 + B1 * s11);
   }
   return val;
 }
@@ -270,7 +270,8 @@ __device__ __forceinline__ R pot_V(const DTricubic<R> &t, R r) {
 // between the two branches and every table load of the item issues in one
 // phase; out-of-region lanes read the (0,0,0) cell, which coalesces.
 template <typename R, bool DERIV>
-__device__ __forceinline__ R tricubic_pa(const DTricubic<R> &t, R q, R z, R s2, int level) {
+__device__ __forceinline__ R tricubic_pa(const DTricubic<R> &t, R q, R z, R s2, int level, int part = 0,
+                                         int nparts = 1) {
   const DGrid<R> &qg = t.qg, &yg = t.yg, &tg = t.tg;
   z = fabs_r(z);
   const R smax = R(2.0) * q;
@@ -282,17 +283,21 @@ __device__ __forceinline__ R tricubic_pa(const DTricubic<R> &t, R q, R z, R s2, 
   const R xy = nonzero ? z / zmax : R(0);
   const R xt = nonzero ? (s - z) / (smax - z) : R(0);
   const R *F = (DERIV ? t.dU : t.U) + (size_t)level * t.nq * t.ny * t.nt * 8;
-  const R tri = tricubic_eval(F, qg, yg, tg, xq, xy, xt);
+  const int k0 = (4 * part) / nparts, k1 = (4 * (part + 1)) / nparts;
+  const R tri = tricubic_eval(F, qg, yg, tg, xq, xy, xt, k0, k1);
   const R r = q + R(0.5) * z;
   const R rp = q - R(0.5) * z;
-  const R vsum = pot_V(t, r) + pot_V(t, rp);
-  R prim;
-  if (DERIV) {
-    prim = R(0.5) * vsum;
-  } else {
-    R beta = t.smallest_beta;
+  R beta = R(0.5);
+  if (!DERIV) {
+    beta = t.smallest_beta;
     for (int i = 0; i < level; i++) beta *= R(2.0);
-    prim = R(0.5) * beta * vsum;
+    beta = R(0.5) * beta;
+  }
+  R prim;
+  if (nparts == 1) {
+    prim = beta * (pot_V(t, r) + pot_V(t, rp));
+  } else {  // part 0 takes V(r), part 1 takes V(r'), any other part nothing
+    prim = part < 2 ? beta * pot_V(t, part == 0 ? r : rp) : R(0);
   }
   return inside ? tri : prim;
 }
@@ -357,6 +362,13 @@ __device__ __forceinline__ LinkGeom<R> link_geom(const double dA[3], const doubl
   return g;
 }
 
+template <typename R>
+__device__ __forceinline__ const DTricubic<R> &tricubic_of(const DevPA &pa);
+template <>
+__device__ __forceinline__ const DTricubic<double> &tricubic_of<double>(const DevPA &pa) { return pa.t64; }
+template <>
+__device__ __forceinline__ const DTricubic<float> &tricubic_of<float>(const DevPA &pa) { return pa.t32; }
+
 // U(q, z, s^2, level) of the pair action (ActionBaseClass's PA.U).
 template <typename R, int KIND>
 __device__ __forceinline__ R pa_U(const DevPA &pa, const typename Pair2<R>::T *diag, const LinkGeom<R> &g,
@@ -382,6 +394,15 @@ __device__ __forceinline__ float pa_U<float, PA_TRICUBIC>(const DevPA &pa, const
                                                           const LinkGeom<float> &g, int level) {
   const DTricubic<float> &t = pa.t32;
   return tricubic_pa<float, false>(t, g.q, g.z, g.s2, level);
+}
+
+// Part `part` of `nparts` of U for a team of lanes sharing one evaluation;
+// the parts sum to U (up to rounding).  The 1-D DavidPA action is not split.
+template <typename R, int KIND>
+__device__ __forceinline__ R pa_U_part(const DevPA &pa, const typename Pair2<R>::T *diag, const LinkGeom<R> &g,
+                                       int level, int part, int nparts) {
+  if (KIND == PA_TRICUBIC) return tricubic_pa<R, false>(tricubic_of<R>(pa), g.q, g.z, g.s2, level, part, nparts);
+  return part == 0 ? pa_U<R, KIND>(pa, diag, g, level) : R(0);
 }
 
 template <typename R>
