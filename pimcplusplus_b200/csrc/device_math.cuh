@@ -61,13 +61,14 @@ __device__ __forceinline__ SplineCell<R> spline_cell(const DGrid<R> &g, R x) {
   if (low < 0) { low = 0; hi = 1; }
   if (hi > (g.n - 1)) { hi = g.n - 1; low = hi - 1; }
   R xl = grid_x(g, low), xh = grid_x(g, hi);
-  // A linear grid's cell width is delta (X(hi) - X(low) differs from it by
-  // one rounding at most), so its inverse is the precomputed deltainv.
+  // A linear grid's cell width is delta (X(hi) - X(low) differs from it by a
+  // rounding), so its inverse is the precomputed deltainv; a = 1 - b keeps the
+  // two weights summing to one in either precision.
   const bool lin = g.type == PIMC_GRID_LINEAR;
   R h = lin ? g.delta : xh - xl;
   R hinv = lin ? g.deltainv : R(1.0) / h;
-  c.a = (xh - x) * hinv;
   c.b = (x - xl) * hinv;
+  c.a = lin ? R(1.0) - c.b : (xh - x) * hinv;
   c.a3 = c.a * c.a * c.a - c.a;
   c.b3 = c.b * c.b * c.b - c.b;
   c.h26 = h * h * R(0.1666666666666666666);
