@@ -227,6 +227,26 @@ int pimc_synchronize(pimc_context *ctx);
 /* The CUDA stream of the context (cudaStream_t as void*). */
 void *pimc_stream(pimc_context *ctx);
 
+/* ---- allocation-free ShortRange SingleAction ----
+ * No counterpart in the reference: it exists for callers that cannot call
+ * cudaMalloc (an application whose memory pool owns every device
+ * allocation, an embedding that forbids allocation after start-up, code
+ * running while a stream is being captured).  It needs no context: every
+ * buffer is the caller's device memory — path [num_time_slices][N][3]
+ * doubles, diag the (y, d2y) pairs of u_00 for this level [num_grid][2] on a
+ * LINEAR grid {grid_start, grid_end, num_grid} (DavidPA, no off-diagonal
+ * terms), out one double — and active/box are host arrays.  Its scratch is a
+ * fixed file-scope device array (2048 block partials, about 16 KB, held by
+ * every GPU that loads the library until exit), so n_active * N * links must
+ * not exceed 524288 (PIMC_E_ARG otherwise).  Calls share that scratch: calls
+ * that overlap on the GPU race, so keep them on one stream.  The first call
+ * on a device looks up the scratch address; make it before any stream
+ * capture.  Enqueued on `stream` (cudaStream_t, NULL = default), no sync. */
+int pimc_shortrange_single_noalloc(const double *path, int num_particles, int num_time_slices,
+                                   const double box[3], const double *diag, double grid_start,
+                                   double grid_end, int num_grid, int slice1, int slice2, const int *active,
+                                   int n_active, int level, double *out, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -29,6 +29,7 @@ if not os.path.exists(LIB_PATH):
 _lib = C.CDLL(LIB_PATH)
 
 PIMC_OK = 0
+PIMC_E_ARG = 1
 OLDMODE, NEWMODE, BOTH = 0, 1, 2
 FP64, MIXED = 0, 1
 ACTION_SHORTRANGE, ACTION_KINETIC, ACTION_LONGRANGE = 0, 1, 2
@@ -130,6 +131,7 @@ _SIGS = {
     "pimc_bisection_occupancy": (_i, [_p, _ip]),
     "pimc_synchronize": (_i, [_p]),
     "pimc_stream": (_p, [_p]),
+    "pimc_shortrange_single_noalloc": (_i, [_p, _i, _i, _dp, _p, _d, _d, _i, _i, _i, _ip, _i, _i, _p, _p]),
 }
 for _name, (_res, _args) in _SIGS.items():
     _f = getattr(_lib, _name)

@@ -1,0 +1,68 @@
+"""The allocation-free ShortRange SingleAction entry point.
+
+pimc_shortrange_single_noalloc serves callers that may not allocate device
+memory (a memory pool that owns every allocation, an embedding that forbids
+allocation after start-up, code running during stream capture): every
+buffer is the caller's, and its scratch is a fixed array inside the library.
+It is called here through the C ABI on device buffers this test owns and
+compared with the context-based pimc_single_action on the same path, on two
+calls in a row (the second reuses the scratch the first left behind).
+
+This file sorts last so that a run stopping at its first failure has run
+every other test already.
+"""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+import pimcplusplus_b200 as P
+from helpers import lj_case, random_walk_path
+from pimcplusplus_b200 import workloads as W
+
+pytestmark = pytest.mark.gpu
+
+REL64 = 1e-12
+
+
+def test_noalloc_matches_context_entry_point(tmp_path):
+    import torch
+
+    cfg, tau, box, dm = lj_case(tmp_path)
+    n, slices = cfg["N"], cfg["M"] + 1
+    path = random_walk_path(n, slices, box, 0.35, 123, far=0.1)
+    d = P.PathData(n, slices, box, tau, W.HE4_LAMBDA, 0)
+    d.set_path(path)
+    d.pa_david_from_dm(dm, 0)
+    tables = P.read_dm(dm, tau)
+    assert tables["grid_type"] == P.GRID_LINEAR
+
+    dev_path = torch.tensor(path, dtype=torch.float64, device="cuda:0").contiguous()
+    out = torch.zeros(1, dtype=torch.float64, device="cuda:0")
+    boxc = np.ascontiguousarray(box, dtype=np.float64)
+    stream = torch.cuda.current_stream().cuda_stream
+    calls = [(3, 11, [7], 0), (8, 16, [2, 40, 5], 1)]
+    for (s1, s2, active, level) in calls:
+        lev = level + tables["tau_pos"]
+        diag = np.stack([tables["ukj"][lev][:, 1], tables["ukj_d2"][lev][:, 1]], axis=1)
+        dev_diag = torch.tensor(diag, dtype=torch.float64, device="cuda:0").contiguous()
+        act = np.ascontiguousarray(active, dtype=np.int32)
+        rc = P.lib().pimc_shortrange_single_noalloc(
+            dev_path.data_ptr(), n, slices, boxc.ctypes.data_as(C.POINTER(C.c_double)), dev_diag.data_ptr(),
+            tables["grid_start"], tables["grid_end"], tables["num_grid"], s1, s2,
+            act.ctypes.data_as(C.POINTER(C.c_int)), len(act), level, out.data_ptr(), stream)
+        assert rc == P.PIMC_OK
+        torch.cuda.synchronize()
+        got = float(out.item())
+        ref = d.single_action(P.ACTION_SHORTRANGE, P.OLDMODE, s1, s2, act, level)
+        assert abs(got - ref) <= REL64 * abs(ref), (s1, s2, active, level, got, ref)
+
+
+def test_noalloc_rejects_oversized_call():
+    box = np.array([10.0, 10.0, 10.0])
+    act = np.array([0], dtype=np.int32)
+    # 600000 particles x 1 link exceeds the 524288-term scratch; rejected before any device work
+    rc = P.lib().pimc_shortrange_single_noalloc(
+        1, 600000, 3, box.ctypes.data_as(C.POINTER(C.c_double)), 1, 1.0, 5.0, 100, 0, 1,
+        act.ctypes.data_as(C.POINTER(C.c_int)), 1, 0, 1, None)
+    assert rc == P.PIMC_E_ARG if hasattr(P, "PIMC_E_ARG") else rc == 1
