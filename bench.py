@@ -352,14 +352,16 @@ def run_ours(args):
         peak, peak_kind = load_peaks()
         value = st32["pair_evals"] / (ms32 / 1000.0)
         value64 = st64["pair_evals"] / (ms64 / 1000.0)
-        per_launch_bytes = st32["pair_evals"] / world / args.steps * BYTES_PER_EVAL["mixed"]
-        achieved = per_launch_bytes / (ms32 / args.steps / 1000.0) / 1e9
+        launches_per_step = nb_launches(args.schedule, blocks)
+        evals_per_launch = st32["pair_evals"] / world / args.steps / launches_per_step
+        ms_per_launch = ms32 / args.steps / launches_per_step
+        achieved = evals_per_launch * BYTES_PER_EVAL["mixed"] / (ms_per_launch / 1000.0) / 1e9
         traffic = None
         prof = os.path.join(ROOT, "profiles", "bisection_c2_traffic.json")
         if os.path.exists(prof):
             with open(prof) as f:
                 pj = json.load(f)
-            traffic = pj.get("dram_bytes_per_pair_eval_mixed", 0) * st32["pair_evals"] / world / args.steps
+            traffic = pj.get("dram_bytes_per_pair_eval_mixed", 0) * evals_per_launch
         cpu = cpu_baseline(1, args.cpu_seconds) if world == 1 and not args.no_cpu else None
         path_bytes = n * slices * 3 * 8
         line = {
@@ -388,7 +390,9 @@ def run_ours(args):
             "gpu_launches": args.steps * 2 * nb_launches(args.schedule, blocks),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
-                         "bytes_per_eval": BYTES_PER_EVAL["mixed"],
+                         "bytes_per_eval": BYTES_PER_EVAL["mixed"], "evals_per_launch": evals_per_launch,
+                         "ms_per_launch": ms_per_launch,
+                         "traffic_source": "profiles/bisection_c2_traffic.json (ncu, one round) scaled by evals",
                          "kernel": "bisection_kernel<PA_TRICUBIC,float>"},
             "clocks": clocks,
         }
