@@ -270,26 +270,57 @@ __device__ __forceinline__ double4 stage_sums(const BisectionArgs &a, const doub
   return make_double4(so, sn, so2, sn2);
 }
 
+// Committed or speculative position of a chain's Local stream.
+struct RngSnap {
+  unsigned long long n;
+  int one_left;
+  double x2;
+};
+
+__device__ __forceinline__ DevRandom rng_from(const RngSnap &s, uint64_t seed, uint32_t stream) {
+  DevRandom r;
+  r.seed = seed;
+  r.stream = stream;
+  r.n = s.n;
+  r.one_left = s.one_left;
+  r.x2 = s.x2;
+  return r;
+}
+__device__ __forceinline__ void rng_store(RngSnap &s, const DevRandom &r) {
+  s.n = r.n;
+  s.one_left = r.one_left;
+  s.x2 = r.x2;
+}
+
 // KIND: pair-action type; R: precision of the pair terms; SHADOW: also
 // evaluate the pair terms in the other precision for the dS error.
 //
-// Per move: the sampler warp (the last warp, owner of the RNG stream) picks
-// the particle and samples the top level.  While the other warps evaluate
-// the OLD and NEW action of stage l, the sampler speculatively samples level
-// l-1 from the stream position that follows stage l's acceptance draw; the
-// draw order is therefore exactly the reference's, and the speculative
-// state is committed only if stage l accepts.
+// Two sampler warps own the Local stream; the committed stream position
+// lives in shared memory.  While the other warps evaluate the OLD and NEW
+// action of stage l:
+//  * the level sampler (the last warp) speculatively samples level l-1 from
+//    the position that follows stage l's acceptance draw — committed if
+//    stage l accepts and the move goes on;
+//  * the move speculator (the warp before it) draws the next move's slice
+//    window and particle from the same position, loads that particle's
+//    window into the spare buffer and samples its top level — committed if
+//    the move ends at this stage (a rejection, or acceptance at level 0),
+//    unless the accepted particle was drawn again, whose window changes.
+// The draw order is therefore exactly the reference's.
 template <int KIND, typename R, bool SHADOW>
 __global__ void __launch_bounds__(512, 1) bisection_kernel(BisectionArgs a) {
   typedef typename Pair2<R>::T P2;
   typedef typename std::conditional<std::is_same<R, double>::value, float, double>::type RS;  // shadow precision
   typedef typename Pair2<RS>::T P2S;
-  __shared__ double w_old[kMaxWindow][3], w_new[kMaxWindow][3];
-  __shared__ double gbuf[3 * 32];
+  __shared__ double win_old[2][kMaxWindow][3], win_new[2][kMaxWindow][3];
+  __shared__ double gbuf[2][3 * 32];
   __shared__ double sh_red[16][4];  // per warp: S_old, S_new, and their shadows
   __shared__ double xchg[2][kMaxCluster][4];
   __shared__ double s_logsr[kMaxLevels], s_logu[kMaxLevels];
-  __shared__ int s_ctl[4];  // slice1, ptcl, stage accepted, status
+  __shared__ int s_ctl[4];   // slice1, ptcl, stage accepted, status
+  __shared__ int s_next[4];  // next move speculated: valid, slice1, ptcl
+  __shared__ double s_next_f[2];
+  __shared__ RngSnap s_rng, s_spec1, s_spec2;
   __shared__ __align__(8) uint64_t s_bar;
   extern __shared__ __align__(16) unsigned char dyn[];
 
@@ -301,7 +332,9 @@ __global__ void __launch_bounds__(512, 1) bisection_kernel(BisectionArgs a) {
   const int lane = tid & 31, warp = tid >> 5;
   const int nwarps = blockDim.x >> 5;
   const int sampler = nwarps - 1;
-  const int ethreads = (nwarps - 1) * 32;  // evaluating threads: every warp but the sampler
+  const int specwarp = nwarps >= 4 ? nwarps - 2 : -1;  // next-move speculator (needs >= 4 warps)
+  const int ethreads = (nwarps - (specwarp >= 0 ? 2 : 1)) * 32;  // evaluating threads: warps below the samplers
+  const bool evaluator = tid < ethreads;
   const DevSystem &sys = a.sys;
   const int N = sys.N;
   const int L = a.num_levels;
@@ -355,13 +388,15 @@ __global__ void __launch_bounds__(512, 1) bisection_kernel(BisectionArgs a) {
     if (SHADOW) diag_smem_s = reinterpret_cast<const P2S *>(dyn + bytes);
   }
 
-  // ---- RNG state: every lane of the sampler warp of every CTA holds the same copy ----
-  DevRandom rng;
-  rng.seed = cs->seed;
-  rng.n = cs->nlocal;
-  rng.stream = cs->stream;
-  rng.one_left = cs->one_left;
-  rng.x2 = cs->x2;
+  const uint64_t seed = cs->seed;
+  const uint32_t stream = cs->stream;
+  if (tid == 0) {
+    s_rng.n = cs->nlocal;
+    s_rng.one_left = cs->one_left;
+    s_rng.x2 = cs->x2;
+    s_ctl[3] = 0;
+    s_next[0] = 0;
+  }
   unsigned long long moves = 0, accepted = 0, stages = 0, pair_evals = 0, flips = 0;
   int status = 0;
   double *path = a.path;
@@ -370,7 +405,7 @@ __global__ void __launch_bounds__(512, 1) bisection_kernel(BisectionArgs a) {
   // Window of this cluster in the concurrent schedule.
   int slice1 = 0;
   if (a.concurrent) {
-    const int o = (int)floor(philox_uniform(rng.seed, kStreamCommon, a.round) * span);
+    const int o = (int)floor(philox_uniform(seed, kStreamCommon, a.round) * span);
     slice1 = o + window * span;
     if (slice1 + span > sys.S - 1) {
       // Inactive this round (uniform over the cluster): mark its trace slots.
@@ -386,176 +421,228 @@ __global__ void __launch_bounds__(512, 1) bisection_kernel(BisectionArgs a) {
     }
   }
   if (KIND == PA_DAVID) cluster.sync();  // every CTA has read xchg[1]
+  __syncthreads();
   const int numLeft = sys.S - span;
-  const int n_blocks = a.concurrent ? 1 : a.n_blocks;
-  if (tid == 0) s_ctl[3] = 0;
+  const int total_moves = (a.concurrent ? 1 : a.n_blocks) * a.steps_per_block;
+  int cur = 0;
+  bool have_next = false;
 
-  for (int blk = 0; blk < n_blocks; blk++) {
-    for (int step = 0; step < a.steps_per_block; step++) {
+  for (int m = 0; m < total_moves; m++) {
+    const int blk = m / a.steps_per_block, step = m - blk * a.steps_per_block;
+    if (!have_next) {
       // ChooseTimeSlices (BisectionBlock.cc:362-374), ChooseParticle (NoPermuteClass.cc:61-68)
       if (warp == sampler) {
+        DevRandom rng = rng_from(s_rng, seed, stream);
         if (!a.concurrent && step == 0) slice1 = rng.LocalInt(numLeft);
         const int p = rng.LocalInt(N);
+        __syncwarp();
         if (lane == 0) {
           s_ctl[0] = slice1;
           s_ctl[1] = p;
+          rng_store(s_rng, rng);
         }
       }
       __syncthreads();
       slice1 = s_ctl[0];
-      const int ptcl = s_ctl[1];
+      const int p = s_ctl[1];
       for (int rel = tid; rel <= span; rel += blockDim.x) {
-        const double *p = path + ((size_t)(slice1 + rel) * N + ptcl) * 3;
-        for (int i = 0; i < 3; i++) w_old[rel][i] = w_new[rel][i] = __ldcg(p + i);
+        const double *q = path + ((size_t)(slice1 + rel) * N + p) * 3;
+        for (int i = 0; i < 3; i++) win_old[cur][rel][i] = win_new[cur][rel][i] = __ldcg(q + i);
       }
       __syncthreads();
       if (warp == sampler) {
-        const double lsr = sample_level_warp(w_old, w_new, gbuf, L, L - 1, sys, rng, lane);
+        DevRandom rng = rng_from(s_rng, seed, stream);
+        const double lsr = sample_level_warp(win_old[cur], win_new[cur], gbuf[0], L, L - 1, sys, rng, lane);
         const double lu = log(rng.Local());
+        __syncwarp();
         if (lane == 0) {
           s_logsr[L - 1] = lsr;
           s_logu[L - 1] = lu;
+          rng_store(s_rng, rng);
         }
       }
       __syncthreads();
+    }
+    slice1 = s_ctl[0];
+    const int ptcl = s_ctl[1];
+    const bool more = m + 1 < total_moves;
+    const bool next_new_block = !a.concurrent && ((m + 1) % a.steps_per_block == 0);
+    double(*w_old)[3] = win_old[cur];
+    double(*w_new)[3] = win_new[cur];
 
-      double prevDS = 0.0, prevDS_s = 0.0;
-      bool acc_all = true;
-      int passed = 0;
-      pimc_move_record rec;
-      if (lead) {
-        rec.slice1 = slice1;
-        rec.ptcl = ptcl;
-        for (int i = 0; i < 8; i++) rec.dS[i] = rec.dS_shadow[i] = 0.0;
-      }
-      int si = 0;
-      for (int level = L - 1; level >= 0; level--, si++) {
-        // ---- LocalStageClass::Attempt (StageClass.cc:49-95) ----
-        DevRandom spec = rng;
-        if (warp != sampler) {
-          const size_t st = KIND == PA_DAVID ? (size_t)david_of<R>(a.pa).diag_stride : 0;
-          const size_t sts = (KIND == PA_DAVID && SHADOW) ? (size_t)david_of<RS>(a.pa).diag_stride : 0;
-          const double4 v = stage_sums<KIND, R, SHADOW>(a, w_old, w_new, diag_smem ? diag_smem + level * st : nullptr,
-                                                        diag_smem_s ? diag_smem_s + level * sts : nullptr, level,
-                                                        slice1, ptcl, rank, CL, tid, ethreads);
-          const double o1 = warp_sum(v.x), n1 = warp_sum(v.y);
-          const double o2 = SHADOW ? warp_sum(v.z) : 0.0, n2 = SHADOW ? warp_sum(v.w) : 0.0;
-          if (lane == 0) {
-            sh_red[warp][0] = o1;
-            sh_red[warp][1] = n1;
-            sh_red[warp][2] = o2;
-            sh_red[warp][3] = n2;
-          }
-        } else {
+    double prevDS = 0.0, prevDS_s = 0.0;
+    bool acc_all = true;
+    int passed = 0;
+    pimc_move_record rec;
+    if (lead) {
+      rec.slice1 = slice1;
+      rec.ptcl = ptcl;
+      for (int i = 0; i < 8; i++) rec.dS[i] = rec.dS_shadow[i] = 0.0;
+    }
+    int si = 0;
+    for (int level = L - 1; level >= 0; level--, si++) {
+      // ---- LocalStageClass::Attempt (StageClass.cc:49-95) ----
+      if (evaluator) {
+        const size_t st = KIND == PA_DAVID ? (size_t)david_of<R>(a.pa).diag_stride : 0;
+        const size_t sts = (KIND == PA_DAVID && SHADOW) ? (size_t)david_of<RS>(a.pa).diag_stride : 0;
+        const double4 v = stage_sums<KIND, R, SHADOW>(a, w_old, w_new, diag_smem ? diag_smem + level * st : nullptr,
+                                                      diag_smem_s ? diag_smem_s + level * sts : nullptr, level,
+                                                      slice1, ptcl, rank, CL, tid, ethreads);
+        const double o1 = warp_sum(v.x), n1 = warp_sum(v.y);
+        const double o2 = SHADOW ? warp_sum(v.z) : 0.0, n2 = SHADOW ? warp_sum(v.w) : 0.0;
+        if (lane == 0) {
+          sh_red[warp][0] = o1;
+          sh_red[warp][1] = n1;
+          sh_red[warp][2] = o2;
+          sh_red[warp][3] = n2;
+        }
+      } else {
+        if (warp == sampler && level > 0) {
           // speculative sampling of the next level (BisectionStage::Sample of stage level-1)
-          if (level > 0) {
-            const double lsr = sample_level_warp(w_old, w_new, gbuf, L, level - 1, sys, spec, lane);
-            const double lu = log(spec.Local());
-            if (lane == 0) {
-              s_logsr[level - 1] = lsr;
-              s_logu[level - 1] = lu;
-            }
-          }
-          if (lane < 4) sh_red[warp][lane] = 0.0;
-        }
-        // Counted as the reference performs them: OLD + NEW of the stage's
-        // links; the OLD terms of later levels evaluated ahead are not counted.
-        if (lead && (level == 0 || a.sr_higher)) pair_evals += 2ull * (unsigned long long)(N - 1) * (span >> level);
-        __syncthreads();
-        // ---- reduce: warps -> CTA (warp 0) -> cluster (DSMEM, rank order) ----
-        const int par = xc & 1;
-        xc++;
-        if (warp == 0 && lane < 4) {
-          double v = 0.0;
-          for (int w = 0; w < nwarps; w++) v += sh_red[w][lane];
-          if (CL > 1)
-            for (unsigned r = 0; r < CL; r++) cluster.map_shared_rank(&xchg[par][rank][0], r)[lane] = v;
-          else
-            xchg[par][0][lane] = v;
-        }
-        if (CL > 1)
-          cluster.sync();
-        else
+          DevRandom spec = rng_from(s_rng, seed, stream);
+          const double lsr = sample_level_warp(w_old, w_new, gbuf[0], L, level - 1, sys, spec, lane);
+          const double lu = log(spec.Local());
           __syncwarp();
-        if (warp == 0) {
-          double v = 0.0;
-          if (lane < 4)
-            for (unsigned r = 0; r < CL; r++) v += xchg[par][r][lane];
-          const double so = __shfl_sync(0xffffffffu, v, 0);
-          const double sn = __shfl_sync(0xffffffffu, v, 1);
-          const double so2 = __shfl_sync(0xffffffffu, v, 2);
-          const double sn2 = __shfl_sync(0xffffffffu, v, 3);
-          // ---- Metropolis test, identical in every CTA ----
-          const double currActionChange = sn - so;
-          const double logsr = s_logsr[level];
-          const double logAcceptProb = logsr - currActionChange + prevDS;
-          const double logu = s_logu[level];
-          bool toAccept = logAcceptProb >= logu;
-          if (toAccept && (fabs(sn) > 1e50 || fabs(so) > 1e50)) {  // StageClass.cc:74-85
-            toAccept = false;
-            status = PIMC_E_STAGING;
-          }
-          if (!isfinite(currActionChange)) status = PIMC_E_NAN;
-          if (SHADOW) {
-            const double dss = sn2 - so2;
-            const bool other = (logsr - dss + prevDS_s) >= logu;
-            if (other != toAccept && lead) flips++;
-            prevDS_s = dss;
-            if (lead && si < 8) rec.dS_shadow[si] = dss;
-          }
-          prevDS = currActionChange;
-          if (lead && si < 8) rec.dS[si] = currActionChange;
           if (lane == 0) {
-            s_ctl[2] = toAccept ? 1 : 0;
-            s_ctl[3] = status;
+            s_logsr[level - 1] = lsr;
+            s_logu[level - 1] = lu;
+            rng_store(s_spec1, spec);
           }
         }
-        __syncthreads();
-        if (tid == 0) stages++;
-        if (!s_ctl[2] || s_ctl[3]) {
-          acc_all = false;
-          break;
+        if (warp == specwarp && more) {
+          // speculative start of the next move, as if this move ends here
+          DevRandom spec = rng_from(s_rng, seed, stream);
+          const int ns1 = next_new_block ? spec.LocalInt(numLeft) : slice1;
+          const int np_ = spec.LocalInt(N);
+          double(*wo)[3] = win_old[cur ^ 1];
+          double(*wn)[3] = win_new[cur ^ 1];
+          for (int rel = lane; rel <= span; rel += 32) {
+            const double *q = path + ((size_t)(ns1 + rel) * N + np_) * 3;
+            for (int i = 0; i < 3; i++) wo[rel][i] = wn[rel][i] = __ldcg(q + i);
+          }
+          __syncwarp();
+          const double lsr = sample_level_warp(wo, wn, gbuf[1], L, L - 1, sys, spec, lane);
+          const double lu = log(spec.Local());
+          __syncwarp();
+          if (lane == 0) {
+            s_next[1] = ns1;
+            s_next[2] = np_;
+            s_next_f[0] = lsr;
+            s_next_f[1] = lu;
+            rng_store(s_spec2, spec);
+          }
         }
-        if (warp == sampler) rng = spec;  // commit the speculative draws of the next level
-        passed++;
+        if (lane < 4) sh_red[warp][lane] = 0.0;
       }
-      // ---- AcceptCopy (PathClass.cc:797-863); a rejected move left HBM untouched ----
-      if (acc_all) {
-        if (rank == 0)
-          for (int rel = tid; rel <= span; rel += blockDim.x) {
-            double v[3] = {w_new[rel][0], w_new[rel][1], w_new[rel][2]};
-            put_in_box_fast(v, sys);
-            double *p = path + ((size_t)(slice1 + rel) * N + ptcl) * 3;
-            p[0] = v[0];
-            p[1] = v[1];
-            p[2] = v[2];
-          }
+      // Counted as the reference performs them: OLD + NEW of the stage's links.
+      if (lead && (level == 0 || a.sr_higher)) pair_evals += 2ull * (unsigned long long)(N - 1) * (span >> level);
+      __syncthreads();
+      // ---- reduce: warps -> CTA (warp 0) -> cluster (DSMEM, rank order) ----
+      const int par = xc & 1;
+      xc++;
+      if (warp == 0 && lane < 4) {
+        double v = 0.0;
+        for (int w = 0; w < nwarps; w++) v += sh_red[w][lane];
         if (CL > 1)
-          cluster.sync();
+          for (unsigned r = 0; r < CL; r++) cluster.map_shared_rank(&xchg[par][rank][0], r)[lane] = v;
         else
-          __syncthreads();
+          xchg[par][0][lane] = v;
       }
-      if (lead) {
-        moves++;
-        if (acc_all) accepted++;
-        if (a.trace) {
-          rec.accepted = acc_all ? 1 : 0;
-          rec.stages_passed = passed;
-          const long long idx = a.concurrent ? a.trace_offset + (long long)window * a.steps_per_block + step
-                                             : a.trace_offset + (long long)blk * a.steps_per_block + step;
-          a.trace[idx] = rec;
+      if (CL > 1)
+        cluster.sync();
+      else
+        __syncwarp();
+      if (warp == 0) {
+        double v = 0.0;
+        if (lane < 4)
+          for (unsigned r = 0; r < CL; r++) v += xchg[par][r][lane];
+        const double so = __shfl_sync(0xffffffffu, v, 0);
+        const double sn = __shfl_sync(0xffffffffu, v, 1);
+        const double so2 = __shfl_sync(0xffffffffu, v, 2);
+        const double sn2 = __shfl_sync(0xffffffffu, v, 3);
+        // ---- Metropolis test, identical in every CTA ----
+        const double currActionChange = sn - so;
+        const double logsr = s_logsr[level];
+        const double logAcceptProb = logsr - currActionChange + prevDS;
+        const double logu = s_logu[level];
+        bool toAccept = logAcceptProb >= logu;
+        if (toAccept && (fabs(sn) > 1e50 || fabs(so) > 1e50)) {  // StageClass.cc:74-85
+          toAccept = false;
+          status = PIMC_E_STAGING;
+        }
+        if (!isfinite(currActionChange)) status = PIMC_E_NAN;
+        if (SHADOW) {
+          const double dss = sn2 - so2;
+          const bool other = (logsr - dss + prevDS_s) >= logu;
+          if (other != toAccept && lead) flips++;
+          prevDS_s = dss;
+          if (lead && si < 8) rec.dS_shadow[si] = dss;
+        }
+        prevDS = currActionChange;
+        if (lead && si < 8) rec.dS[si] = currActionChange;
+        // commit the stream position the outcome selects
+        const bool ends = !toAccept || level == 0 || status != 0;
+        if (lane == 0) {
+          s_ctl[2] = toAccept ? 1 : 0;
+          s_ctl[3] = status;
+          int nv = 0;
+          if (!ends) {
+            s_rng = s_spec1;
+          } else if (status == 0 && more && specwarp >= 0 && !(toAccept && s_next[2] == ptcl)) {
+            s_rng = s_spec2;
+            s_ctl[0] = s_next[1];
+            s_ctl[1] = s_next[2];
+            s_logsr[L - 1] = s_next_f[0];
+            s_logu[L - 1] = s_next_f[1];
+            nv = 1;
+          }
+          s_next[0] = nv;
         }
       }
-      if (s_ctl[3] != 0) break;
+      __syncthreads();
+      if (tid == 0) stages++;
+      if (!s_ctl[2] || s_ctl[3]) {
+        acc_all = false;
+        break;
+      }
+      passed++;
+    }
+    have_next = s_next[0] != 0;
+    // ---- AcceptCopy (PathClass.cc:797-863); a rejected move left HBM untouched ----
+    if (acc_all) {
+      if (rank == 0)
+        for (int rel = tid; rel <= span; rel += blockDim.x) {
+          double v[3] = {w_new[rel][0], w_new[rel][1], w_new[rel][2]};
+          put_in_box_fast(v, sys);
+          double *q = path + ((size_t)(slice1 + rel) * N + ptcl) * 3;
+          q[0] = v[0];
+          q[1] = v[1];
+          q[2] = v[2];
+        }
+      if (CL > 1)
+        cluster.sync();
+      else
+        __syncthreads();
+    }
+    if (lead) {
+      moves++;
+      if (acc_all) accepted++;
+      if (a.trace) {
+        rec.accepted = acc_all ? 1 : 0;
+        rec.stages_passed = passed;
+        const long long idx = a.concurrent ? a.trace_offset + (long long)window * a.steps_per_block + step
+                                           : a.trace_offset + (long long)blk * a.steps_per_block + step;
+        a.trace[idx] = rec;
+      }
     }
     if (s_ctl[3] != 0) break;
-  }
-  if (warp == sampler && lane == 0 && rank == 0) {
-    cs->nlocal = rng.n;
-    cs->one_left = rng.one_left;
-    cs->x2 = rng.x2;
+    if (have_next) cur ^= 1;
+    __syncthreads();  // every thread has read s_ctl / s_next before the next move rewrites them
   }
   if (lead) {
+    cs->nlocal = s_rng.n;
+    cs->one_left = s_rng.one_left;
+    cs->x2 = s_rng.x2;
     cs->moves += moves;
     cs->accepted += accepted;
     cs->stages += stages;
