@@ -281,6 +281,37 @@ class PathData:
     def synchronize(self):
         self._check(_lib.pimc_synchronize(self.h), "synchronize")
 
+    # ---- long range: PathClass k-vectors and rho_k, LongRangeClass tables ----
+    def setup_kvecs(self, kcutoff):
+        nk = C.c_int()
+        self._check(_lib.pimc_setup_kvecs(self.h, kcutoff, C.byref(nk)), "setup_kvecs")
+        self.num_k = nk.value
+        return nk.value
+
+    def kvecs(self):
+        out = np.empty((self.num_k, 3))
+        self._check(_lib.pimc_get_kvecs(self.h, _dptr(out)), "get_kvecs")
+        return out
+
+    def set_longrange(self, ulong_k, ulong_r0, ushort_k0, ulong_k0, dulong_k, dulong_r0, dushort_k0, dulong_k0,
+                      use_background=True):
+        arrs = [np.ascontiguousarray(a, dtype=np.float64) for a in
+                (ulong_k, ulong_r0, ushort_k0, ulong_k0, dulong_k, dulong_r0, dushort_k0, dulong_k0)]
+        self._check(_lib.pimc_set_longrange(self.h, arrs[1].shape[0], *[_dptr(a) for a in arrs],
+                                            int(use_background)), "set_longrange")
+
+    def calc_rhok(self):
+        self._check(_lib.pimc_calc_rhok(self.h), "calc_rhok")
+
+    def update_rhok(self, slice1, slice2, active, level):
+        a = np.ascontiguousarray(active, dtype=np.int32)
+        self._check(_lib.pimc_update_rhok(self.h, slice1, slice2, _iptr(a), len(a), level), "update_rhok")
+
+    def get_rhok(self, copy=OLDMODE):
+        out = np.empty((self.S, self.num_k, 2))
+        self._check(_lib.pimc_get_rhok(self.h, copy, _dptr(out)), "get_rhok")
+        return out[..., 0] + 1j * out[..., 1]
+
 
 class ActionBaseClass:
     """ActionBaseClass (PIMC++/src/Actions/ActionBase.h:31-75) over the device."""
@@ -316,6 +347,14 @@ class KineticClass(ActionBaseClass):
 
     def GetName(self):
         return "Kinetic"
+
+
+class LongRangeClass(ActionBaseClass):
+    """LongRangeClass (PIMC++/src/Actions/LongRangeClass.cc:273-442)."""
+    kind = ACTION_LONGRANGE
+
+    def GetName(self):
+        return "LongRange"
 
 
 class BisectionBlock:

@@ -13,6 +13,7 @@
 
 #include "action_kernels.cuh"
 #include "bisection.cuh"
+#include "longrange.cuh"
 #include "pimc_internal.h"
 
 using namespace pimc;
@@ -130,6 +131,41 @@ int finish_scalar(pimc_context *ctx, double *out) {
   return PIMC_OK;
 }
 
+LRDesc lr_desc(const pimc_context *ctx) {
+  LRDesc lr;
+  lr.nk = ctx->num_k;
+  for (int d = 0; d < 3; d++) {
+    lr.kmax[d] = ctx->kmax[d];
+    lr.kbox[d] = ctx->kbox[d];
+  }
+  lr.coff[0] = 0;
+  lr.coff[1] = 2 * ctx->kmax[0] + 1;
+  lr.coff[2] = lr.coff[1] + 2 * ctx->kmax[1] + 1;
+  lr.kidx = ctx->d_kidx;
+  return lr;
+}
+
+// PairActionFitClass::IsLongRange of the context's pair action.
+bool pa_long_range(const pimc_context *ctx) { return ctx->pa.kind == PA_TRICUBIC; }
+
+// The constant (Madelung, k=0 / background) part of LongRangeClass's sum over
+// slices [slice1, slice2] step 2^level (LongRangeClass.cc:320-366).
+double lr_constant(const pimc_context *ctx, int slice1, int slice2, int level, bool deriv) {
+  const int skip = 1 << level;
+  const double N = (double)ctx->sys.N;
+  const double r0 = deriv ? ctx->dulong_r0[level] : ctx->ulong_r0[level];
+  const double sk0 = deriv ? ctx->dushort_k0[level] : ctx->ushort_k0[level];
+  const double lk0 = deriv ? ctx->dulong_k0[level] : ctx->ulong_k0[level];
+  double homo = 0.0, background = 0.0, k0Homo = 0.0;
+  for (int slice = slice1; slice <= slice2; slice += skip) {
+    const double factor = (slice == slice1 || slice == slice2) ? 0.5 : 1.0;
+    homo -= factor * 0.5 * N * r0;
+    background -= factor * 0.5 * N * N * sk0;
+    k0Homo += factor * 0.5 * N * N * lk0;
+  }
+  return homo + (ctx->use_background ? background : k0Homo);
+}
+
 }  // namespace
 
 extern "C" {
@@ -215,6 +251,11 @@ int pimc_destroy(pimc_context *ctx) {
   if (ctx->h_out) cudaFreeHost(ctx->h_out);
   cudaFree(ctx->d_chain);
   cudaFree(ctx->d_trace);
+  cudaFree(ctx->d_kidx);
+  cudaFree(ctx->d_rhok[0]);
+  cudaFree(ctx->d_rhok[1]);
+  cudaFree(ctx->d_ulong_k);
+  cudaFree(ctx->d_dulong_k);
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
   delete ctx;
   return PIMC_OK;
@@ -381,6 +422,9 @@ int pimc_get_path(pimc_context *ctx, int copy, double *path) {
   return PIMC_OK;
 }
 
+static int longrange_single(pimc_context *ctx, int copy, int slice1, int slice2, const ActiveList &act, int level,
+                            double *out);
+
 static int check_slices(pimc_context *ctx, int slice1, int slice2, int level, bool inclusive) {
   if (level < 0 || level >= kMaxLevels) return fail(ctx, PIMC_E_ARG, "level out of range");
   if (slice1 < 0 || slice2 < slice1 || slice2 >= ctx->sys.S) return fail(ctx, PIMC_E_ARG, "slice range out of range");
@@ -398,6 +442,7 @@ int pimc_single_action(pimc_context *ctx, int action, int copy, int slice1, int 
   ActiveList act;
   if ((rc = check_active(ctx, active, n_active, act))) return rc;
   CK(cudaSetDevice(ctx->device));
+  if (action == PIMC_ACTION_LONGRANGE) return longrange_single(ctx, copy, slice1, slice2, act, level, out);
   const int skip = 1 << level;
   const int nlinks = (slice2 - slice1 + skip - 1) / skip;
   ReduceTarget t{ctx->stream, ctx->d_partials, ctx->d_counter, ctx->d_out};
@@ -427,12 +472,58 @@ int pimc_single_action(pimc_context *ctx, int action, int copy, int slice1, int 
   return finish_scalar(ctx, out);
 }
 
+// LongRangeClass::SingleAction (LongRangeClass.cc:273-371): on the NEW copy
+// rho_k is first updated from OLD for the active particles.
+static int longrange_single(pimc_context *ctx, int copy, int slice1, int slice2, const ActiveList &act, int level,
+                            double *out) {
+  if (!ctx->lr_ready) return fail(ctx, PIMC_E_STATE, "pimc_set_longrange not called");
+  if (level >= ctx->lr_levels) return fail(ctx, PIMC_E_ARG, "level beyond the long-range tables");
+  const int skip = 1 << level;
+  if (slice2 > ctx->sys.S - 1) return fail(ctx, PIMC_E_ARG, "slice range out of range");
+  const LRDesc lr = lr_desc(ctx);
+  if (copy == PIMC_NEW)
+    CK(launch_rhok_update(ctx->stream, ctx->d_path[0], ctx->d_path[1], ctx->sys.N, lr, act, slice1, slice2, skip,
+                          ctx->d_rhok[0], ctx->d_rhok[1]));
+  double ksum = 0.0;
+  if (pa_long_range(ctx)) {
+    ReduceTarget t{ctx->stream, ctx->d_partials, ctx->d_counter, ctx->d_out};
+    CK(launch_lr_sum(t, ctx->d_rhok[copy], lr, ctx->d_ulong_k + (size_t)level * ctx->num_k, slice1, slice2, skip,
+                     ctx->sm_count));
+    int rc = finish_scalar(ctx, &ksum);
+    if (rc) return rc;
+  } else {
+    CK(cudaStreamSynchronize(ctx->stream));
+  }
+  *out = ksum + lr_constant(ctx, slice1, slice2, level, false);
+  return PIMC_OK;
+}
+
 int pimc_d_dbeta(pimc_context *ctx, int action, int slice1, int slice2, int level, double *out) {
   if (!ctx || !out) return PIMC_E_ARG;
   int rc = check_slices(ctx, slice1, slice2, level, false);
   if (rc) return rc;
   CK(cudaSetDevice(ctx->device));
   const int skip = 1 << level;
+  if (action == PIMC_ACTION_LONGRANGE) {
+    // LongRangeClass::d_dBeta (LongRangeClass.cc:374-442): rho_k of the OLD
+    // copy recomputed (CalcRho_ks_Fast), then the dU tables.
+    if (!ctx->lr_ready) return fail(ctx, PIMC_E_STATE, "pimc_set_longrange not called");
+    if (level >= ctx->lr_levels) return fail(ctx, PIMC_E_ARG, "level beyond the long-range tables");
+    const LRDesc lr = lr_desc(ctx);
+    CK(launch_rhok_full(ctx->stream, ctx->d_path[0], ctx->sys.N, ctx->sys.S, lr, ctx->d_rhok[0]));
+    double ksum = 0.0;
+    if (pa_long_range(ctx)) {
+      ReduceTarget t{ctx->stream, ctx->d_partials, ctx->d_counter, ctx->d_out};
+      CK(launch_lr_sum(t, ctx->d_rhok[0], lr, ctx->d_dulong_k + (size_t)level * ctx->num_k, slice1, slice2, skip,
+                       ctx->sm_count));
+      int rc2 = finish_scalar(ctx, &ksum);
+      if (rc2) return rc2;
+    } else {
+      CK(cudaStreamSynchronize(ctx->stream));
+    }
+    *out = ksum + lr_constant(ctx, slice1, slice2, level, true);
+    return PIMC_OK;
+  }
   const int nlinks = (slice2 - slice1 + skip - 1) / skip;
   if (nlinks == 0) {
     *out = 0.0;
@@ -466,6 +557,7 @@ int pimc_accept_copy(pimc_context *ctx, int slice1, int slice2, const int *activ
   if (n_active == 0) return PIMC_OK;
   CK(cudaSetDevice(ctx->device));
   CK(launch_accept(ctx->stream, ctx->d_path[0], ctx->d_path[1], ctx->sys, act, slice1, slice2));
+  if (ctx->num_k > 0) CK(launch_rhok_copy(ctx->stream, ctx->d_rhok[1], ctx->d_rhok[0], ctx->num_k, slice1, slice2));
   CK(cudaStreamSynchronize(ctx->stream));
   return PIMC_OK;
 }
@@ -479,6 +571,7 @@ int pimc_reject_copy(pimc_context *ctx, int slice1, int slice2, const int *activ
   if (n_active == 0) return PIMC_OK;
   CK(cudaSetDevice(ctx->device));
   CK(launch_reject(ctx->stream, ctx->d_path[0], ctx->d_path[1], ctx->sys, act, slice1, slice2));
+  if (ctx->num_k > 0) CK(launch_rhok_copy(ctx->stream, ctx->d_rhok[0], ctx->d_rhok[1], ctx->num_k, slice1, slice2));
   CK(cudaStreamSynchronize(ctx->stream));
   return PIMC_OK;
 }
@@ -659,18 +752,121 @@ int pimc_synchronize(pimc_context *ctx) {
 
 void *pimc_stream(pimc_context *ctx) { return ctx ? (void *)ctx->stream : nullptr; }
 
-// Long-range entry points are declared in the header; until the rho_k
-// kernels are linked in they report PIMC_E_STATE.
-int pimc_setup_kvecs(pimc_context *ctx, double, int *) { return fail(ctx, PIMC_E_STATE, "long range not built"); }
-int pimc_get_kvecs(pimc_context *ctx, double *) { return fail(ctx, PIMC_E_STATE, "long range not built"); }
-int pimc_set_longrange(pimc_context *ctx, int, const double *, const double *, const double *, const double *,
-                       const double *, const double *, const double *, const double *, int) {
-  return fail(ctx, PIMC_E_STATE, "long range not built");
+// PathClass::SetupkVecs3D (PathClass.cc:534-586), one species.
+int pimc_setup_kvecs(pimc_context *ctx, double kcutoff, int *num_k) {
+  if (!ctx || !num_k || !(kcutoff > 0.0)) return fail(ctx, PIMC_E_ARG, "bad kcutoff");
+  CK(cudaSetDevice(ctx->device));
+  for (int i = 0; i < 3; i++) ctx->kbox[i] = 2.0 * M_PI / ctx->sys.box[i];
+  for (int i = 0; i < 3; i++) ctx->kmax[i] = (int)std::ceil(1.1 * kcutoff / ctx->kbox[i]);
+  for (int i = 0; i < 3; i++)
+    if (ctx->kmax[i] > 64) return fail(ctx, PIMC_E_ARG, "kCutoff too large (more than 64 k-points per dimension)");
+  std::vector<int3> kidx;
+  ctx->kvecs.clear();
+  for (int ix = -ctx->kmax[0]; ix <= ctx->kmax[0]; ix++) {
+    const double k0 = ix * ctx->kbox[0];
+    for (int iy = -ctx->kmax[1]; iy <= ctx->kmax[1]; iy++) {
+      const double k1 = iy * ctx->kbox[1];
+      for (int iz = -ctx->kmax[2]; iz <= ctx->kmax[2]; iz++) {
+        const double k2 = iz * ctx->kbox[2];
+        // the half-space of PathClass Include() (PathClass.cc:281-292)
+        const bool include = (k0 > 0.0) || (k0 == 0.0 && k1 > 0.0) || (k0 == 0.0 && k1 == 0.0 && k2 > 0.0);
+        if ((k0 * k0 + k1 * k1 + k2 * k2 < kcutoff * kcutoff) && include) {
+          ctx->kvecs.push_back(k0);
+          ctx->kvecs.push_back(k1);
+          ctx->kvecs.push_back(k2);
+          kidx.push_back(make_int3(ix + ctx->kmax[0], iy + ctx->kmax[1], iz + ctx->kmax[2]));
+        }
+      }
+    }
+  }
+  if (kidx.size() > 1024) return fail(ctx, PIMC_E_ARG, "more than 1024 k-vectors");
+  ctx->num_k = (int)kidx.size();
+  ctx->kcutoff = kcutoff;
+  cudaFree(ctx->d_kidx);
+  cudaFree(ctx->d_rhok[0]);
+  cudaFree(ctx->d_rhok[1]);
+  ctx->d_kidx = nullptr;
+  ctx->d_rhok[0] = ctx->d_rhok[1] = nullptr;
+  if (ctx->num_k > 0) {
+    CK(cudaMalloc(&ctx->d_kidx, kidx.size() * sizeof(int3)));
+    CK(cudaMemcpy(ctx->d_kidx, kidx.data(), kidx.size() * sizeof(int3), cudaMemcpyHostToDevice));
+    for (int c = 0; c < 2; c++) {
+      CK(cudaMalloc(&ctx->d_rhok[c], (size_t)ctx->sys.S * ctx->num_k * sizeof(double2)));
+      CK(cudaMemset(ctx->d_rhok[c], 0, (size_t)ctx->sys.S * ctx->num_k * sizeof(double2)));
+    }
+  }
+  *num_k = ctx->num_k;
+  return PIMC_OK;
 }
-int pimc_calc_rhok(pimc_context *ctx) { return fail(ctx, PIMC_E_STATE, "long range not built"); }
-int pimc_update_rhok(pimc_context *ctx, int, int, const int *, int, int) {
-  return fail(ctx, PIMC_E_STATE, "long range not built");
+
+int pimc_get_kvecs(pimc_context *ctx, double *kvecs) {
+  if (!ctx || !kvecs) return PIMC_E_ARG;
+  std::memcpy(kvecs, ctx->kvecs.data(), ctx->kvecs.size() * sizeof(double));
+  return PIMC_OK;
 }
-int pimc_get_rhok(pimc_context *ctx, int, double *) { return fail(ctx, PIMC_E_STATE, "long range not built"); }
+
+int pimc_set_longrange(pimc_context *ctx, int num_levels, const double *ulong_k, const double *ulong_r0,
+                       const double *ushort_k0, const double *ulong_k0, const double *dulong_k,
+                       const double *dulong_r0, const double *dushort_k0, const double *dulong_k0,
+                       int use_background) {
+  if (!ctx) return PIMC_E_ARG;
+  if (ctx->num_k <= 0) return fail(ctx, PIMC_E_STATE, "pimc_setup_kvecs not called");
+  if (num_levels < 1 || !ulong_k || !ulong_r0 || !ushort_k0 || !ulong_k0 || !dulong_k || !dulong_r0 ||
+      !dushort_k0 || !dulong_k0)
+    return fail(ctx, PIMC_E_ARG, "bad long-range tables");
+  CK(cudaSetDevice(ctx->device));
+  const size_t n = (size_t)num_levels * ctx->num_k;
+  cudaFree(ctx->d_ulong_k);
+  cudaFree(ctx->d_dulong_k);
+  ctx->d_ulong_k = ctx->d_dulong_k = nullptr;
+  CK(cudaMalloc(&ctx->d_ulong_k, n * sizeof(double)));
+  CK(cudaMalloc(&ctx->d_dulong_k, n * sizeof(double)));
+  CK(cudaMemcpy(ctx->d_ulong_k, ulong_k, n * sizeof(double), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(ctx->d_dulong_k, dulong_k, n * sizeof(double), cudaMemcpyHostToDevice));
+  ctx->ulong_r0.assign(ulong_r0, ulong_r0 + num_levels);
+  ctx->ushort_k0.assign(ushort_k0, ushort_k0 + num_levels);
+  ctx->ulong_k0.assign(ulong_k0, ulong_k0 + num_levels);
+  ctx->dulong_r0.assign(dulong_r0, dulong_r0 + num_levels);
+  ctx->dushort_k0.assign(dushort_k0, dushort_k0 + num_levels);
+  ctx->dulong_k0.assign(dulong_k0, dulong_k0 + num_levels);
+  ctx->lr_levels = num_levels;
+  ctx->use_background = use_background;
+  ctx->lr_ready = true;
+  return PIMC_OK;
+}
+
+// PathClass::UpdateRho_ks() full recompute (PathClass.cc:710-718): OLD, then NEW = OLD.
+int pimc_calc_rhok(pimc_context *ctx) {
+  if (!ctx) return PIMC_E_ARG;
+  if (ctx->num_k <= 0) return fail(ctx, PIMC_E_STATE, "pimc_setup_kvecs not called");
+  CK(cudaSetDevice(ctx->device));
+  CK(launch_rhok_full(ctx->stream, ctx->d_path[0], ctx->sys.N, ctx->sys.S, lr_desc(ctx), ctx->d_rhok[0]));
+  CK(cudaMemcpyAsync(ctx->d_rhok[1], ctx->d_rhok[0], (size_t)ctx->sys.S * ctx->num_k * sizeof(double2),
+                     cudaMemcpyDeviceToDevice, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  return PIMC_OK;
+}
+
+int pimc_update_rhok(pimc_context *ctx, int slice1, int slice2, const int *active, int n_active, int level) {
+  if (!ctx) return PIMC_E_ARG;
+  if (ctx->num_k <= 0) return fail(ctx, PIMC_E_STATE, "pimc_setup_kvecs not called");
+  int rc = check_slices(ctx, slice1, slice2, level, true);
+  if (rc) return rc;
+  ActiveList act;
+  if ((rc = check_active(ctx, active, n_active, act))) return rc;
+  CK(cudaSetDevice(ctx->device));
+  CK(launch_rhok_update(ctx->stream, ctx->d_path[0], ctx->d_path[1], ctx->sys.N, lr_desc(ctx), act, slice1, slice2,
+                        1 << level, ctx->d_rhok[0], ctx->d_rhok[1]));
+  CK(cudaStreamSynchronize(ctx->stream));
+  return PIMC_OK;
+}
+
+int pimc_get_rhok(pimc_context *ctx, int copy, double *out) {
+  if (!ctx || !out || copy < 0 || copy > 1) return PIMC_E_ARG;
+  if (ctx->num_k <= 0) return fail(ctx, PIMC_E_STATE, "pimc_setup_kvecs not called");
+  CK(cudaSetDevice(ctx->device));
+  CK(cudaMemcpy(out, ctx->d_rhok[copy], (size_t)ctx->sys.S * ctx->num_k * sizeof(double2), cudaMemcpyDeviceToHost));
+  return PIMC_OK;
+}
 
 }  // extern "C"

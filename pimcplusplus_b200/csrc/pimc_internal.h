@@ -147,8 +147,17 @@ struct pimc_context {
   pimc_move_record *d_trace = nullptr;
   size_t trace_cap = 0;
   int sm_count = 0;
-  // long range
+  // long range (one species): k-vectors, rho_k [copy][slice][k], breakup tables
   int num_k = 0;
   double kcutoff = 0;
+  int kmax[3] = {0, 0, 0};
+  double kbox[3] = {0, 0, 0};
+  std::vector<double> kvecs;  // [k][3]
+  int3 *d_kidx = nullptr;
+  double2 *d_rhok[2] = {nullptr, nullptr};
+  bool lr_ready = false;
+  int lr_levels = 0, use_background = 0;
+  double *d_ulong_k = nullptr, *d_dulong_k = nullptr;  // [levels][k]
+  std::vector<double> ulong_r0, ushort_k0, ulong_k0, dulong_r0, dushort_k0, dulong_k0;
   std::string last_error;
 };
