@@ -227,6 +227,47 @@ int pimc_synchronize(pimc_context *ctx);
 /* The CUDA stream of the context (cudaStream_t as void*). */
 void *pimc_stream(pimc_context *ctx);
 
+/* ---- many independent chains in one persistent launch ----
+ * The reference runs independent Markov chains as clones, one per MPI
+ * group (PathDataClass.cc:244-268).  Here a batch holds chains of uneven
+ * N, M and tau, each a sequential-schedule BisectionBlock driver with a
+ * DavidPA diagonal action u_00(r; tau_l) (no off-diagonal terms) on its own
+ * linear grid; one launch runs n_blocks blocks of moves on every chain, the
+ * chains taken by CTAs from an atomic queue, largest first. */
+typedef struct pimc_batch pimc_batch;
+
+typedef struct pimc_chain_desc {
+  int num_particles;        /* N */
+  int num_time_slices;      /* path rows, M+1 */
+  double box[3];
+  double tau;
+  double lambda;            /* hbar^2/(2m), one species */
+  int num_images;
+  int num_levels;           /* Move{NumLevels} */
+  int steps_per_block;      /* Move{StepsPerBlock} */
+  uint64_t seed;            /* Local stream key */
+  double grid_start, grid_end;
+  int num_grid;
+  int num_tau;              /* tables for tau * 2^l, l = 0..num_tau-1 */
+  int tau_pos;              /* level of this chain's tau in the tables */
+  const double *u00;        /* [num_tau][num_grid] diagonal action (host) */
+  const double *path;       /* [num_time_slices][N][3] initial path (host) */
+} pimc_chain_desc;
+
+int pimc_batch_create(int device, int n_chains, const pimc_chain_desc *chains, pimc_batch **out);
+int pimc_batch_destroy(pimc_batch *b);
+int pimc_batch_last_error(pimc_batch *b, char *buf, int len);
+/* precision: PIMC_FP64 or PIMC_MIXED; threads_per_cta 64..256 (0 = 128);
+ * ctas: persistent CTAs (0 = every CTA that fits, capped at the chain count). */
+int pimc_batch_config(pimc_batch *b, int precision, int shadow, int threads_per_cta, int ctas);
+/* n_blocks blocks of moves on every chain; trace: [chain][n_blocks*steps]
+ * records (chains with fewer steps leave zeros) or NULL; stats: totals. */
+int pimc_batch_run(pimc_batch *b, int n_blocks, pimc_move_record *trace, pimc_bisection_stats *stats);
+int pimc_batch_run_async(pimc_batch *b, int n_blocks);
+int pimc_batch_get_stats(pimc_batch *b, int chain /* -1: all */, pimc_bisection_stats *stats);
+int pimc_batch_get_path(pimc_batch *b, int chain, double *path);
+int pimc_batch_synchronize(pimc_batch *b);
+
 /* ---- allocation-free ShortRange SingleAction ----
  * No counterpart in the reference: it exists for callers that cannot call
  * cudaMalloc (an application whose memory pool owns every device

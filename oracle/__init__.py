@@ -50,6 +50,7 @@ def lib():
         "oracle_philox_uniform": (d, [u64, u32, u64]),
         "oracle_philox_block": (None, [C.POINTER(C.c_uint32), C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)]),
         "oracle_pa_david_from_dm": (p, [C.c_char_p, d, i]),
+        "oracle_pa_david_arrays": (p, [d, d, i, i, i, dp, dp, i, i]),
         "oracle_pa_tricubic": (p, [d, d, i, d, d, i, d, d, i, i, d, dp, dp, d, d, i, dp]),
         "oracle_pa_classical_coulomb": (p, [d, i, d]),
         "oracle_pa_free": (None, [p]),
@@ -133,6 +134,14 @@ class PairAction:
     @classmethod
     def from_dm(cls, path: str, desired_tau: float, num_offdiag_terms: int = 0):
         return cls(lib().oracle_pa_david_from_dm(path.encode(), desired_tau, num_offdiag_terms))
+
+    @classmethod
+    def david_arrays(cls, grid_start, grid_end, ukj, dukj, tau_pos=0, num_offdiag_terms=0):
+        ukj = np.ascontiguousarray(ukj, dtype=np.float64)
+        dukj = np.ascontiguousarray(dukj, dtype=np.float64)
+        nt, ng, nc = ukj.shape
+        return cls(lib().oracle_pa_david_arrays(grid_start, grid_end, ng, nc, nt, _dp(ukj), _dp(dukj), tau_pos,
+                                                num_offdiag_terms))
 
     @classmethod
     def tricubic(cls, qgrid, ygrid, tgrid, smallest_beta, umat, dumat, pot_grid, pot_data):

@@ -650,6 +650,28 @@ OraclePA *oracle_pa_david_from_dm(const char *path, double desired_tau, int num_
   return pa;
 }
 
+// DavidPAClass tables from arrays on a LINEAR grid: ukj/dukj [tau][grid][ncols]
+// (column 0 the potential), splines built like ReadDavidSquarerFile does.
+OraclePA *oracle_pa_david_arrays(double grid_start, double grid_end, int n, int ncols, int ntau, const double *ukj,
+                                 const double *dukj, int tau_pos, int num_terms) {
+  OraclePA *pa = new OraclePA();
+  pa->kind = 1;
+  pa->NumTerms = num_terms;
+  pa->NumTau = ntau;
+  pa->TauPos = tau_pos;
+  pa->NumUKJ = ncols - 1;
+  pa->ugrid.InitLinear(grid_start, grid_end, n);
+  pa->dugrid = pa->ugrid;
+  std::vector<double> sd(ncols, 5.0e30), ed(ncols, 0.0);
+  pa->ukj.assign(ntau, MultiSpline());
+  pa->dukj.assign(ntau, MultiSpline());
+  for (int lev = 0; lev < ntau; lev++) {
+    pa->ukj[lev].Init(&pa->ugrid, ukj + (size_t)lev * n * ncols, ncols, sd.data(), ed.data());
+    pa->dukj[lev].Init(&pa->dugrid, dukj + (size_t)lev * n * ncols, ncols, sd.data(), ed.data());
+  }
+  return pa;
+}
+
 OraclePA *oracle_pa_tricubic(double q0, double q1, int nq, double y0, double y1, int ny, double t0,
                              double t1, int nt, int num_betas, double smallest_beta, const double *umat,
                              const double *dumat, double pot_start, double pot_end, int pot_n,

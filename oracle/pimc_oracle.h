@@ -40,6 +40,9 @@ void oracle_philox_block(const uint32_t ctr[4], const uint32_t key[2], uint32_t 
 /* ---- Pair actions ---- */
 /* Reads an ASCII squarer .dm file (DavidPAClass::ReadDavidSquarerFile). */
 OraclePA *oracle_pa_david_from_dm(const char *path, double desired_tau, int num_offdiag_terms);
+/* DavidPAClass tables from arrays on a LINEAR grid: ukj/dukj [tau][grid][ncols]. */
+OraclePA *oracle_pa_david_arrays(double grid_start, double grid_end, int n, int ncols, int ntau, const double *ukj,
+                                 const double *dukj, int tau_pos, int num_terms);
 /* PAtricubicFitClass with a SplinePot potential (PAtricubicFit.cc:794-865). */
 OraclePA *oracle_pa_tricubic(double q0, double q1, int nq, double y0, double y1, int ny,
                              double t0, double t1, int nt, int num_betas, double smallest_beta,

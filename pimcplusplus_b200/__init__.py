@@ -77,6 +77,27 @@ class BisectionDesc(C.Structure):
     ]
 
 
+class ChainDesc(C.Structure):
+    _fields_ = [
+        ("num_particles", C.c_int),
+        ("num_time_slices", C.c_int),
+        ("box", C.c_double * 3),
+        ("tau", C.c_double),
+        ("lambda_", C.c_double),
+        ("num_images", C.c_int),
+        ("num_levels", C.c_int),
+        ("steps_per_block", C.c_int),
+        ("seed", C.c_uint64),
+        ("grid_start", C.c_double),
+        ("grid_end", C.c_double),
+        ("num_grid", C.c_int),
+        ("num_tau", C.c_int),
+        ("tau_pos", C.c_int),
+        ("u00", C.POINTER(C.c_double)),
+        ("path", C.POINTER(C.c_double)),
+    ]
+
+
 class BisectionStats(C.Structure):
     _fields_ = [
         ("moves", C.c_int64),
@@ -131,6 +152,15 @@ _SIGS = {
     "pimc_bisection_occupancy": (_i, [_p, _ip]),
     "pimc_synchronize": (_i, [_p]),
     "pimc_stream": (_p, [_p]),
+    "pimc_batch_create": (_i, [_i, _i, C.POINTER(ChainDesc), C.POINTER(_p)]),
+    "pimc_batch_destroy": (_i, [_p]),
+    "pimc_batch_last_error": (_i, [_p, C.c_char_p, _i]),
+    "pimc_batch_config": (_i, [_p, _i, _i, _i, _i]),
+    "pimc_batch_run": (_i, [_p, _i, _p, C.POINTER(BisectionStats)]),
+    "pimc_batch_run_async": (_i, [_p, _i]),
+    "pimc_batch_get_stats": (_i, [_p, _i, C.POINTER(BisectionStats)]),
+    "pimc_batch_get_path": (_i, [_p, _i, _dp]),
+    "pimc_batch_synchronize": (_i, [_p]),
     "pimc_shortrange_single_noalloc": (_i, [_p, _i, _i, _dp, _p, _d, _d, _i, _i, _i, _ip, _i, _i, _p, _p]),
 }
 for _name, (_res, _args) in _SIGS.items():
@@ -407,3 +437,89 @@ class BisectionBlock:
         st = BisectionStats()
         self.PathData._check(_lib.pimc_bisection_get_stats(self.PathData.h, C.byref(st)), "get_stats")
         return st.as_dict()
+
+
+class BatchChains:
+    """Many independent chains (the reference's clones) advanced by one
+    persistent launch of the device BisectionBlock driver.
+
+    chains: list of dicts with keys N, slices, box, tau, lam, num_levels,
+    steps_per_block, seed, grid (start, end, n), u00 [num_tau][n], tau_pos,
+    path [slices][N][3], num_images (optional).
+    """
+
+    def __init__(self, chains, device=0, precision=MIXED, shadow=False, threads_per_cta=0, ctas=0):
+        self._keep = []
+        descs = (ChainDesc * len(chains))()
+        self.shapes = []
+        for i, c in enumerate(chains):
+            u00 = np.ascontiguousarray(c["u00"], dtype=np.float64)
+            path = np.ascontiguousarray(c["path"], dtype=np.float64)
+            self._keep += [u00, path]
+            d = descs[i]
+            d.num_particles = c["N"]
+            d.num_time_slices = c["slices"]
+            for k in range(3):
+                d.box[k] = c["box"][k]
+            d.tau = c["tau"]
+            d.lambda_ = c["lam"]
+            d.num_images = c.get("num_images", 0)
+            d.num_levels = c["num_levels"]
+            d.steps_per_block = c["steps_per_block"]
+            d.seed = c["seed"]
+            d.grid_start, d.grid_end, d.num_grid = c["grid"][0], c["grid"][1], int(c["grid"][2])
+            d.num_tau = u00.shape[0]
+            d.tau_pos = c.get("tau_pos", 0)
+            d.u00 = _dptr(u00)
+            d.path = _dptr(path)
+            self.shapes.append(path.shape)
+        h = _p()
+        rc = _lib.pimc_batch_create(device, len(chains), descs, C.byref(h))
+        if rc:
+            raise PimcError(rc, "pimc_batch_create")
+        self.h = h
+        self.n = len(chains)
+        self.steps = max(c["steps_per_block"] for c in chains)
+        self.config(precision, shadow, threads_per_cta, ctas)
+
+    def _check(self, rc, what):
+        if rc:
+            buf = C.create_string_buffer(512)
+            _lib.pimc_batch_last_error(self.h, buf, 512)
+            raise PimcError(rc, f"{what}: {buf.value.decode(errors='replace')}")
+
+    def config(self, precision=MIXED, shadow=False, threads_per_cta=0, ctas=0):
+        self._check(_lib.pimc_batch_config(self.h, precision, int(shadow), threads_per_cta, ctas), "batch_config")
+
+    def run(self, n_blocks, trace=False):
+        st = BisectionStats()
+        rec = np.zeros(self.n * n_blocks * self.steps, dtype=MOVE_RECORD) if trace else None
+        ptr = rec.ctypes.data_as(_p) if trace else None
+        self._check(_lib.pimc_batch_run(self.h, n_blocks, ptr, C.byref(st)), "batch_run")
+        if trace:
+            rec = rec.reshape(self.n, n_blocks * self.steps)
+        return rec, st.as_dict()
+
+    def run_async(self, n_blocks):
+        self._check(_lib.pimc_batch_run_async(self.h, n_blocks), "batch_run_async")
+
+    def synchronize(self):
+        self._check(_lib.pimc_batch_synchronize(self.h), "batch_synchronize")
+
+    def stats(self, chain=-1):
+        st = BisectionStats()
+        self._check(_lib.pimc_batch_get_stats(self.h, chain, C.byref(st)), "batch_get_stats")
+        return st.as_dict()
+
+    def path(self, chain):
+        out = np.empty(self.shapes[chain])
+        self._check(_lib.pimc_batch_get_path(self.h, chain, _dptr(out)), "batch_get_path")
+        return out
+
+    def close(self):
+        if getattr(self, "h", None):
+            _lib.pimc_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()

@@ -1,0 +1,338 @@
+// Batched independent chains (the reference's clone parallelism,
+// PathDataClass.cc:244-268, on one GPU): C ABI over batch_kernel.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <new>
+#include <numeric>
+#include <string>
+#include <vector>
+
+#include "bisection.cuh"
+#include "pimc_internal.h"
+
+using namespace pimc;
+
+struct pimc_batch {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  int n_chains = 0;
+  std::vector<pimc_chain_desc> desc;
+  std::vector<size_t> path_off;  // doubles
+  std::vector<BisectionArgs> jobs;
+  double *d_paths = nullptr;
+  size_t path_doubles = 0;
+  std::vector<void *> owned;
+  BisectionArgs *d_jobs = nullptr;
+  int *d_order = nullptr;
+  unsigned int *d_queue = nullptr;
+  ChainState *d_chains = nullptr;
+  pimc_move_record *d_trace = nullptr;
+  size_t trace_cap = 0;
+  int precision = PIMC_MIXED, shadow = 0, threads = 128;
+  size_t dyn = 0;
+  int blocks = 0;
+  int sm_count = 0;
+  std::string last_error;
+};
+
+namespace {
+
+int bfail(pimc_batch *b, int code, const std::string &msg) {
+  if (b) b->last_error = msg;
+  return code;
+}
+
+#define BCK(call)                                                                               \
+  do {                                                                                          \
+    cudaError_t e_ = (call);                                                                    \
+    if (e_ != cudaSuccess) return bfail(b, PIMC_E_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+  } while (0)
+
+template <typename T>
+int bupload(pimc_batch *b, const std::vector<T> &host, const T **dev) {
+  void *p = nullptr;
+  BCK(cudaMalloc(&p, host.size() * sizeof(T) + 16));
+  b->owned.push_back(p);
+  BCK(cudaMemset(p, 0, host.size() * sizeof(T) + 16));
+  BCK(cudaMemcpy(p, host.data(), host.size() * sizeof(T), cudaMemcpyHostToDevice));
+  *dev = static_cast<const T *>(p);
+  return PIMC_OK;
+}
+
+// The diagonal DavidPA column of one chain: (y, d2y) pairs per level, the
+// natural-start / zero-end-slope spline of DavidPAClass (DavidPAClass.cc:760-763).
+template <typename R>
+int build_diag(pimc_batch *b, const pimc_chain_desc &c, const HostGrid &g, DDavid<R> &d) {
+  d.grid.type = PIMC_GRID_LINEAR;
+  d.grid.n = g.n;
+  d.grid.start = (R)g.start;
+  d.grid.end = (R)g.end;
+  d.grid.delta = (R)g.delta;
+  d.grid.deltainv = (R)g.deltainv;
+  d.grid.r0 = 0;
+  d.grid.log_spacing = 0;
+  d.grid.x = nullptr;
+  d.ncols = 2;
+  d.num_tau = c.num_tau;
+  d.tau_pos = c.tau_pos;
+  d.num_terms = 0;
+  d.uy = d.ud2 = d.duy = d.dud2 = nullptr;
+  d.diag_stride = (g.n + 1) & ~1;
+  std::vector<R> diag((size_t)c.num_tau * d.diag_stride * 2, (R)0);
+  std::vector<double> d2(g.n);
+  for (int lev = 0; lev < c.num_tau; lev++) {
+    const double *y = c.u00 + (size_t)lev * g.n;
+    spline_second_derivs(g, y, 1, 0, 5.0e30, 0.0, d2.data());
+    for (int i = 0; i < g.n; i++) {
+      diag[((size_t)lev * d.diag_stride + i) * 2] = (R)y[i];
+      diag[((size_t)lev * d.diag_stride + i) * 2 + 1] = (R)d2[i];
+    }
+  }
+  return bupload(b, diag, &d.diag);
+}
+
+}  // namespace
+
+extern "C" {
+
+int pimc_batch_create(int device, int n_chains, const pimc_chain_desc *chains, pimc_batch **out) {
+  if (!out || !chains || n_chains < 1) return PIMC_E_ARG;
+  *out = nullptr;
+  pimc_batch *b = new (std::nothrow) pimc_batch();
+  if (!b) return PIMC_E_NOMEM;
+  b->device = device;
+  b->n_chains = n_chains;
+  b->desc.assign(chains, chains + n_chains);
+  cudaError_t e = cudaSetDevice(device);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&b->sm_count, cudaDevAttrMultiProcessorCount, device);
+  if (e != cudaSuccess) {
+    pimc_batch_destroy(b);
+    return PIMC_E_CUDA;
+  }
+  // validate and lay out the paths
+  size_t total = 0;
+  size_t maxdyn = 0;
+  for (int i = 0; i < n_chains; i++) {
+    const pimc_chain_desc &c = chains[i];
+    if (c.num_particles < 2 || c.num_particles > (1 << 20) || c.num_time_slices < 3 || !c.path || !c.u00 ||
+        !(c.tau > 0.0) || c.num_images < 0 || c.num_levels < 1 || c.num_levels > 6 ||
+        (1 << c.num_levels) >= c.num_time_slices || c.steps_per_block < 1 || c.num_grid < 3 ||
+        !(c.grid_end > c.grid_start) || c.num_tau < 1 || c.tau_pos < 0 || c.tau_pos + c.num_levels > c.num_tau) {
+      int rc = bfail(b, PIMC_E_ARG, "chain " + std::to_string(i) + ": bad description");
+      pimc_batch_destroy(b);
+      return rc;
+    }
+    for (int d = 0; d < 3; d++)
+      if (!(c.box[d] > 0.0)) {
+        pimc_batch_destroy(b);
+        return PIMC_E_ARG;
+      }
+    b->path_off.push_back(total);
+    total += (size_t)c.num_time_slices * c.num_particles * 3;
+    const size_t stride = (size_t)((c.num_grid + 1) & ~1);
+    maxdyn = std::max(maxdyn, (size_t)c.num_levels * stride * sizeof(double2));
+  }
+  b->path_doubles = total;
+  b->dyn = maxdyn;  // FP64 pairs; the FP32 run needs half
+  e = cudaMalloc(&b->d_paths, total * sizeof(double));
+  if (e == cudaSuccess) e = cudaMalloc(&b->d_chains, n_chains * sizeof(ChainState));
+  if (e == cudaSuccess) e = cudaMemset(b->d_chains, 0, n_chains * sizeof(ChainState));
+  if (e == cudaSuccess) e = cudaMalloc(&b->d_jobs, n_chains * sizeof(BisectionArgs));
+  if (e == cudaSuccess) e = cudaMalloc(&b->d_order, n_chains * sizeof(int));
+  if (e == cudaSuccess) e = cudaMalloc(&b->d_queue, sizeof(unsigned int));
+  if (e != cudaSuccess) {
+    pimc_batch_destroy(b);
+    return PIMC_E_CUDA;
+  }
+  std::vector<ChainState> cs(n_chains);
+  b->jobs.resize(n_chains);
+  for (int i = 0; i < n_chains; i++) {
+    const pimc_chain_desc &c = chains[i];
+    e = cudaMemcpy(b->d_paths + b->path_off[i], c.path,
+                   (size_t)c.num_time_slices * c.num_particles * 3 * sizeof(double), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) {
+      pimc_batch_destroy(b);
+      return PIMC_E_CUDA;
+    }
+    HostGrid g;
+    g.init_linear(c.grid_start, c.grid_end, c.num_grid);
+    BisectionArgs &j = b->jobs[i];
+    std::memset(&j, 0, sizeof(j));
+    j.path = b->d_paths + b->path_off[i];
+    DevSystem &s = j.sys;
+    s.N = c.num_particles;
+    s.S = c.num_time_slices;
+    for (int d = 0; d < 3; d++) {
+      s.box[d] = c.box[d];
+      s.boxinv[d] = 1.0 / c.box[d];
+    }
+    s.tau = c.tau;
+    s.lambda = c.lambda;
+    s.num_images = c.num_images;
+    j.pa.kind = PA_DAVID;
+    int rc = build_diag<double>(b, c, g, j.pa.d64);
+    if (!rc) rc = build_diag<float>(b, c, g, j.pa.d32);
+    if (rc) {
+      pimc_batch_destroy(b);
+      return rc;
+    }
+    j.chains = b->d_chains + i;
+    j.num_levels = c.num_levels;
+    j.steps_per_block = c.steps_per_block;
+    j.sr_higher = 1;
+    j.concurrent = 0;
+    cs[i].seed = c.seed;
+    cs[i].stream = kStreamLocal;
+  }
+  // largest chains first: cost ~ N * 2^L * StepsPerBlock
+  std::vector<int> order(n_chains);
+  std::iota(order.begin(), order.end(), 0);
+  std::stable_sort(order.begin(), order.end(), [&](int x, int y) {
+    const double cx = (double)chains[x].num_particles * (1 << chains[x].num_levels) * chains[x].steps_per_block;
+    const double cy = (double)chains[y].num_particles * (1 << chains[y].num_levels) * chains[y].steps_per_block;
+    return cx > cy;
+  });
+  e = cudaMemcpy(b->d_jobs, b->jobs.data(), n_chains * sizeof(BisectionArgs), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(b->d_order, order.data(), n_chains * sizeof(int), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(b->d_chains, cs.data(), n_chains * sizeof(ChainState), cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) {
+    pimc_batch_destroy(b);
+    return PIMC_E_CUDA;
+  }
+  *out = b;
+  return PIMC_OK;
+}
+
+int pimc_batch_destroy(pimc_batch *b) {
+  if (!b) return PIMC_E_ARG;
+  cudaSetDevice(b->device);
+  if (b->stream) cudaStreamSynchronize(b->stream);
+  for (void *p : b->owned) cudaFree(p);
+  cudaFree(b->d_paths);
+  cudaFree(b->d_chains);
+  cudaFree(b->d_jobs);
+  cudaFree(b->d_order);
+  cudaFree(b->d_queue);
+  cudaFree(b->d_trace);
+  if (b->stream) cudaStreamDestroy(b->stream);
+  delete b;
+  return PIMC_OK;
+}
+
+int pimc_batch_last_error(pimc_batch *b, char *buf, int len) {
+  if (!b || !buf || len <= 0) return PIMC_E_ARG;
+  std::snprintf(buf, (size_t)len, "%s", b->last_error.c_str());
+  return PIMC_OK;
+}
+
+int pimc_batch_config(pimc_batch *b, int precision, int shadow, int threads_per_cta, int ctas) {
+  if (!b) return PIMC_E_ARG;
+  if (precision != PIMC_FP64 && precision != PIMC_MIXED) return bfail(b, PIMC_E_ARG, "bad precision");
+  if (threads_per_cta != 0 && (threads_per_cta < 64 || threads_per_cta > 256 || threads_per_cta % 32))
+    return bfail(b, PIMC_E_ARG, "threads_per_cta must be a multiple of 32 in 64..256");
+  if (ctas < 0) return bfail(b, PIMC_E_ARG, "ctas must be >= 0");
+  BCK(cudaSetDevice(b->device));
+  b->precision = precision;
+  b->shadow = shadow;
+  b->threads = threads_per_cta ? threads_per_cta : 128;
+  const size_t dyn = precision == PIMC_MIXED ? b->dyn / 2 + 16 : b->dyn;
+  int per_sm = 0;
+  BCK(batch_occupancy(precision, shadow, b->threads, dyn, &per_sm));
+  if (per_sm < 1) return bfail(b, PIMC_E_ARG, "configuration does not fit on an SM");
+  b->blocks = ctas ? ctas : std::min(b->n_chains, per_sm * b->sm_count);
+  return PIMC_OK;
+}
+
+static int batch_launch(pimc_batch *b, int n_blocks, pimc_move_record *dtrace, long long per_chain) {
+  if (b->blocks == 0) {
+    int rc = pimc_batch_config(b, b->precision, b->shadow, b->threads, 0);
+    if (rc) return rc;
+  }
+  BCK(cudaMemsetAsync(b->d_queue, 0, sizeof(unsigned int), b->stream));
+  BatchArgs a;
+  a.jobs = b->d_jobs;
+  a.order = b->d_order;
+  a.queue = b->d_queue;
+  a.n_chains = b->n_chains;
+  a.n_blocks = n_blocks;
+  a.trace = dtrace;
+  a.trace_per_chain = per_chain;
+  const size_t dyn = b->precision == PIMC_MIXED ? b->dyn / 2 + 16 : b->dyn;
+  BCK(launch_batch(a, b->precision, b->shadow, b->blocks, b->threads, dyn, b->stream));
+  return PIMC_OK;
+}
+
+int pimc_batch_run_async(pimc_batch *b, int n_blocks) {
+  if (!b || n_blocks < 0) return PIMC_E_ARG;
+  BCK(cudaSetDevice(b->device));
+  return batch_launch(b, n_blocks, nullptr, 0);
+}
+
+int pimc_batch_run(pimc_batch *b, int n_blocks, pimc_move_record *trace, pimc_bisection_stats *stats) {
+  if (!b || n_blocks < 0) return PIMC_E_ARG;
+  BCK(cudaSetDevice(b->device));
+  int spb = 0;
+  for (const auto &c : b->desc) spb = std::max(spb, c.steps_per_block);
+  const long long per_chain = (long long)n_blocks * spb;
+  const size_t nrec = (size_t)per_chain * b->n_chains;
+  if (trace && nrec > b->trace_cap) {
+    cudaFree(b->d_trace);
+    b->d_trace = nullptr;
+    b->trace_cap = 0;
+    BCK(cudaMalloc(&b->d_trace, nrec * sizeof(pimc_move_record)));
+    b->trace_cap = nrec;
+  }
+  if (trace) BCK(cudaMemsetAsync(b->d_trace, 0, nrec * sizeof(pimc_move_record), b->stream));
+  int rc = batch_launch(b, n_blocks, trace ? b->d_trace : nullptr, per_chain);
+  if (rc) return rc;
+  if (trace) BCK(cudaMemcpyAsync(trace, b->d_trace, nrec * sizeof(pimc_move_record), cudaMemcpyDeviceToHost, b->stream));
+  BCK(cudaStreamSynchronize(b->stream));
+  pimc_bisection_stats st;
+  rc = pimc_batch_get_stats(b, -1, &st);
+  if (rc) return rc;
+  if (stats) *stats = st;
+  if (st.status) return bfail(b, st.status, std::string("device status: ") + pimc_status_string(st.status));
+  return PIMC_OK;
+}
+
+int pimc_batch_get_stats(pimc_batch *b, int chain, pimc_bisection_stats *stats) {
+  if (!b || !stats || chain < -1 || chain >= b->n_chains) return PIMC_E_ARG;
+  BCK(cudaSetDevice(b->device));
+  std::vector<ChainState> cs(b->n_chains);
+  BCK(cudaMemcpyAsync(cs.data(), b->d_chains, cs.size() * sizeof(ChainState), cudaMemcpyDeviceToHost, b->stream));
+  BCK(cudaStreamSynchronize(b->stream));
+  std::memset(stats, 0, sizeof(*stats));
+  for (int i = 0; i < b->n_chains; i++) {
+    if (chain >= 0 && i != chain) continue;
+    const ChainState &c = cs[i];
+    stats->moves += (int64_t)c.moves;
+    stats->accepted += (int64_t)c.accepted;
+    stats->stages_attempted += (int64_t)c.stages;
+    stats->pair_evals += (int64_t)c.pair_evals;
+    stats->flips += (int64_t)c.flips;
+    if (c.status && !stats->status) stats->status = c.status;
+  }
+  return PIMC_OK;
+}
+
+int pimc_batch_get_path(pimc_batch *b, int chain, double *path) {
+  if (!b || !path || chain < 0 || chain >= b->n_chains) return PIMC_E_ARG;
+  BCK(cudaSetDevice(b->device));
+  const pimc_chain_desc &c = b->desc[chain];
+  BCK(cudaMemcpy(path, b->d_paths + b->path_off[chain],
+                 (size_t)c.num_time_slices * c.num_particles * 3 * sizeof(double), cudaMemcpyDeviceToHost));
+  return PIMC_OK;
+}
+
+int pimc_batch_synchronize(pimc_batch *b) {
+  if (!b) return PIMC_E_ARG;
+  BCK(cudaSetDevice(b->device));
+  BCK(cudaStreamSynchronize(b->stream));
+  return PIMC_OK;
+}
+
+}  // extern "C"

@@ -307,27 +307,43 @@ __device__ __forceinline__ void rng_store(RngSnap &s, const DevRandom &r) {
 //    the move ends at this stage (a rejection, or acceptance at level 0),
 //    unless the accepted particle was drawn again, whose window changes.
 // The draw order is therefore exactly the reference's.
+// Shared state of one CTA while it runs a job.
+struct KernelShared {
+  double win_old[2][kMaxWindow][3], win_new[2][kMaxWindow][3];
+  double gbuf[2][3 * 32];
+  double sh_red[16][4];  // per warp: S_old, S_new, and their shadows
+  double xchg[2][kMaxCluster][4];
+  double s_logsr[kMaxLevels], s_logu[kMaxLevels];
+  int s_ctl[4];   // slice1, ptcl, stage accepted, status
+  int s_next[4];  // next move speculated: valid, slice1, ptcl
+  double s_next_f[2];
+  RngSnap s_rng, s_spec1, s_spec2;
+};
+
+// The moves of one job — one chain, or one window of a chain — on this CTA
+// (cluster rank `rank` of `CL`).  `phase` is the parity of the table-staging
+// mbarrier `bar`, flipped once per staging.
 template <int KIND, typename R, bool SHADOW>
-__global__ void __launch_bounds__(512, 1) bisection_kernel(BisectionArgs a) {
+__device__ void run_job(const BisectionArgs &a, ChainState *cs, int window, unsigned rank, unsigned CL,
+                        cg::cluster_group &cluster, unsigned char *dyn, KernelShared &S, uint64_t *bar_ptr,
+                        unsigned &phase) {
   typedef typename Pair2<R>::T P2;
   typedef typename std::conditional<std::is_same<R, double>::value, float, double>::type RS;  // shadow precision
   typedef typename Pair2<RS>::T P2S;
-  __shared__ double win_old[2][kMaxWindow][3], win_new[2][kMaxWindow][3];
-  __shared__ double gbuf[2][3 * 32];
-  __shared__ double sh_red[16][4];  // per warp: S_old, S_new, and their shadows
-  __shared__ double xchg[2][kMaxCluster][4];
-  __shared__ double s_logsr[kMaxLevels], s_logu[kMaxLevels];
-  __shared__ int s_ctl[4];   // slice1, ptcl, stage accepted, status
-  __shared__ int s_next[4];  // next move speculated: valid, slice1, ptcl
-  __shared__ double s_next_f[2];
-  __shared__ RngSnap s_rng, s_spec1, s_spec2;
-  __shared__ __align__(8) uint64_t s_bar;
-  extern __shared__ __align__(16) unsigned char dyn[];
-
-  cg::cluster_group cluster = cg::this_cluster();
-  const unsigned rank = cluster.block_rank();
-  const unsigned CL = cluster.num_blocks();
-  const int window = (int)(blockIdx.x / CL);
+  auto &win_old = S.win_old;
+  auto &win_new = S.win_new;
+  auto &gbuf = S.gbuf;
+  auto &sh_red = S.sh_red;
+  auto &xchg = S.xchg;
+  auto &s_logsr = S.s_logsr;
+  auto &s_logu = S.s_logu;
+  auto &s_ctl = S.s_ctl;
+  auto &s_next = S.s_next;
+  auto &s_next_f = S.s_next_f;
+  auto &s_rng = S.s_rng;
+  auto &s_spec1 = S.s_spec1;
+  auto &s_spec2 = S.s_spec2;
+  uint64_t &s_bar = *bar_ptr;
   const int tid = threadIdx.x;
   const int lane = tid & 31, warp = tid >> 5;
   const int nwarps = blockDim.x >> 5;
@@ -339,7 +355,6 @@ __global__ void __launch_bounds__(512, 1) bisection_kernel(BisectionArgs a) {
   const int N = sys.N;
   const int L = a.num_levels;
   const int span = 1 << L;
-  ChainState *cs = a.chains + (a.concurrent ? window : 0);
   const bool lead = (rank == 0 && tid == 0);
 
   // ---- stage the diagonal DavidPA columns into shared memory (bulk TMA) ----
@@ -353,9 +368,8 @@ __global__ void __launch_bounds__(512, 1) bisection_kernel(BisectionArgs a) {
     const unsigned bytes = (unsigned)(L * d.diag_stride * sizeof(P2));
     unsigned bytes_s = 0;
     if (SHADOW) bytes_s = (unsigned)(L * david_of<RS>(a.pa).diag_stride * sizeof(P2S));
+    __syncthreads();  // the previous job's readers of the staged tables are done
     if (tid == 0) {
-      mbar_init(&s_bar, 1);
-      asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
       asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
       mbar_expect_tx(&s_bar, bytes + bytes_s);
       bulk_g2s(dyn, reinterpret_cast<const P2 *>(d.diag) + (size_t)d.tau_pos * d.diag_stride, bytes, &s_bar);
@@ -368,22 +382,26 @@ __global__ void __launch_bounds__(512, 1) bisection_kernel(BisectionArgs a) {
     __syncthreads();
     int ok = 0;
     for (int it = 0; it < (1 << 22); it++)
-      if (mbar_try_wait(&s_bar, 0)) {
+      if (mbar_try_wait(&s_bar, phase)) {
         ok = 1;
         break;
       }
     ok = __syncthreads_and(ok);
-    if (tid < (int)CL) cluster.map_shared_rank(&xchg[1][rank][0], tid)[0] = ok ? 1.0 : 0.0;
-    cluster.sync();
-    int all_ok = 1;
-    for (unsigned r = 0; r < CL; r++) all_ok &= (xchg[1][r][0] != 0.0);
+    int all_ok = ok;
+    if (CL > 1) {
+      if (tid < (int)CL) cluster.map_shared_rank(&xchg[1][rank][0], tid)[0] = ok ? 1.0 : 0.0;
+      cluster.sync();
+      for (unsigned r = 0; r < CL; r++) all_ok &= (xchg[1][r][0] != 0.0);
+    }
     if (!all_ok) {
       // Give a late copy a second bounded chance to land before this CTA exits.
-      for (int it = 0; it < (1 << 22) && !ok; it++) ok = mbar_try_wait(&s_bar, 0);
+      for (int it = 0; it < (1 << 22) && !ok; it++) ok = mbar_try_wait(&s_bar, phase);
       if (lead) atomicExch(&cs->status, PIMC_E_CAP);
-      cluster.sync();
+      if (CL > 1) cluster.sync();
+      phase ^= 1u;
       return;
     }
+    phase ^= 1u;
     diag_smem = reinterpret_cast<const P2 *>(dyn);
     if (SHADOW) diag_smem_s = reinterpret_cast<const P2S *>(dyn + bytes);
   }
@@ -416,11 +434,11 @@ __global__ void __launch_bounds__(512, 1) bisection_kernel(BisectionArgs a) {
           r.ptcl = -1;
           a.trace[a.trace_offset + (long long)window * a.steps_per_block + st] = r;
         }
-      if (KIND == PA_DAVID) cluster.sync();  // xchg[1] no longer read by peers
+      if (KIND == PA_DAVID && CL > 1) cluster.sync();  // xchg[1] no longer read by peers
       return;
     }
   }
-  if (KIND == PA_DAVID) cluster.sync();  // every CTA has read xchg[1]
+  if (KIND == PA_DAVID && CL > 1) cluster.sync();  // every CTA has read xchg[1]
   __syncthreads();
   const int numLeft = sys.S - span;
   const int total_moves = (a.concurrent ? 1 : a.n_blocks) * a.steps_per_block;
@@ -651,7 +669,72 @@ __global__ void __launch_bounds__(512, 1) bisection_kernel(BisectionArgs a) {
     if (status) cs->status = status;
   }
   if (CL > 1) cluster.sync();
+  __syncthreads();
 }
+
+// One chain on a thread-block cluster: the sequential schedule (one launch
+// runs n_blocks blocks), or one round of the concurrent-window schedule
+// (cluster w works window w).
+template <int KIND, typename R, bool SHADOW>
+__global__ void __launch_bounds__(512, 1) bisection_kernel(BisectionArgs a) {
+  __shared__ KernelShared S;
+  __shared__ __align__(8) uint64_t s_bar;
+  extern __shared__ __align__(16) unsigned char dyn[];
+  cg::cluster_group cluster = cg::this_cluster();
+  const unsigned rank = cluster.block_rank();
+  const unsigned CL = cluster.num_blocks();
+  const int window = (int)(blockIdx.x / CL);
+  if (threadIdx.x == 0) {
+    mbar_init(&s_bar, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  unsigned phase = 0;
+  ChainState *cs = a.chains + (a.concurrent ? window : 0);
+  run_job<KIND, R, SHADOW>(a, cs, window, rank, CL, cluster, dyn, S, &s_bar, phase);
+}
+
+// Many independent chains in one persistent launch (the reference's clone
+// parallelism): each CTA takes the next chain from an atomic queue (chains
+// ordered by estimated cost, largest first), copies its job description to
+// shared memory, stages its tables and runs all of its moves for this
+// launch, then takes the next one.
+template <int KIND, typename R, bool SHADOW>
+__global__ void __launch_bounds__(256, 2) batch_kernel(BatchArgs b) {
+  __shared__ KernelShared S;
+  __shared__ BisectionArgs job;
+  __shared__ int s_chain;
+  __shared__ __align__(8) uint64_t s_bar;
+  extern __shared__ __align__(16) unsigned char dyn[];
+  cg::cluster_group cluster = cg::this_cluster();
+  if (threadIdx.x == 0) {
+    mbar_init(&s_bar, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  unsigned phase = 0;
+  for (int guard = 0; guard < b.n_chains + 1; guard++) {
+    if (threadIdx.x == 0) s_chain = (int)atomicAdd(b.queue, 1u);
+    __syncthreads();
+    const int c = s_chain;
+    if (c >= b.n_chains) break;
+    const int chain = b.order[c];
+    {
+      const int *src = reinterpret_cast<const int *>(b.jobs + chain);
+      int *dst = reinterpret_cast<int *>(&job);
+      for (int i = threadIdx.x; i < (int)(sizeof(BisectionArgs) / sizeof(int)); i += blockDim.x) dst[i] = src[i];
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      job.n_blocks = b.n_blocks;
+      job.trace = b.trace ? b.trace + (long long)chain * b.trace_per_chain : nullptr;
+      job.trace_offset = 0;
+    }
+    __syncthreads();
+    run_job<KIND, R, SHADOW>(job, job.chains, 0, 0, 1, cluster, dyn, S, &s_bar, phase);
+  }
+}
+
 
 template <int KIND, typename R, bool SHADOW>
 static cudaError_t launch_t(const BisectionArgs &a, int cl, int clusters, int threads, size_t dyn, cudaStream_t st) {
@@ -714,6 +797,42 @@ cudaError_t bisection_occupancy(const BisectionArgs &a, int precision, int shado
                            : occupancy_t<PA_TRICUBIC, float, false>(cl, threads, dyn, max_clusters);
   return shadow ? occupancy_t<PA_TRICUBIC, double, true>(cl, threads, dyn, max_clusters)
                 : occupancy_t<PA_TRICUBIC, double, false>(cl, threads, dyn, max_clusters);
+}
+
+template <int KIND, typename R, bool SHADOW>
+static cudaError_t launch_batch_t(const BatchArgs &b, int blocks, int threads, size_t dyn, cudaStream_t st) {
+  auto kfn = batch_kernel<KIND, R, SHADOW>;
+  cudaError_t e = cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn);
+  if (e != cudaSuccess) return e;
+  kfn<<<blocks, threads, dyn, st>>>(b);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_batch(const BatchArgs &b, int precision, int shadow, int blocks, int threads, size_t dyn,
+                         cudaStream_t st) {
+  if (dyn > (size_t)100 * 1024) return cudaErrorInvalidValue;  // two CTAs per SM must fit
+  if (threads < 64 || threads > 256 || threads % 32 || blocks < 1) return cudaErrorInvalidValue;
+  if (precision == PIMC_MIXED)
+    return shadow ? launch_batch_t<PA_DAVID, float, true>(b, blocks, threads, dyn, st)
+                  : launch_batch_t<PA_DAVID, float, false>(b, blocks, threads, dyn, st);
+  return shadow ? launch_batch_t<PA_DAVID, double, true>(b, blocks, threads, dyn, st)
+                : launch_batch_t<PA_DAVID, double, false>(b, blocks, threads, dyn, st);
+}
+
+template <int KIND, typename R, bool SHADOW>
+static cudaError_t batch_occupancy_t(int threads, size_t dyn, int *blocks_per_sm) {
+  auto kfn = batch_kernel<KIND, R, SHADOW>;
+  cudaError_t e = cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn);
+  if (e != cudaSuccess) return e;
+  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, kfn, threads, dyn);
+}
+
+cudaError_t batch_occupancy(int precision, int shadow, int threads, size_t dyn, int *blocks_per_sm) {
+  if (precision == PIMC_MIXED)
+    return shadow ? batch_occupancy_t<PA_DAVID, float, true>(threads, dyn, blocks_per_sm)
+                  : batch_occupancy_t<PA_DAVID, float, false>(threads, dyn, blocks_per_sm);
+  return shadow ? batch_occupancy_t<PA_DAVID, double, true>(threads, dyn, blocks_per_sm)
+                : batch_occupancy_t<PA_DAVID, double, false>(threads, dyn, blocks_per_sm);
 }
 
 size_t bisection_dyn_smem(const BisectionArgs &a, int precision, int shadow) {

@@ -21,6 +21,23 @@ struct BisectionArgs {
 
 cudaError_t bisection_occupancy(const BisectionArgs &a, int precision, int shadow, int cluster_ctas, int threads,
                                 int *max_clusters);
+// Many chains in one persistent launch: jobs[] (one sequential-schedule job
+// per chain, each with its own path, tables and ChainState), taken in the
+// order order[] through the atomic counter *queue (zero at launch).
+struct BatchArgs {
+  const BisectionArgs *jobs;
+  const int *order;
+  unsigned int *queue;
+  int n_chains;
+  int n_blocks;                 // blocks of moves each chain runs in this launch
+  pimc_move_record *trace;      // [chain][n_blocks * steps_per_block] or nullptr
+  long long trace_per_chain;
+};
+
+cudaError_t launch_batch(const BatchArgs &b, int precision, int shadow, int blocks, int threads, size_t dyn,
+                         cudaStream_t st);
+cudaError_t batch_occupancy(int precision, int shadow, int threads, size_t dyn, int *blocks_per_sm);
+
 size_t bisection_dyn_smem(const BisectionArgs &a, int precision, int shadow);
 cudaError_t launch_bisection(const BisectionArgs &a, int precision, int shadow, int cluster_ctas, int clusters,
                              int threads, cudaStream_t st);

@@ -141,3 +141,46 @@ def make_dm_for(cfg, directory, r_min=1.5):
     path = os.path.join(directory, f"lj_{cfg['N']}_{cfg['M']}.dm")
     write_primitive_dm(path, r_min, box[0] / 2.0, cfg["npts"], tau, cfg["levels"] + 1, pot)
     return path
+
+
+def lj_chain(n, m, temp, rho, levels, seed, steps_per_block=1, npts=200, r_min=1.5, rng=None):
+    """One LJ He-4 chain for the batched driver: its diagonal primitive
+    action u_00(r; tau_l) = tau_l V(r) on a linear grid [r_min, L/2] (last
+    point zeroed as the .dm reader does) and a seeded initial path."""
+    tau = 1.0 / (temp * m)
+    box = box_for_density(n, rho)
+    r = r_min + np.arange(npts) * ((box[0] / 2.0 - r_min) / (npts - 1))
+    v = lj(r)
+    taus = tau * 2.0 ** np.arange(levels + 1)
+    u00 = taus[:, None] * v[None, :]
+    u00[:, -1] = 0.0
+    rng = rng or np.random.default_rng(seed)
+    pts = np.zeros((n, 3))
+    for i in range(n):
+        for _ in range(1000):
+            c = (rng.random(3) - 0.5) * box
+            d = pts[:i] - c
+            d -= np.round(d / box) * box
+            if i == 0 or np.min(np.sum(d * d, axis=1)) >= (0.9 * LJ_SIGMA) ** 2:
+                break
+        pts[i] = c
+    path = np.repeat(pts[None], m + 1, axis=0)
+    return dict(N=n, slices=m + 1, box=box, tau=tau, lam=HE4_LAMBDA, num_levels=levels,
+                steps_per_block=steps_per_block, seed=seed, grid=(r_min, float(box[0] / 2.0), npts), u00=u00,
+                tau_pos=0, path=path)
+
+
+def c3_chains(count, seed=0, steps_per_block=1, npts=200):
+    """Config C3: chains with N in {32..512}, M in {16..128}, T in [1,4] K,
+    density in [0.018, 0.024] A^-3, level chosen so 2^L <= M/2 (at most 4)."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(count):
+        n = int(rng.choice([32, 64, 128, 256, 512]))
+        m = int(rng.choice([16, 32, 64, 128]))
+        temp = float(rng.uniform(1.0, 4.0))
+        rho = float(rng.uniform(0.018, 0.024))
+        levels = min(4, int(np.log2(m)) - 1)
+        out.append(lj_chain(n, m, temp, rho, levels, seed=1000 + i, steps_per_block=steps_per_block, npts=npts,
+                            rng=np.random.default_rng(1000 + i)))
+    return out

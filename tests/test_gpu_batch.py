@@ -1,0 +1,69 @@
+"""Many independent chains in one persistent launch against the oracle:
+each chain's accept trace and final path must equal its own sequential
+oracle run (FP64), whatever CTA ran it and in whatever order."""
+import numpy as np
+import pytest
+
+import oracle as O
+import pimcplusplus_b200 as P
+from pimcplusplus_b200 import workloads as W
+
+pytestmark = pytest.mark.gpu
+
+
+def make_chains():
+    rng = np.random.default_rng(77)
+    chains = []
+    for i in range(12):
+        n = int(rng.choice([16, 24, 40]))
+        m = int(rng.choice([8, 16, 32]))
+        levels = 2 if m == 8 else 3
+        chains.append(W.lj_chain(n, m, float(rng.uniform(1.0, 4.0)), 0.02186, levels, seed=500 + i,
+                                 steps_per_block=2, npts=200, rng=np.random.default_rng(500 + i)))
+    return chains
+
+
+def oracle_run(c, n_blocks):
+    ng = c["grid"][2]
+    nt = c["u00"].shape[0]
+    ukj = np.zeros((nt, ng, 2))
+    ukj[:, :, 1] = c["u00"]
+    pa = O.PairAction.david_arrays(c["grid"][0], c["grid"][1], ukj, np.zeros_like(ukj), 0, 0)
+    s = O.System(c["N"], c["slices"], c["box"], c["tau"], c["lam"], 0)
+    s.set_pa(pa)
+    s.set_path(c["path"])
+    s.bisection_config(c["num_levels"], c["steps_per_block"])
+    s.rng_seed(c["seed"])
+    recs = s.run_bisection(n_blocks)
+    return recs, s.get_path(0), pa
+
+
+@pytest.mark.parametrize("threads", [64, 128, 256])
+def test_batch_matches_oracle_per_chain(threads):
+    chains = make_chains()
+    b = P.BatchChains(chains, precision=P.FP64, threads_per_cta=threads, ctas=5)
+    n_blocks = 25
+    trace, stats = b.run(n_blocks, trace=True)
+    total = 0
+    for i, c in enumerate(chains):
+        ref, ref_path, _ = oracle_run(c, n_blocks)
+        got = trace[i]
+        for k, r in enumerate(ref):
+            g = got[k]
+            assert (r.slice1, r.ptcl, r.accepted, r.stages_passed) == (
+                int(g["slice1"]), int(g["ptcl"]), int(g["accepted"]), int(g["stages_passed"])), (i, k)
+            for j in range(8):
+                assert abs(r.dS[j] - g["dS"][j]) <= 1e-9 * max(1.0, abs(r.dS[j])), (i, k, j)
+        assert np.max(np.abs(b.path(i) - ref_path)) < 1e-9, i
+        total += len(ref)
+    assert stats["moves"] == total and stats["status"] == 0
+    b.close()
+
+
+def test_batch_mixed_runs_and_accepts():
+    chains = make_chains()
+    b = P.BatchChains(chains, precision=P.MIXED, threads_per_cta=128)
+    _, stats = b.run(40)
+    assert stats["status"] == 0
+    assert 0.02 < stats["accepted"] / stats["moves"] < 0.98
+    b.close()
