@@ -94,6 +94,16 @@ int build_diag(pimc_batch *b, const pimc_chain_desc &c, const HostGrid &g, DDavi
   return bupload(b, diag, &d.diag);
 }
 
+// Shared memory for the staged tables: the working precision's column plus,
+// with the shadow evaluation, the other precision's (FP32 pairs are half the
+// FP64 bytes).
+size_t batch_dyn(const pimc_batch *b) {
+  const size_t b64 = b->dyn, b32 = b->dyn / 2;
+  size_t d = b->precision == PIMC_MIXED ? b32 : b64;
+  if (b->shadow) d += b->precision == PIMC_MIXED ? b64 : b32;
+  return d + 16;
+}
+
 }  // namespace
 
 extern "C" {
@@ -137,7 +147,7 @@ int pimc_batch_create(int device, int n_chains, const pimc_chain_desc *chains, p
     maxdyn = std::max(maxdyn, (size_t)c.num_levels * stride * sizeof(double2));
   }
   b->path_doubles = total;
-  b->dyn = maxdyn;  // FP64 pairs; the FP32 run needs half
+  b->dyn = maxdyn;  // FP64 pairs; see batch_dyn for the other configurations
   e = cudaMalloc(&b->d_paths, total * sizeof(double));
   if (e == cudaSuccess) e = cudaMalloc(&b->d_chains, n_chains * sizeof(ChainState));
   if (e == cudaSuccess) e = cudaMemset(b->d_chains, 0, n_chains * sizeof(ChainState));
@@ -239,7 +249,7 @@ int pimc_batch_config(pimc_batch *b, int precision, int shadow, int threads_per_
   b->precision = precision;
   b->shadow = shadow;
   b->threads = threads_per_cta ? threads_per_cta : 128;
-  const size_t dyn = precision == PIMC_MIXED ? b->dyn / 2 + 16 : b->dyn;
+  const size_t dyn = batch_dyn(b);
   int per_sm = 0;
   BCK(batch_occupancy(precision, shadow, b->threads, dyn, &per_sm));
   if (per_sm < 1) return bfail(b, PIMC_E_ARG, "configuration does not fit on an SM");
@@ -261,7 +271,7 @@ static int batch_launch(pimc_batch *b, int n_blocks, pimc_move_record *dtrace, l
   a.n_blocks = n_blocks;
   a.trace = dtrace;
   a.trace_per_chain = per_chain;
-  const size_t dyn = b->precision == PIMC_MIXED ? b->dyn / 2 + 16 : b->dyn;
+  const size_t dyn = batch_dyn(b);
   BCK(launch_batch(a, b->precision, b->shadow, b->blocks, b->threads, dyn, b->stream));
   return PIMC_OK;
 }

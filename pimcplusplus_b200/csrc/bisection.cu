@@ -368,6 +368,12 @@ __device__ void run_job(const BisectionArgs &a, ChainState *cs, int window, unsi
     const unsigned bytes = (unsigned)(L * d.diag_stride * sizeof(P2));
     unsigned bytes_s = 0;
     if (SHADOW) bytes_s = (unsigned)(L * david_of<RS>(a.pa).diag_stride * sizeof(P2S));
+    unsigned dyn_size;
+    asm("mov.u32 %0, %%dynamic_smem_size;" : "=r"(dyn_size));
+    if (bytes + bytes_s > dyn_size) {  // uniform over the cluster: same job, same launch
+      if (lead) atomicExch(&cs->status, PIMC_E_CAP);
+      return;
+    }
     __syncthreads();  // the previous job's readers of the staged tables are done
     if (tid == 0) {
       asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
