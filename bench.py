@@ -348,6 +348,8 @@ def run_ours(args):
         dist.all_reduce(v)
         e2e_evals_timed = float(v.item())
 
+    c3 = None if args.no_c3 else run_c3(args, P, torch, flush, local, rank, world, agg)
+
     if rank == 0:
         peak, peak_kind = load_peaks()
         value = st32["pair_evals"] / (ms32 / 1000.0)
@@ -396,6 +398,9 @@ def run_ours(args):
                          "kernel": "bisection_kernel<PA_TRICUBIC,float>"},
             "clocks": clocks,
         }
+        if c3:
+            line["c3"] = c3
+            line["gpu_launches"] += c3.pop("_launches")
         if cpu:
             line["cpu_baseline"] = {"value": cpu["value"], "unit": UNIT, "cores": cpu["cores"], "kind": "port",
                                     "sample": cpu["sample"]}
@@ -403,6 +408,101 @@ def run_ours(args):
     if dist:
         dist.barrier()
         dist.destroy_process_group()
+
+
+def run_c3(args, P, torch, flush, local, rank, world, agg):
+    """Batched uneven chains (one persistent launch per step, replayed from a
+    CUDA graph) in mixed and FP64 precision, beside the plain FP64 path: the
+    same kind of chains advanced one at a time by the single-chain driver."""
+    from pimcplusplus_b200 import workloads as W
+
+    chains = W.c3_chains(args.c3_chains, seed=rank, steps_per_block=args.c3_steps_per_block)
+    nb = args.c3_blocks
+
+    def timed_batch(precision):
+        b = P.BatchChains(chains, device=local, precision=precision)
+        tune = b.autotune(nb)
+        stream = torch.cuda.ExternalStream(b.stream, device=f"cuda:{local}")
+        for _ in range(args.warmup):
+            b.run_async(nb)
+        b.synchronize()
+        s0 = b.stats()
+        times = []
+        torch.cuda.synchronize()
+        for _ in range(args.steps):
+            with torch.cuda.stream(stream):
+                flush.zero_()
+                e0 = torch.cuda.Event(enable_timing=True)
+                e1 = torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                b.run_async(nb)
+                e1.record(stream)
+            e1.synchronize()
+            times.append(e0.elapsed_time(e1))
+        s1 = b.stats()
+        if s1["status"]:
+            raise RuntimeError(f"batch device status {s1['status']}")
+        b.close()
+        st = {k: s1[k] - s0[k] for k in ("moves", "accepted", "pair_evals", "stages_attempted")}
+        ms, st = agg(float(np.sum(times)), st)
+        return ms, st, tune
+
+    ms32, st32, tune32 = timed_batch(P.MIXED)
+    ms64, st64, tune64 = timed_batch(P.FP64)
+
+    # plain path: chains one at a time through the single-chain device driver
+    def plain(precision, sample):
+        tot_ms, acc, mv, ev = 0.0, 0, 0, 0
+        for c in sample:
+            d = P.PathData(c["N"], c["slices"], c["box"], c["tau"], c["lam"], 0, device=local)
+            ng = c["grid"][2]
+            ukj = np.zeros((c["u00"].shape[0], ng, 2))
+            ukj[:, :, 1] = c["u00"]
+            d.pa_david(P.GRID_LINEAR, c["grid"][0], c["grid"][1], ukj, np.zeros_like(ukj), 0, 0)
+            d.set_path(c["path"])
+            bb = P.BisectionBlock(d, c["num_levels"], c["steps_per_block"], precision=precision,
+                                  schedule=P.SEQUENTIAL)
+            bb.seed(c["seed"])
+            bb.MakeMoves(1, trace=False)
+            stream = torch.cuda.ExternalStream(P.lib().pimc_stream(d.h), device=f"cuda:{local}")
+            s0 = bb.stats()
+            with torch.cuda.stream(stream):
+                e0 = torch.cuda.Event(enable_timing=True)
+                e1 = torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                bb.launch_async(nb)
+                e1.record(stream)
+            e1.synchronize()
+            s1 = bb.stats()
+            tot_ms += e0.elapsed_time(e1)
+            acc += s1["accepted"] - s0["accepted"]
+            mv += s1["moves"] - s0["moves"]
+            ev += s1["pair_evals"] - s0["pair_evals"]
+            d.close()
+        return tot_ms, dict(accepted=acc, moves=mv, pair_evals=ev)
+
+    sample = chains[: args.c3_plain_sample]
+    pms64, pst64 = agg(*plain(P.FP64, sample))
+    pms32, pst32 = agg(*plain(P.MIXED, sample))
+
+    def rates(ms, st):
+        s = ms / 1000.0
+        return {"accepted_moves_per_s": st["accepted"] / s, "moves_per_s": st["moves"] / s,
+                "pair_evals_per_s": st["pair_evals"] / s}
+
+    r32, r64, p64, p32 = rates(ms32, st32), rates(ms64, st64), rates(pms64, pst64), rates(pms32, pst32)
+    return {
+        "workload": f"{len(chains)} LJ He-4 chains, N in {{32..512}}, M in {{16..128}}, T in [1,4] K, "
+                    f"rho in [0.018,0.024], primitive u00 on 1000 points, level <= 4, "
+                    f"{nb * args.c3_steps_per_block} moves per chain per step",
+        "batched_mixed": dict(r32, ms_per_step=ms32 / args.steps, autotune=tune32),
+        "batched_fp64": dict(r64, ms_per_step=ms64 / args.steps, autotune=tune64),
+        "plain_fp64": dict(p64, chains_sampled=len(sample), note="one chain at a time, single-chain driver"),
+        "plain_mixed": dict(p32, chains_sampled=len(sample)),
+        "batched_mixed_over_plain_fp64": r32["accepted_moves_per_s"] / p64["accepted_moves_per_s"],
+        "batched_mixed_over_batched_fp64": r32["accepted_moves_per_s"] / r64["accepted_moves_per_s"],
+        "_launches": 2 * args.steps,
+    }
 
 
 def nb_launches(schedule, blocks):
@@ -424,6 +524,11 @@ def main():
     ap.add_argument("--accuracy-moves", type=int, default=1000)
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-c3", action="store_true")
+    ap.add_argument("--c3-chains", type=int, default=1024)
+    ap.add_argument("--c3-blocks", type=int, default=4)
+    ap.add_argument("--c3-steps-per-block", type=int, default=4)
+    ap.add_argument("--c3-plain-sample", type=int, default=32)
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)

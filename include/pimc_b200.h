@@ -263,10 +263,20 @@ int pimc_batch_config(pimc_batch *b, int precision, int shadow, int threads_per_
 /* n_blocks blocks of moves on every chain; trace: [chain][n_blocks*steps]
  * records (chains with fewer steps leave zeros) or NULL; stats: totals. */
 int pimc_batch_run(pimc_batch *b, int n_blocks, pimc_move_record *trace, pimc_bisection_stats *stats);
+/* Enqueues n_blocks blocks of moves on every chain, no sync.  The launch is
+ * captured once as a CUDA graph and replayed while n_blocks and the
+ * configuration stay the same. */
 int pimc_batch_run_async(pimc_batch *b, int n_blocks);
+/* Times n_blocks blocks under each candidate threads_per_cta (64..256) with
+ * every CTA that fits or one CTA per SM, keeps the fastest with the current
+ * precision and shadow setting, and puts the chains back in their state
+ * from before the probes.  Outputs may be NULL. */
+int pimc_batch_autotune(pimc_batch *b, int n_blocks, int *threads_per_cta, int *ctas, double *ms);
 int pimc_batch_get_stats(pimc_batch *b, int chain /* -1: all */, pimc_bisection_stats *stats);
 int pimc_batch_get_path(pimc_batch *b, int chain, double *path);
 int pimc_batch_synchronize(pimc_batch *b);
+/* The batch's CUDA stream (cudaStream_t) for event timing and ordering. */
+void *pimc_batch_stream(pimc_batch *b);
 
 /* ---- allocation-free ShortRange SingleAction ----
  * No counterpart in the reference: it exists for callers that cannot call

@@ -158,9 +158,11 @@ _SIGS = {
     "pimc_batch_config": (_i, [_p, _i, _i, _i, _i]),
     "pimc_batch_run": (_i, [_p, _i, _p, C.POINTER(BisectionStats)]),
     "pimc_batch_run_async": (_i, [_p, _i]),
+    "pimc_batch_autotune": (_i, [_p, _i, C.POINTER(_i), C.POINTER(_i), C.POINTER(C.c_double)]),
     "pimc_batch_get_stats": (_i, [_p, _i, C.POINTER(BisectionStats)]),
     "pimc_batch_get_path": (_i, [_p, _i, _dp]),
     "pimc_batch_synchronize": (_i, [_p]),
+    "pimc_batch_stream": (_p, [_p]),
     "pimc_shortrange_single_noalloc": (_i, [_p, _i, _i, _dp, _p, _d, _d, _i, _i, _i, _ip, _i, _i, _p, _p]),
 }
 for _name, (_res, _args) in _SIGS.items():
@@ -505,6 +507,16 @@ class BatchChains:
 
     def synchronize(self):
         self._check(_lib.pimc_batch_synchronize(self.h), "batch_synchronize")
+
+    @property
+    def stream(self):
+        return _lib.pimc_batch_stream(self.h)
+
+    def autotune(self, n_blocks=1):
+        """Pick threads_per_cta and the CTA count by timing; chains keep their state."""
+        t, c, ms = _i(), _i(), C.c_double()
+        self._check(_lib.pimc_batch_autotune(self.h, n_blocks, C.byref(t), C.byref(c), C.byref(ms)), "batch_autotune")
+        return dict(threads_per_cta=t.value, ctas=c.value, ms=ms.value)
 
     def stats(self, chain=-1):
         st = BisectionStats()

@@ -35,6 +35,11 @@ struct pimc_batch {
   size_t dyn = 0;
   int blocks = 0;
   int sm_count = 0;
+  // the launch (queue reset + persistent kernel) captured as a CUDA graph,
+  // valid for graph_blocks blocks of moves under configuration cfg_version
+  cudaGraphExec_t graph = nullptr;
+  int graph_blocks = -1;
+  int cfg_version = 0, graph_version = -1;
   std::string last_error;
 };
 
@@ -62,10 +67,14 @@ int bupload(pimc_batch *b, const std::vector<T> &host, const T **dev) {
   return PIMC_OK;
 }
 
-// The diagonal DavidPA column of one chain: (y, d2y) pairs per level, the
-// natural-start / zero-end-slope spline of DavidPAClass (DavidPAClass.cc:760-763).
+// The diagonal DavidPA column of one chain, appended to `host` (R pairs):
+// (y, d2y) per grid point and level, the natural-start / zero-end-slope
+// spline of DavidPAClass (DavidPAClass.cc:760-763).  Every chain's block
+// starts at a multiple of 2 pairs so a level's bulk copy stays 16-byte
+// aligned.  d.diag receives the OFFSET in pairs; it is rebased once the
+// packed array is on the device.
 template <typename R>
-int build_diag(pimc_batch *b, const pimc_chain_desc &c, const HostGrid &g, DDavid<R> &d) {
+void build_diag(const pimc_chain_desc &c, const HostGrid &g, std::vector<R> &host, DDavid<R> &d) {
   d.grid.type = PIMC_GRID_LINEAR;
   d.grid.n = g.n;
   d.grid.start = (R)g.start;
@@ -81,17 +90,30 @@ int build_diag(pimc_batch *b, const pimc_chain_desc &c, const HostGrid &g, DDavi
   d.num_terms = 0;
   d.uy = d.ud2 = d.duy = d.dud2 = nullptr;
   d.diag_stride = (g.n + 1) & ~1;
-  std::vector<R> diag((size_t)c.num_tau * d.diag_stride * 2, (R)0);
+  const size_t base = host.size() / 2;  // pairs
+  host.resize(host.size() + (size_t)c.num_tau * d.diag_stride * 2, (R)0);
   std::vector<double> d2(g.n);
   for (int lev = 0; lev < c.num_tau; lev++) {
     const double *y = c.u00 + (size_t)lev * g.n;
     spline_second_derivs(g, y, 1, 0, 5.0e30, 0.0, d2.data());
+    R *o = host.data() + (base + (size_t)lev * d.diag_stride) * 2;
     for (int i = 0; i < g.n; i++) {
-      diag[((size_t)lev * d.diag_stride + i) * 2] = (R)y[i];
-      diag[((size_t)lev * d.diag_stride + i) * 2 + 1] = (R)d2[i];
+      o[2 * i] = (R)y[i];
+      o[2 * i + 1] = (R)d2[i];
     }
   }
-  return bupload(b, diag, &d.diag);
+  d.diag = reinterpret_cast<const R *>(base);
+}
+
+template <typename R>
+void rebase_diag(DDavid<R> &d, const R *dev) {
+  d.diag = dev + 2 * reinterpret_cast<size_t>(d.diag);
+}
+
+void drop_graph(pimc_batch *b) {
+  if (b->graph) cudaGraphExecDestroy(b->graph);
+  b->graph = nullptr;
+  b->graph_blocks = -1;
 }
 
 // Shared memory for the staged tables: the working precision's column plus,
@@ -159,6 +181,8 @@ int pimc_batch_create(int device, int n_chains, const pimc_chain_desc *chains, p
     return PIMC_E_CUDA;
   }
   std::vector<ChainState> cs(n_chains);
+  std::vector<double> diag64;
+  std::vector<float> diag32;
   b->jobs.resize(n_chains);
   for (int i = 0; i < n_chains; i++) {
     const pimc_chain_desc &c = chains[i];
@@ -184,12 +208,8 @@ int pimc_batch_create(int device, int n_chains, const pimc_chain_desc *chains, p
     s.lambda = c.lambda;
     s.num_images = c.num_images;
     j.pa.kind = PA_DAVID;
-    int rc = build_diag<double>(b, c, g, j.pa.d64);
-    if (!rc) rc = build_diag<float>(b, c, g, j.pa.d32);
-    if (rc) {
-      pimc_batch_destroy(b);
-      return rc;
-    }
+    build_diag<double>(c, g, diag64, j.pa.d64);
+    build_diag<float>(c, g, diag32, j.pa.d32);
     j.chains = b->d_chains + i;
     j.num_levels = c.num_levels;
     j.steps_per_block = c.steps_per_block;
@@ -197,6 +217,20 @@ int pimc_batch_create(int device, int n_chains, const pimc_chain_desc *chains, p
     j.concurrent = 0;
     cs[i].seed = c.seed;
     cs[i].stream = kStreamLocal;
+  }
+  {
+    const double *p64 = nullptr;
+    const float *p32 = nullptr;
+    int rc = bupload(b, diag64, &p64);
+    if (!rc) rc = bupload(b, diag32, &p32);
+    if (rc) {
+      pimc_batch_destroy(b);
+      return rc;
+    }
+    for (auto &j : b->jobs) {
+      rebase_diag(j.pa.d64, p64);
+      rebase_diag(j.pa.d32, p32);
+    }
   }
   // largest chains first: cost ~ N * 2^L * StepsPerBlock
   std::vector<int> order(n_chains);
@@ -221,6 +255,7 @@ int pimc_batch_destroy(pimc_batch *b) {
   if (!b) return PIMC_E_ARG;
   cudaSetDevice(b->device);
   if (b->stream) cudaStreamSynchronize(b->stream);
+  drop_graph(b);
   for (void *p : b->owned) cudaFree(p);
   cudaFree(b->d_paths);
   cudaFree(b->d_chains);
@@ -254,6 +289,7 @@ int pimc_batch_config(pimc_batch *b, int precision, int shadow, int threads_per_
   BCK(batch_occupancy(precision, shadow, b->threads, dyn, &per_sm));
   if (per_sm < 1) return bfail(b, PIMC_E_ARG, "configuration does not fit on an SM");
   b->blocks = ctas ? ctas : std::min(b->n_chains, per_sm * b->sm_count);
+  b->cfg_version++;
   return PIMC_OK;
 }
 
@@ -279,7 +315,101 @@ static int batch_launch(pimc_batch *b, int n_blocks, pimc_move_record *dtrace, l
 int pimc_batch_run_async(pimc_batch *b, int n_blocks) {
   if (!b || n_blocks < 0) return PIMC_E_ARG;
   BCK(cudaSetDevice(b->device));
-  return batch_launch(b, n_blocks, nullptr, 0);
+  if (b->blocks == 0) {
+    int rc = pimc_batch_config(b, b->precision, b->shadow, b->threads, 0);
+    if (rc) return rc;
+  }
+  if (!b->graph || b->graph_blocks != n_blocks || b->graph_version != b->cfg_version) {
+    drop_graph(b);
+    BCK(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeRelaxed));
+    const int rc = batch_launch(b, n_blocks, nullptr, 0);
+    cudaGraph_t g = nullptr;
+    const cudaError_t e = cudaStreamEndCapture(b->stream, &g);
+    if (rc) {
+      if (g) cudaGraphDestroy(g);
+      return rc;
+    }
+    if (e != cudaSuccess) return bfail(b, PIMC_E_CUDA, std::string("capture: ") + cudaGetErrorString(e));
+    const cudaError_t ei = cudaGraphInstantiate(&b->graph, g, 0);
+    cudaGraphDestroy(g);
+    if (ei != cudaSuccess) {
+      b->graph = nullptr;
+      return bfail(b, PIMC_E_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(ei));
+    }
+    b->graph_blocks = n_blocks;
+    b->graph_version = b->cfg_version;
+  }
+  BCK(cudaGraphLaunch(b->graph, b->stream));
+  return PIMC_OK;
+}
+
+int pimc_batch_autotune(pimc_batch *b, int n_blocks, int *threads_out, int *ctas_out, double *ms_out) {
+  if (!b || n_blocks < 1) return PIMC_E_ARG;
+  BCK(cudaSetDevice(b->device));
+  BCK(cudaStreamSynchronize(b->stream));
+  // The probes advance the chains: keep their state and put it back after.
+  double *save_paths = nullptr;
+  ChainState *save_cs = nullptr;
+  BCK(cudaMalloc(&save_paths, b->path_doubles * sizeof(double)));
+  cudaError_t e = cudaMalloc(&save_cs, b->n_chains * sizeof(ChainState));
+  if (e != cudaSuccess) {
+    cudaFree(save_paths);
+    return bfail(b, PIMC_E_CUDA, "autotune: no room for the state copy");
+  }
+  e = cudaMemcpyAsync(save_paths, b->d_paths, b->path_doubles * sizeof(double), cudaMemcpyDeviceToDevice, b->stream);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(save_cs, b->d_chains, b->n_chains * sizeof(ChainState), cudaMemcpyDeviceToDevice, b->stream);
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  if (e == cudaSuccess) e = cudaEventCreate(&e0);
+  if (e == cudaSuccess) e = cudaEventCreate(&e1);
+  const int precision = b->precision, shadow = b->shadow;
+  int best_t = 0, best_c = 0, rc = PIMC_OK;
+  float best_ms = 0.f;
+  const int cand_threads[] = {64, 96, 128, 160, 192, 256};
+  for (int ti = 0; ti < 6 && e == cudaSuccess && rc == PIMC_OK; ti++) {
+    for (int mode = 0; mode < 2 && rc == PIMC_OK; mode++) {
+      // mode 0: every CTA that fits; mode 1: one CTA per SM
+      rc = pimc_batch_config(b, precision, shadow, cand_threads[ti], mode ? std::min(b->n_chains, b->sm_count) : 0);
+      if (rc == PIMC_E_ARG) {  // does not fit: not a candidate
+        rc = PIMC_OK;
+        continue;
+      }
+      if (rc) break;
+      rc = batch_launch(b, n_blocks, nullptr, 0);  // warm-up (module load, caches)
+      if (rc) break;
+      e = cudaEventRecord(e0, b->stream);
+      if (e == cudaSuccess) rc = batch_launch(b, n_blocks, nullptr, 0);
+      if (e == cudaSuccess && rc == PIMC_OK) e = cudaEventRecord(e1, b->stream);
+      if (e == cudaSuccess && rc == PIMC_OK) e = cudaEventSynchronize(e1);
+      float ms = 0.f;
+      if (e == cudaSuccess && rc == PIMC_OK) e = cudaEventElapsedTime(&ms, e0, e1);
+      if (e != cudaSuccess || rc) break;
+      if (best_t == 0 || ms < best_ms) {
+        best_ms = ms;
+        best_t = cand_threads[ti];
+        best_c = b->blocks;
+      }
+    }
+  }
+  cudaError_t er = cudaMemcpyAsync(b->d_paths, save_paths, b->path_doubles * sizeof(double),
+                                   cudaMemcpyDeviceToDevice, b->stream);
+  if (er == cudaSuccess)
+    er = cudaMemcpyAsync(b->d_chains, save_cs, b->n_chains * sizeof(ChainState), cudaMemcpyDeviceToDevice, b->stream);
+  if (er == cudaSuccess) er = cudaStreamSynchronize(b->stream);
+  cudaFree(save_paths);
+  cudaFree(save_cs);
+  if (e0) cudaEventDestroy(e0);
+  if (e1) cudaEventDestroy(e1);
+  if (rc) return rc;
+  if (e != cudaSuccess) return bfail(b, PIMC_E_CUDA, std::string("autotune: ") + cudaGetErrorString(e));
+  if (er != cudaSuccess) return bfail(b, PIMC_E_CUDA, std::string("autotune restore: ") + cudaGetErrorString(er));
+  if (best_t == 0) return bfail(b, PIMC_E_ARG, "autotune: no configuration fits");
+  rc = pimc_batch_config(b, precision, shadow, best_t, best_c);
+  if (rc) return rc;
+  if (threads_out) *threads_out = best_t;
+  if (ctas_out) *ctas_out = best_c;
+  if (ms_out) *ms_out = best_ms;
+  return PIMC_OK;
 }
 
 int pimc_batch_run(pimc_batch *b, int n_blocks, pimc_move_record *trace, pimc_bisection_stats *stats) {
@@ -337,6 +467,8 @@ int pimc_batch_get_path(pimc_batch *b, int chain, double *path) {
                  (size_t)c.num_time_slices * c.num_particles * 3 * sizeof(double), cudaMemcpyDeviceToHost));
   return PIMC_OK;
 }
+
+void *pimc_batch_stream(pimc_batch *b) { return b ? (void *)b->stream : nullptr; }
 
 int pimc_batch_synchronize(pimc_batch *b) {
   if (!b) return PIMC_E_ARG;

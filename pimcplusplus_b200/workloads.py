@@ -170,9 +170,23 @@ def lj_chain(n, m, temp, rho, levels, seed, steps_per_block=1, npts=200, r_min=1
                 tau_pos=0, path=path)
 
 
-def c3_chains(count, seed=0, steps_per_block=1, npts=200):
-    """Config C3: chains with N in {32..512}, M in {16..128}, T in [1,4] K,
-    density in [0.018, 0.024] A^-3, level chosen so 2^L <= M/2 (at most 4)."""
+def lattice_path(n, slices, box, rng, jitter=0.1):
+    """n particles on the first n sites of a simple-cubic lattice filling the
+    box, each displaced by up to +-jitter of the lattice spacing, copied to
+    every slice (a classical start: no overlaps at liquid densities)."""
+    side = int(np.ceil(n ** (1.0 / 3.0) - 1e-9))
+    idx = np.arange(side ** 3)[:n]
+    ijk = np.stack([idx // (side * side), (idx // side) % side, idx % side], axis=1).astype(np.float64)
+    a = np.asarray(box, dtype=np.float64) / side
+    pts = (ijk + 0.5 + jitter * (rng.random((n, 3)) * 2.0 - 1.0)) * a - 0.5 * np.asarray(box)
+    return np.repeat(pts[None], slices, axis=0)
+
+
+def c3_chains(count, seed=0, steps_per_block=4, npts=1000, max_levels=4):
+    """Batched uneven chains: N from {32,64,128,256,512}, M from
+    {16,32,64,128}, T uniform in [1,4] K, density uniform in
+    [0.018,0.024] A^-3, each with its own seed and primitive u_00 table on a
+    npts-point linear grid to L/2; bisection level min(max_levels, log2 M - 1)."""
     rng = np.random.default_rng(seed)
     out = []
     for i in range(count):
@@ -180,7 +194,15 @@ def c3_chains(count, seed=0, steps_per_block=1, npts=200):
         m = int(rng.choice([16, 32, 64, 128]))
         temp = float(rng.uniform(1.0, 4.0))
         rho = float(rng.uniform(0.018, 0.024))
-        levels = min(4, int(np.log2(m)) - 1)
-        out.append(lj_chain(n, m, temp, rho, levels, seed=1000 + i, steps_per_block=steps_per_block, npts=npts,
-                            rng=np.random.default_rng(1000 + i)))
+        levels = min(max_levels, int(np.log2(m)) - 1)
+        tau = 1.0 / (temp * m)
+        box = box_for_density(n, rho)
+        r_min = 1.5
+        r = r_min + np.arange(npts) * ((box[0] / 2.0 - r_min) / (npts - 1))
+        u00 = (tau * 2.0 ** np.arange(levels + 1))[:, None] * lj(r)[None, :]
+        u00[:, -1] = 0.0
+        path = lattice_path(n, m + 1, box, np.random.default_rng((seed << 20) + i))
+        out.append(dict(N=n, slices=m + 1, box=box, tau=tau, lam=HE4_LAMBDA, num_levels=levels,
+                        steps_per_block=steps_per_block, seed=(seed << 20) + 1000 + i,
+                        grid=(r_min, float(box[0] / 2.0), npts), u00=u00, tau_pos=0, path=path, T=temp, rho=rho))
     return out

@@ -67,3 +67,19 @@ def test_batch_mixed_runs_and_accepts():
     assert stats["status"] == 0
     assert 0.02 < stats["accepted"] / stats["moves"] < 0.98
     b.close()
+
+
+def test_batch_autotune_keeps_state_and_graph_replay_matches_oracle():
+    chains = make_chains()
+    b = P.BatchChains(chains, precision=P.FP64)
+    tune = b.autotune(3)
+    assert tune["threads_per_cta"] in (64, 96, 128, 160, 192, 256) and tune["ctas"] >= 1
+    for _ in range(3):  # the same launch replayed from its CUDA graph
+        b.run_async(5)
+    b.synchronize()
+    st = b.stats()
+    assert st["status"] == 0
+    for i in (0, 3, 7, 11):
+        _, ref_path, _ = oracle_run(chains[i], 15)
+        assert np.max(np.abs(b.path(i) - ref_path)) < 1e-9, i
+    b.close()
