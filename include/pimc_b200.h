@@ -257,9 +257,15 @@ typedef struct pimc_chain_desc {
 int pimc_batch_create(int device, int n_chains, const pimc_chain_desc *chains, pimc_batch **out);
 int pimc_batch_destroy(pimc_batch *b);
 int pimc_batch_last_error(pimc_batch *b, char *buf, int len);
-/* precision: PIMC_FP64 or PIMC_MIXED; threads_per_cta 64..256 (0 = 128);
- * ctas: persistent CTAs (0 = every CTA that fits, capped at the chain count). */
-int pimc_batch_config(pimc_batch *b, int precision, int shadow, int threads_per_cta, int ctas);
+/* precision: PIMC_FP64 or PIMC_MIXED; threads_per_cta 64..512 (0 = 256);
+ * ctas: persistent CTAs (0 = every CTA that fits, capped at the chain count).
+ * Chains run largest first (cost N * 2^levels * steps_per_block).  A CTA
+ * runs the costliest chains with all its threads; with max_split = 1 or 2 it
+ * divides into 2 or 4 groups, each running its own chain, for the chains
+ * whose cost is at most split_ratio (split_ratio^2) of the largest.  Groups
+ * must keep 64+ threads, a multiple of 32. */
+int pimc_batch_config(pimc_batch *b, int precision, int shadow, int threads_per_cta, int ctas, int max_split,
+                      double split_ratio);
 /* n_blocks blocks of moves on every chain; trace: [chain][n_blocks*steps]
  * records (chains with fewer steps leave zeros) or NULL; stats: totals. */
 int pimc_batch_run(pimc_batch *b, int n_blocks, pimc_move_record *trace, pimc_bisection_stats *stats);
@@ -267,11 +273,13 @@ int pimc_batch_run(pimc_batch *b, int n_blocks, pimc_move_record *trace, pimc_bi
  * captured once as a CUDA graph and replayed while n_blocks and the
  * configuration stay the same. */
 int pimc_batch_run_async(pimc_batch *b, int n_blocks);
-/* Times n_blocks blocks under each candidate threads_per_cta (64..256) with
- * every CTA that fits or one CTA per SM, keeps the fastest with the current
- * precision and shadow setting, and puts the chains back in their state
- * from before the probes.  Outputs may be NULL. */
-int pimc_batch_autotune(pimc_batch *b, int n_blocks, int *threads_per_cta, int *ctas, double *ms);
+/* Times n_blocks blocks under each candidate threads_per_cta (128, 256,
+ * 384, 512) x max_split (0..2) x split_ratio (1/2, 1/4) with every CTA that
+ * fits, keeps the fastest with the current precision and shadow setting,
+ * and puts the chains back in their state from before the probes.  Outputs
+ * may be NULL. */
+int pimc_batch_autotune(pimc_batch *b, int n_blocks, int *threads_per_cta, int *ctas, int *max_split,
+                        double *split_ratio, double *ms);
 int pimc_batch_get_stats(pimc_batch *b, int chain /* -1: all */, pimc_bisection_stats *stats);
 int pimc_batch_get_path(pimc_batch *b, int chain, double *path);
 int pimc_batch_synchronize(pimc_batch *b);

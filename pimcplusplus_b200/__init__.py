@@ -155,10 +155,11 @@ _SIGS = {
     "pimc_batch_create": (_i, [_i, _i, C.POINTER(ChainDesc), C.POINTER(_p)]),
     "pimc_batch_destroy": (_i, [_p]),
     "pimc_batch_last_error": (_i, [_p, C.c_char_p, _i]),
-    "pimc_batch_config": (_i, [_p, _i, _i, _i, _i]),
+    "pimc_batch_config": (_i, [_p, _i, _i, _i, _i, _i, _d]),
     "pimc_batch_run": (_i, [_p, _i, _p, C.POINTER(BisectionStats)]),
     "pimc_batch_run_async": (_i, [_p, _i]),
-    "pimc_batch_autotune": (_i, [_p, _i, C.POINTER(_i), C.POINTER(_i), C.POINTER(C.c_double)]),
+    "pimc_batch_autotune": (_i, [_p, _i, C.POINTER(_i), C.POINTER(_i), C.POINTER(_i), C.POINTER(_d),
+                                 C.POINTER(_d)]),
     "pimc_batch_get_stats": (_i, [_p, _i, C.POINTER(BisectionStats)]),
     "pimc_batch_get_path": (_i, [_p, _i, _dp]),
     "pimc_batch_synchronize": (_i, [_p]),
@@ -241,9 +242,9 @@ class PathData:
         self._keep = []
 
     def close(self):
-        if getattr(self, "h", None):
+        if getattr(self, "h", None) and _lib is not None:
             _lib.pimc_destroy(self.h)
-            self.h = None
+        self.h = None
 
     def __del__(self):
         self.close()
@@ -450,7 +451,8 @@ class BatchChains:
     path [slices][N][3], num_images (optional).
     """
 
-    def __init__(self, chains, device=0, precision=MIXED, shadow=False, threads_per_cta=0, ctas=0):
+    def __init__(self, chains, device=0, precision=MIXED, shadow=False, threads_per_cta=0, ctas=0, max_split=0,
+                 split_ratio=0.5):
         self._keep = []
         descs = (ChainDesc * len(chains))()
         self.shapes = []
@@ -482,7 +484,7 @@ class BatchChains:
         self.h = h
         self.n = len(chains)
         self.steps = max(c["steps_per_block"] for c in chains)
-        self.config(precision, shadow, threads_per_cta, ctas)
+        self.config(precision, shadow, threads_per_cta, ctas, max_split, split_ratio)
 
     def _check(self, rc, what):
         if rc:
@@ -490,8 +492,9 @@ class BatchChains:
             _lib.pimc_batch_last_error(self.h, buf, 512)
             raise PimcError(rc, f"{what}: {buf.value.decode(errors='replace')}")
 
-    def config(self, precision=MIXED, shadow=False, threads_per_cta=0, ctas=0):
-        self._check(_lib.pimc_batch_config(self.h, precision, int(shadow), threads_per_cta, ctas), "batch_config")
+    def config(self, precision=MIXED, shadow=False, threads_per_cta=0, ctas=0, max_split=0, split_ratio=0.5):
+        self._check(_lib.pimc_batch_config(self.h, precision, int(shadow), threads_per_cta, ctas, max_split,
+                                           split_ratio), "batch_config")
 
     def run(self, n_blocks, trace=False):
         st = BisectionStats()
@@ -514,9 +517,10 @@ class BatchChains:
 
     def autotune(self, n_blocks=1):
         """Pick threads_per_cta and the CTA count by timing; chains keep their state."""
-        t, c, ms = _i(), _i(), C.c_double()
-        self._check(_lib.pimc_batch_autotune(self.h, n_blocks, C.byref(t), C.byref(c), C.byref(ms)), "batch_autotune")
-        return dict(threads_per_cta=t.value, ctas=c.value, ms=ms.value)
+        t, c, sp, r, ms = _i(), _i(), _i(), C.c_double(), C.c_double()
+        self._check(_lib.pimc_batch_autotune(self.h, n_blocks, C.byref(t), C.byref(c), C.byref(sp), C.byref(r),
+                                             C.byref(ms)), "batch_autotune")
+        return dict(threads_per_cta=t.value, ctas=c.value, max_split=sp.value, split_ratio=r.value, ms=ms.value)
 
     def stats(self, chain=-1):
         st = BisectionStats()
@@ -529,9 +533,9 @@ class BatchChains:
         return out
 
     def close(self):
-        if getattr(self, "h", None):
+        if getattr(self, "h", None) and _lib is not None:
             _lib.pimc_batch_destroy(self.h)
-            self.h = None
+        self.h = None
 
     def __del__(self):
         self.close()

@@ -31,7 +31,10 @@ struct pimc_batch {
   ChainState *d_chains = nullptr;
   pimc_move_record *d_trace = nullptr;
   size_t trace_cap = 0;
-  int precision = PIMC_MIXED, shadow = 0, threads = 128;
+  int precision = PIMC_MIXED, shadow = 0, threads = 256;
+  int max_split = 0;
+  int split[kMaxSplit] = {};
+  std::vector<double> cost_sorted;  // estimated cost of each queue position
   size_t dyn = 0;
   int blocks = 0;
   int sm_count = 0;
@@ -119,12 +122,14 @@ void drop_graph(pimc_batch *b) {
 // Shared memory for the staged tables: the working precision's column plus,
 // with the shadow evaluation, the other precision's (FP32 pairs are half the
 // FP64 bytes).
-size_t batch_dyn(const pimc_batch *b) {
+// One slot's share; the launch holds 2^max_split slots.
+size_t batch_dyn_slot(const pimc_batch *b) {
   const size_t b64 = b->dyn, b32 = b->dyn / 2;
   size_t d = b->precision == PIMC_MIXED ? b32 : b64;
   if (b->shadow) d += b->precision == PIMC_MIXED ? b64 : b32;
-  return d + 16;
+  return (d + 15) & ~(size_t)15;
 }
+size_t batch_dyn(const pimc_batch *b) { return batch_dyn_slot(b) << b->max_split; }
 
 }  // namespace
 
@@ -240,6 +245,10 @@ int pimc_batch_create(int device, int n_chains, const pimc_chain_desc *chains, p
     const double cy = (double)chains[y].num_particles * (1 << chains[y].num_levels) * chains[y].steps_per_block;
     return cx > cy;
   });
+  b->cost_sorted.resize(n_chains);
+  for (int i = 0; i < n_chains; i++)
+    b->cost_sorted[i] =
+        (double)chains[order[i]].num_particles * (1 << chains[order[i]].num_levels) * chains[order[i]].steps_per_block;
   e = cudaMemcpy(b->d_jobs, b->jobs.data(), n_chains * sizeof(BisectionArgs), cudaMemcpyHostToDevice);
   if (e == cudaSuccess) e = cudaMemcpy(b->d_order, order.data(), n_chains * sizeof(int), cudaMemcpyHostToDevice);
   if (e == cudaSuccess) e = cudaMemcpy(b->d_chains, cs.data(), n_chains * sizeof(ChainState), cudaMemcpyHostToDevice);
@@ -274,20 +283,43 @@ int pimc_batch_last_error(pimc_batch *b, char *buf, int len) {
   return PIMC_OK;
 }
 
-int pimc_batch_config(pimc_batch *b, int precision, int shadow, int threads_per_cta, int ctas) {
+int pimc_batch_config(pimc_batch *b, int precision, int shadow, int threads_per_cta, int ctas, int max_split,
+                      double split_ratio) {
   if (!b) return PIMC_E_ARG;
   if (precision != PIMC_FP64 && precision != PIMC_MIXED) return bfail(b, PIMC_E_ARG, "bad precision");
-  if (threads_per_cta != 0 && (threads_per_cta < 64 || threads_per_cta > 256 || threads_per_cta % 32))
-    return bfail(b, PIMC_E_ARG, "threads_per_cta must be a multiple of 32 in 64..256");
+  const int threads = threads_per_cta ? threads_per_cta : 256;
+  if (max_split < 0 || max_split > kMaxSplit) return bfail(b, PIMC_E_ARG, "max_split must be in 0..2");
+  if (threads < 64 || threads > 512 || (threads >> max_split) % 32 || (threads >> max_split) < 64)
+    return bfail(b, PIMC_E_ARG, "threads_per_cta must be in 64..512 and split into groups of 64+ (multiples of 32)");
+  if (max_split > 0 && !(split_ratio > 0.0 && split_ratio < 1.0))
+    return bfail(b, PIMC_E_ARG, "split_ratio must be in (0, 1)");
   if (ctas < 0) return bfail(b, PIMC_E_ARG, "ctas must be >= 0");
   BCK(cudaSetDevice(b->device));
+  const int old_split = b->max_split;
   b->precision = precision;
   b->shadow = shadow;
-  b->threads = threads_per_cta ? threads_per_cta : 128;
+  b->threads = threads;
+  b->max_split = max_split;
+  // level k+1 groups take the chains from the first queue position whose
+  // cost is at most ratio^(k+1) of the largest
+  for (int k = 0; k < kMaxSplit; k++) {
+    int pos = b->n_chains;
+    if (k < max_split) {
+      const double lim = b->cost_sorted[0] * std::pow(split_ratio, k + 1);
+      pos = 0;
+      while (pos < b->n_chains && b->cost_sorted[pos] > lim) pos++;
+    }
+    b->split[k] = pos;
+  }
   const size_t dyn = batch_dyn(b);
   int per_sm = 0;
-  BCK(batch_occupancy(precision, shadow, b->threads, dyn, &per_sm));
-  if (per_sm < 1) return bfail(b, PIMC_E_ARG, "configuration does not fit on an SM");
+  cudaError_t e = dyn > (size_t)140 * 1024 ? cudaErrorInvalidValue
+                                           : batch_occupancy(precision, shadow, b->threads, dyn, &per_sm);
+  if (e != cudaSuccess || per_sm < 1) {
+    b->max_split = old_split;
+    cudaGetLastError();
+    return bfail(b, PIMC_E_ARG, "configuration does not fit on an SM");
+  }
   b->blocks = ctas ? ctas : std::min(b->n_chains, per_sm * b->sm_count);
   b->cfg_version++;
   return PIMC_OK;
@@ -295,7 +327,7 @@ int pimc_batch_config(pimc_batch *b, int precision, int shadow, int threads_per_
 
 static int batch_launch(pimc_batch *b, int n_blocks, pimc_move_record *dtrace, long long per_chain) {
   if (b->blocks == 0) {
-    int rc = pimc_batch_config(b, b->precision, b->shadow, b->threads, 0);
+    int rc = pimc_batch_config(b, b->precision, b->shadow, b->threads, 0, 0, 0.5);
     if (rc) return rc;
   }
   BCK(cudaMemsetAsync(b->d_queue, 0, sizeof(unsigned int), b->stream));
@@ -307,6 +339,9 @@ static int batch_launch(pimc_batch *b, int n_blocks, pimc_move_record *dtrace, l
   a.n_blocks = n_blocks;
   a.trace = dtrace;
   a.trace_per_chain = per_chain;
+  a.max_split = b->max_split;
+  for (int k = 0; k < kMaxSplit; k++) a.split[k] = b->split[k];
+  a.dyn_per_slot = (unsigned)batch_dyn_slot(b);
   const size_t dyn = batch_dyn(b);
   BCK(launch_batch(a, b->precision, b->shadow, b->blocks, b->threads, dyn, b->stream));
   return PIMC_OK;
@@ -316,7 +351,7 @@ int pimc_batch_run_async(pimc_batch *b, int n_blocks) {
   if (!b || n_blocks < 0) return PIMC_E_ARG;
   BCK(cudaSetDevice(b->device));
   if (b->blocks == 0) {
-    int rc = pimc_batch_config(b, b->precision, b->shadow, b->threads, 0);
+    int rc = pimc_batch_config(b, b->precision, b->shadow, b->threads, 0, 0, 0.5);
     if (rc) return rc;
   }
   if (!b->graph || b->graph_blocks != n_blocks || b->graph_version != b->cfg_version) {
@@ -343,7 +378,8 @@ int pimc_batch_run_async(pimc_batch *b, int n_blocks) {
   return PIMC_OK;
 }
 
-int pimc_batch_autotune(pimc_batch *b, int n_blocks, int *threads_out, int *ctas_out, double *ms_out) {
+int pimc_batch_autotune(pimc_batch *b, int n_blocks, int *threads_out, int *ctas_out, int *split_out,
+                        double *ratio_out, double *ms_out) {
   if (!b || n_blocks < 1) return PIMC_E_ARG;
   BCK(cudaSetDevice(b->device));
   BCK(cudaStreamSynchronize(b->stream));
@@ -363,34 +399,37 @@ int pimc_batch_autotune(pimc_batch *b, int n_blocks, int *threads_out, int *ctas
   if (e == cudaSuccess) e = cudaEventCreate(&e0);
   if (e == cudaSuccess) e = cudaEventCreate(&e1);
   const int precision = b->precision, shadow = b->shadow;
-  int best_t = 0, best_c = 0, rc = PIMC_OK;
+  int best_t = 0, best_c = 0, best_s = 0, rc = PIMC_OK;
+  double best_r = 0.5;
   float best_ms = 0.f;
-  const int cand_threads[] = {64, 96, 128, 160, 192, 256};
-  for (int ti = 0; ti < 6 && e == cudaSuccess && rc == PIMC_OK; ti++) {
-    for (int mode = 0; mode < 2 && rc == PIMC_OK; mode++) {
-      // mode 0: every CTA that fits; mode 1: one CTA per SM
-      rc = pimc_batch_config(b, precision, shadow, cand_threads[ti], mode ? std::min(b->n_chains, b->sm_count) : 0);
-      if (rc == PIMC_E_ARG) {  // does not fit: not a candidate
-        rc = PIMC_OK;
-        continue;
+  const int cand_threads[] = {128, 256, 384, 512};
+  const double cand_ratio[] = {0.5, 0.25};
+  for (int ti = 0; ti < 4 && e == cudaSuccess && rc == PIMC_OK; ti++)
+    for (int ms_ = 0; ms_ <= kMaxSplit && rc == PIMC_OK && e == cudaSuccess; ms_++)
+      for (int ri = 0; ri < (ms_ ? 2 : 1) && rc == PIMC_OK && e == cudaSuccess; ri++) {
+        rc = pimc_batch_config(b, precision, shadow, cand_threads[ti], 0, ms_, cand_ratio[ri]);
+        if (rc == PIMC_E_ARG) {  // does not fit: not a candidate
+          rc = PIMC_OK;
+          continue;
+        }
+        if (rc) break;
+        rc = batch_launch(b, n_blocks, nullptr, 0);  // warm-up (module load, caches)
+        if (rc) break;
+        e = cudaEventRecord(e0, b->stream);
+        if (e == cudaSuccess) rc = batch_launch(b, n_blocks, nullptr, 0);
+        if (e == cudaSuccess && rc == PIMC_OK) e = cudaEventRecord(e1, b->stream);
+        if (e == cudaSuccess && rc == PIMC_OK) e = cudaEventSynchronize(e1);
+        float ms = 0.f;
+        if (e == cudaSuccess && rc == PIMC_OK) e = cudaEventElapsedTime(&ms, e0, e1);
+        if (e != cudaSuccess || rc) break;
+        if (best_t == 0 || ms < best_ms) {
+          best_ms = ms;
+          best_t = cand_threads[ti];
+          best_c = b->blocks;
+          best_s = ms_;
+          best_r = cand_ratio[ri];
+        }
       }
-      if (rc) break;
-      rc = batch_launch(b, n_blocks, nullptr, 0);  // warm-up (module load, caches)
-      if (rc) break;
-      e = cudaEventRecord(e0, b->stream);
-      if (e == cudaSuccess) rc = batch_launch(b, n_blocks, nullptr, 0);
-      if (e == cudaSuccess && rc == PIMC_OK) e = cudaEventRecord(e1, b->stream);
-      if (e == cudaSuccess && rc == PIMC_OK) e = cudaEventSynchronize(e1);
-      float ms = 0.f;
-      if (e == cudaSuccess && rc == PIMC_OK) e = cudaEventElapsedTime(&ms, e0, e1);
-      if (e != cudaSuccess || rc) break;
-      if (best_t == 0 || ms < best_ms) {
-        best_ms = ms;
-        best_t = cand_threads[ti];
-        best_c = b->blocks;
-      }
-    }
-  }
   cudaError_t er = cudaMemcpyAsync(b->d_paths, save_paths, b->path_doubles * sizeof(double),
                                    cudaMemcpyDeviceToDevice, b->stream);
   if (er == cudaSuccess)
@@ -404,10 +443,12 @@ int pimc_batch_autotune(pimc_batch *b, int n_blocks, int *threads_out, int *ctas
   if (e != cudaSuccess) return bfail(b, PIMC_E_CUDA, std::string("autotune: ") + cudaGetErrorString(e));
   if (er != cudaSuccess) return bfail(b, PIMC_E_CUDA, std::string("autotune restore: ") + cudaGetErrorString(er));
   if (best_t == 0) return bfail(b, PIMC_E_ARG, "autotune: no configuration fits");
-  rc = pimc_batch_config(b, precision, shadow, best_t, best_c);
+  rc = pimc_batch_config(b, precision, shadow, best_t, best_c, best_s, best_r);
   if (rc) return rc;
   if (threads_out) *threads_out = best_t;
   if (ctas_out) *ctas_out = best_c;
+  if (split_out) *split_out = best_s;
+  if (ratio_out) *ratio_out = best_r;
   if (ms_out) *ms_out = best_ms;
   return PIMC_OK;
 }

@@ -84,7 +84,7 @@ __device__ __forceinline__ double warp_sum(double v) {
 // BisectionStageClass::Sample (BisectionStage.cc:128-289) for one level on
 // the window held in shared memory, run by one full warp: writes the NEW
 // midpoints and returns log T_old - log T_new (identical in every lane).
-__device__ double sample_level_warp(double (*w_old)[3], double (*w_new)[3], double *gbuf, int num_levels, int level,
+__device__ __forceinline__ double sample_level_warp(double (*w_old)[3], double (*w_new)[3], double *gbuf, int num_levels, int level,
                                     const DevSystem &s, DevRandom &rng, int lane) {
   const int skip = 1 << (level + 1);
   const int nmid = (1 << num_levels) >> (level + 1);
@@ -199,7 +199,18 @@ __device__ __forceinline__ double4 stage_sums(const BisectionArgs &a, const doub
     while (T < tmax && items * T * 2 <= ethreads) T *= 2;
     if (T == 1) {
       // Two items per pass so a thread's partner and table loads overlap.
-      for (int it0 = beg + etid; it0 < end; it0 += 2 * ethreads) {
+      // Item it is (link, j) = (it / np, it % np); both pass items advance
+      // by the same stride, so (link, j) is carried instead of divided.
+      const int stride = 2 * ethreads;
+      const int qs = stride / np, rs = stride - qs * np;
+      int lk[2], jj[2];
+#pragma unroll
+      for (int u = 0; u < 2; u++) {
+        const int it = beg + etid + u * ethreads;
+        lk[u] = it / np;
+        jj[u] = it - lk[u] * np;
+      }
+      for (int it0 = beg + etid; it0 < end; it0 += stride) {
         double a2[2][3], b2[2][3];
         int r0s[2];
         bool live[2];
@@ -207,9 +218,8 @@ __device__ __forceinline__ double4 stage_sums(const BisectionArgs &a, const doub
         for (int u = 0; u < 2; u++) {
           const int it = it0 + u * ethreads;
           live[u] = it < end;
-          const int itc = live[u] ? it : it0;
-          const int link = itc / np;
-          const int j = itc - link * np;
+          const int link = live[u] ? lk[u] : lk[0];
+          const int j = live[u] ? jj[u] : jj[0];
           const int p2 = j < ptcl ? j : j + 1;
           r0s[u] = link * skip;
           const double *pa_ = path + ((size_t)(slice1 + r0s[u]) * N + p2) * 3;
@@ -218,6 +228,15 @@ __device__ __forceinline__ double4 stage_sums(const BisectionArgs &a, const doub
           for (int i = 0; i < 3; i++) {
             a2[u][i] = __ldcg(pa_ + i);
             b2[u][i] = __ldcg(pb_ + i);
+          }
+        }
+#pragma unroll
+        for (int u = 0; u < 2; u++) {
+          jj[u] += rs;
+          lk[u] += qs;
+          if (jj[u] >= np) {
+            jj[u] -= np;
+            lk[u]++;
           }
         }
 #pragma unroll
@@ -277,8 +296,10 @@ struct RngSnap {
   double x2;
 };
 
-__device__ __forceinline__ DevRandom rng_from(const RngSnap &s, uint64_t seed, uint32_t stream) {
+__device__ __forceinline__ DevRandom rng_from(const RngSnap &s, uint64_t seed, uint32_t stream,
+                                              const RngTab *tab) {
   DevRandom r;
+  r.tab = tab;
   r.seed = seed;
   r.stream = stream;
   r.n = s.n;
@@ -318,6 +339,42 @@ struct KernelShared {
   int s_next[4];  // next move speculated: valid, slice1, ptcl
   double s_next_f[2];
   RngSnap s_rng, s_spec1, s_spec2;
+  int s_ok;
+  RngTab tab;
+};
+
+// Storage of the precomputed stream tables of a CTA: NF parts of kTabFine
+// positions; a group uses a contiguous run of parts.
+constexpr int kTabFine = 256;
+template <int NF>
+struct RngStore {
+  double u[NF * (kTabFine + 2)];
+  double lu[NF * kTabFine], x1[NF * kTabFine], x2[NF * kTabFine];
+  unsigned char acc[NF * kTabFine];
+  template <int NF2>
+  __device__ __forceinline__ RngTab part(int first, int count) {
+    RngTab t;
+    t.u = u + first * (kTabFine + 2);
+    t.lu = lu + first * kTabFine;
+    t.x1 = x1 + first * kTabFine;
+    t.x2 = x2 + first * kTabFine;
+    t.acc = acc + first * kTabFine;
+    t.tb = 0;
+    t.W = count * kTabFine;
+    return t;
+  }
+};
+
+// The threads that run one job: a warp-aligned contiguous range of the CTA
+// synchronised by its own named barrier (the whole CTA, or a part of it when
+// a CTA runs several small chains side by side).
+struct Group {
+  int tid;       // thread index within the group
+  int size;      // threads in the group, a multiple of 32
+  unsigned bar;  // named barrier id
+  __device__ __forceinline__ void sync() const {
+    asm volatile("bar.sync %0, %1;" ::"r"(bar), "r"(size) : "memory");
+  }
 };
 
 // The moves of one job — one chain, or one window of a chain — on this CTA
@@ -325,8 +382,8 @@ struct KernelShared {
 // mbarrier `bar`, flipped once per staging.
 template <int KIND, typename R, bool SHADOW>
 __device__ void run_job(const BisectionArgs &a, ChainState *cs, int window, unsigned rank, unsigned CL,
-                        cg::cluster_group &cluster, unsigned char *dyn, KernelShared &S, uint64_t *bar_ptr,
-                        unsigned &phase) {
+                        cg::cluster_group &cluster, const Group &G, unsigned char *dyn, unsigned dyn_cap,
+                        KernelShared &S, uint64_t *bar_ptr, unsigned &phase, const RngTab &tab_mem) {
   typedef typename Pair2<R>::T P2;
   typedef typename std::conditional<std::is_same<R, double>::value, float, double>::type RS;  // shadow precision
   typedef typename Pair2<RS>::T P2S;
@@ -344,9 +401,9 @@ __device__ void run_job(const BisectionArgs &a, ChainState *cs, int window, unsi
   auto &s_spec1 = S.s_spec1;
   auto &s_spec2 = S.s_spec2;
   uint64_t &s_bar = *bar_ptr;
-  const int tid = threadIdx.x;
+  const int tid = G.tid;
   const int lane = tid & 31, warp = tid >> 5;
-  const int nwarps = blockDim.x >> 5;
+  const int nwarps = G.size >> 5;
   const int sampler = nwarps - 1;
   const int specwarp = nwarps >= 4 ? nwarps - 2 : -1;  // next-move speculator (needs >= 4 warps)
   const int ethreads = (nwarps - (specwarp >= 0 ? 2 : 1)) * 32;  // evaluating threads: warps below the samplers
@@ -368,13 +425,11 @@ __device__ void run_job(const BisectionArgs &a, ChainState *cs, int window, unsi
     const unsigned bytes = (unsigned)(L * d.diag_stride * sizeof(P2));
     unsigned bytes_s = 0;
     if (SHADOW) bytes_s = (unsigned)(L * david_of<RS>(a.pa).diag_stride * sizeof(P2S));
-    unsigned dyn_size;
-    asm("mov.u32 %0, %%dynamic_smem_size;" : "=r"(dyn_size));
-    if (bytes + bytes_s > dyn_size) {  // uniform over the cluster: same job, same launch
+    if (bytes + bytes_s > dyn_cap) {  // uniform over the cluster: same job, same launch
       if (lead) atomicExch(&cs->status, PIMC_E_CAP);
       return;
     }
-    __syncthreads();  // the previous job's readers of the staged tables are done
+    G.sync();  // the previous job's readers of the staged tables are done
     if (tid == 0) {
       asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
       mbar_expect_tx(&s_bar, bytes + bytes_s);
@@ -385,14 +440,18 @@ __device__ void run_job(const BisectionArgs &a, ChainState *cs, int window, unsi
                  &s_bar);
       }
     }
-    __syncthreads();
+    G.sync();
     int ok = 0;
     for (int it = 0; it < (1 << 22); it++)
       if (mbar_try_wait(&s_bar, phase)) {
         ok = 1;
         break;
       }
-    ok = __syncthreads_and(ok);
+    if (tid == 0) S.s_ok = 1;
+    G.sync();
+    if (!ok) S.s_ok = 0;
+    G.sync();
+    ok = S.s_ok;
     int all_ok = ok;
     if (CL > 1) {
       if (tid < (int)CL) cluster.map_shared_rank(&xchg[1][rank][0], tid)[0] = ok ? 1.0 : 0.0;
@@ -420,6 +479,8 @@ __device__ void run_job(const BisectionArgs &a, ChainState *cs, int window, unsi
     s_rng.x2 = cs->x2;
     s_ctl[3] = 0;
     s_next[0] = 0;
+    S.tab = tab_mem;
+    S.tab.W = 0;  // filled below
   }
   unsigned long long moves = 0, accepted = 0, stages = 0, pair_evals = 0, flips = 0;
   int status = 0;
@@ -445,7 +506,9 @@ __device__ void run_job(const BisectionArgs &a, ChainState *cs, int window, unsi
     }
   }
   if (KIND == PA_DAVID && CL > 1) cluster.sync();  // every CTA has read xchg[1]
-  __syncthreads();
+  G.sync();
+  auto gsync = [&]() { G.sync(); };
+  rng_tab_fill(S.tab, tab_mem.W, seed, stream, s_rng.n, tid, G.size, gsync);
   const int numLeft = sys.S - span;
   const int total_moves = (a.concurrent ? 1 : a.n_blocks) * a.steps_per_block;
   int cur = 0;
@@ -456,7 +519,7 @@ __device__ void run_job(const BisectionArgs &a, ChainState *cs, int window, unsi
     if (!have_next) {
       // ChooseTimeSlices (BisectionBlock.cc:362-374), ChooseParticle (NoPermuteClass.cc:61-68)
       if (warp == sampler) {
-        DevRandom rng = rng_from(s_rng, seed, stream);
+        DevRandom rng = rng_from(s_rng, seed, stream, &S.tab);
         if (!a.concurrent && step == 0) slice1 = rng.LocalInt(numLeft);
         const int p = rng.LocalInt(N);
         __syncwarp();
@@ -466,18 +529,18 @@ __device__ void run_job(const BisectionArgs &a, ChainState *cs, int window, unsi
           rng_store(s_rng, rng);
         }
       }
-      __syncthreads();
+      G.sync();
       slice1 = s_ctl[0];
       const int p = s_ctl[1];
-      for (int rel = tid; rel <= span; rel += blockDim.x) {
+      for (int rel = tid; rel <= span; rel += G.size) {
         const double *q = path + ((size_t)(slice1 + rel) * N + p) * 3;
         for (int i = 0; i < 3; i++) win_old[cur][rel][i] = win_new[cur][rel][i] = __ldcg(q + i);
       }
-      __syncthreads();
+      G.sync();
       if (warp == sampler) {
-        DevRandom rng = rng_from(s_rng, seed, stream);
+        DevRandom rng = rng_from(s_rng, seed, stream, &S.tab);
         const double lsr = sample_level_warp(win_old[cur], win_new[cur], gbuf[0], L, L - 1, sys, rng, lane);
-        const double lu = log(rng.Local());
+        const double lu = rng.LocalLog();
         __syncwarp();
         if (lane == 0) {
           s_logsr[L - 1] = lsr;
@@ -485,7 +548,7 @@ __device__ void run_job(const BisectionArgs &a, ChainState *cs, int window, unsi
           rng_store(s_rng, rng);
         }
       }
-      __syncthreads();
+      G.sync();
     }
     slice1 = s_ctl[0];
     const int ptcl = s_ctl[1];
@@ -523,9 +586,9 @@ __device__ void run_job(const BisectionArgs &a, ChainState *cs, int window, unsi
       } else {
         if (warp == sampler && level > 0) {
           // speculative sampling of the next level (BisectionStage::Sample of stage level-1)
-          DevRandom spec = rng_from(s_rng, seed, stream);
+          DevRandom spec = rng_from(s_rng, seed, stream, &S.tab);
           const double lsr = sample_level_warp(w_old, w_new, gbuf[0], L, level - 1, sys, spec, lane);
-          const double lu = log(spec.Local());
+          const double lu = spec.LocalLog();
           __syncwarp();
           if (lane == 0) {
             s_logsr[level - 1] = lsr;
@@ -535,7 +598,7 @@ __device__ void run_job(const BisectionArgs &a, ChainState *cs, int window, unsi
         }
         if (warp == specwarp && more) {
           // speculative start of the next move, as if this move ends here
-          DevRandom spec = rng_from(s_rng, seed, stream);
+          DevRandom spec = rng_from(s_rng, seed, stream, &S.tab);
           const int ns1 = next_new_block ? spec.LocalInt(numLeft) : slice1;
           const int np_ = spec.LocalInt(N);
           double(*wo)[3] = win_old[cur ^ 1];
@@ -546,7 +609,7 @@ __device__ void run_job(const BisectionArgs &a, ChainState *cs, int window, unsi
           }
           __syncwarp();
           const double lsr = sample_level_warp(wo, wn, gbuf[1], L, L - 1, sys, spec, lane);
-          const double lu = log(spec.Local());
+          const double lu = spec.LocalLog();
           __syncwarp();
           if (lane == 0) {
             s_next[1] = ns1;
@@ -560,7 +623,7 @@ __device__ void run_job(const BisectionArgs &a, ChainState *cs, int window, unsi
       }
       // Counted as the reference performs them: OLD + NEW of the stage's links.
       if (lead && (level == 0 || a.sr_higher)) pair_evals += 2ull * (unsigned long long)(N - 1) * (span >> level);
-      __syncthreads();
+      G.sync();
       // ---- reduce: warps -> CTA (warp 0) -> cluster (DSMEM, rank order) ----
       const int par = xc & 1;
       xc++;
@@ -623,7 +686,7 @@ __device__ void run_job(const BisectionArgs &a, ChainState *cs, int window, unsi
           s_next[0] = nv;
         }
       }
-      __syncthreads();
+      G.sync();
       if (tid == 0) stages++;
       if (!s_ctl[2] || s_ctl[3]) {
         acc_all = false;
@@ -635,7 +698,7 @@ __device__ void run_job(const BisectionArgs &a, ChainState *cs, int window, unsi
     // ---- AcceptCopy (PathClass.cc:797-863); a rejected move left HBM untouched ----
     if (acc_all) {
       if (rank == 0)
-        for (int rel = tid; rel <= span; rel += blockDim.x) {
+        for (int rel = tid; rel <= span; rel += G.size) {
           double v[3] = {w_new[rel][0], w_new[rel][1], w_new[rel][2]};
           put_in_box_fast(v, sys);
           double *q = path + ((size_t)(slice1 + rel) * N + ptcl) * 3;
@@ -646,7 +709,7 @@ __device__ void run_job(const BisectionArgs &a, ChainState *cs, int window, unsi
       if (CL > 1)
         cluster.sync();
       else
-        __syncthreads();
+        G.sync();
     }
     if (lead) {
       moves++;
@@ -661,7 +724,11 @@ __device__ void run_job(const BisectionArgs &a, ChainState *cs, int window, unsi
     }
     if (s_ctl[3] != 0) break;
     if (have_next) cur ^= 1;
-    __syncthreads();  // every thread has read s_ctl / s_next before the next move rewrites them
+    G.sync();  // every thread has read s_ctl / s_next before the next move rewrites them
+    // Refill the stream table once less than half of it is ahead of the
+    // committed position (the next move's draws, if any, are committed).
+    if ((long long)(S.tab.tb + (uint64_t)S.tab.W) - (long long)s_rng.n < (long long)(tab_mem.W >> 1))
+      rng_tab_fill(S.tab, tab_mem.W, seed, stream, s_rng.n, tid, G.size, gsync);
   }
   if (lead) {
     cs->nlocal = s_rng.n;
@@ -675,7 +742,7 @@ __device__ void run_job(const BisectionArgs &a, ChainState *cs, int window, unsi
     if (status) cs->status = status;
   }
   if (CL > 1) cluster.sync();
-  __syncthreads();
+  G.sync();
 }
 
 // One chain on a thread-block cluster: the sequential schedule (one launch
@@ -684,6 +751,7 @@ __device__ void run_job(const BisectionArgs &a, ChainState *cs, int window, unsi
 template <int KIND, typename R, bool SHADOW>
 __global__ void __launch_bounds__(512, 1) bisection_kernel(BisectionArgs a) {
   __shared__ KernelShared S;
+  __shared__ RngStore<2> store;
   __shared__ __align__(8) uint64_t s_bar;
   extern __shared__ __align__(16) unsigned char dyn[];
   cg::cluster_group cluster = cg::this_cluster();
@@ -697,47 +765,87 @@ __global__ void __launch_bounds__(512, 1) bisection_kernel(BisectionArgs a) {
   __syncthreads();
   unsigned phase = 0;
   ChainState *cs = a.chains + (a.concurrent ? window : 0);
-  run_job<KIND, R, SHADOW>(a, cs, window, rank, CL, cluster, dyn, S, &s_bar, phase);
+  const Group G = {(int)threadIdx.x, (int)blockDim.x, 0u};
+  unsigned dyn_size;
+  asm("mov.u32 %0, %%dynamic_smem_size;" : "=r"(dyn_size));
+  const RngTab tab = store.part<2>(0, 2);
+  run_job<KIND, R, SHADOW>(a, cs, window, rank, CL, cluster, G, dyn, dyn_size, S, &s_bar, phase, tab);
 }
 
 // Many independent chains in one persistent launch (the reference's clone
-// parallelism): each CTA takes the next chain from an atomic queue (chains
-// ordered by estimated cost, largest first), copies its job description to
-// shared memory, stages its tables and runs all of its moves for this
-// launch, then takes the next one.
+// parallelism).  Chains are queued by estimated cost, largest first, behind
+// one atomic counter.  A CTA starts as one group of all its threads; a group
+// takes the next chain and, when that chain's queue position is at or past
+// the split point of its level (split[k]) and a finer level exists, halves:
+// the first half keeps the chain, the second half takes a new one.  The
+// costliest chains therefore run on the whole CTA and the cheap tail on
+// 1/2 or 1/4 of it, so the step is not held up by its largest chains while
+// small chains still fill the SMs.  Group (k, p) — level k, position p —
+// owns threads [p, p+1) * blockDim/2^k, named barrier 2^k + p, and the
+// per-slot shared state of slot p * 2^(max_split-k) (its table copy
+// included).
+constexpr size_t kBatchStoreBytes = (sizeof(RngStore<1 << kMaxSplit>) + 15) & ~(size_t)15;
+
 template <int KIND, typename R, bool SHADOW>
-__global__ void __launch_bounds__(256, 2) batch_kernel(BatchArgs b) {
-  __shared__ KernelShared S;
-  __shared__ BisectionArgs job;
-  __shared__ int s_chain;
-  __shared__ __align__(8) uint64_t s_bar;
-  extern __shared__ __align__(16) unsigned char dyn[];
+__global__ void __launch_bounds__(512, 1) batch_kernel(BatchArgs b) {
+  constexpr int kSlots = 1 << kMaxSplit;
+  __shared__ KernelShared S[kSlots];
+  __shared__ BisectionArgs jobs[kSlots];
+  __shared__ int s_chain[kSlots];
+  __shared__ __align__(8) uint64_t s_bar[kSlots];
+  extern __shared__ __align__(16) unsigned char dyn_all[];
+  // dynamic shared memory: the stream tables, then the slots' staged tables
+  RngStore<kSlots> &store = *reinterpret_cast<RngStore<kSlots> *>(dyn_all);
+  unsigned char *dyn = dyn_all + kBatchStoreBytes;
   cg::cluster_group cluster = cg::this_cluster();
-  if (threadIdx.x == 0) {
-    mbar_init(&s_bar, 1);
+  if (threadIdx.x < kSlots) {
+    mbar_init(&s_bar[threadIdx.x], 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   __syncthreads();
+  int k = 0, p = 0;
+  int c = -1;  // queue position in hand (group-uniform)
   unsigned phase = 0;
-  for (int guard = 0; guard < b.n_chains + 1; guard++) {
-    if (threadIdx.x == 0) s_chain = (int)atomicAdd(b.queue, 1u);
-    __syncthreads();
-    const int c = s_chain;
-    if (c >= b.n_chains) break;
+  for (int guard = 0; guard < 2 * b.n_chains + 2 * kSlots + 2; guard++) {
+    const int gsize = (int)blockDim.x >> k;
+    const Group G = {(int)threadIdx.x - p * gsize, gsize, (1u << k) + (unsigned)p};
+    const int slot = p << (b.max_split - k);
+    if (c < 0) {
+      if (G.tid == 0) s_chain[slot] = (int)atomicAdd(b.queue, 1u);
+      G.sync();
+      c = s_chain[slot];
+      G.sync();  // s_chain[slot] is rewritten only after every thread read it
+      if (c >= b.n_chains) break;
+    }
+    if (k < b.max_split && c >= b.split[k]) {
+      const int half = gsize >> 1;
+      const int second = G.tid >= half ? 1 : 0;
+      k++;
+      p = 2 * p + second;
+      if (second) {
+        c = -1;
+        phase = 0;  // this half's slot has an unused mbarrier
+      }
+      continue;
+    }
     const int chain = b.order[c];
+    BisectionArgs &job = jobs[slot];
     {
       const int *src = reinterpret_cast<const int *>(b.jobs + chain);
       int *dst = reinterpret_cast<int *>(&job);
-      for (int i = threadIdx.x; i < (int)(sizeof(BisectionArgs) / sizeof(int)); i += blockDim.x) dst[i] = src[i];
+      for (int i = G.tid; i < (int)(sizeof(BisectionArgs) / sizeof(int)); i += gsize) dst[i] = src[i];
     }
-    __syncthreads();
-    if (threadIdx.x == 0) {
+    G.sync();
+    if (G.tid == 0) {
       job.n_blocks = b.n_blocks;
       job.trace = b.trace ? b.trace + (long long)chain * b.trace_per_chain : nullptr;
       job.trace_offset = 0;
     }
-    __syncthreads();
-    run_job<KIND, R, SHADOW>(job, job.chains, 0, 0, 1, cluster, dyn, S, &s_bar, phase);
+    G.sync();
+    const RngTab tab = store.part<kSlots>(p << (kMaxSplit - k), 1 << (kMaxSplit - k));
+    run_job<KIND, R, SHADOW>(job, job.chains, 0, 0, 1, cluster, G, dyn + (size_t)slot * b.dyn_per_slot,
+                             b.dyn_per_slot, S[slot], &s_bar[slot], phase, tab);
+    c = -1;
   }
 }
 
@@ -808,6 +916,7 @@ cudaError_t bisection_occupancy(const BisectionArgs &a, int precision, int shado
 template <int KIND, typename R, bool SHADOW>
 static cudaError_t launch_batch_t(const BatchArgs &b, int blocks, int threads, size_t dyn, cudaStream_t st) {
   auto kfn = batch_kernel<KIND, R, SHADOW>;
+  dyn += kBatchStoreBytes;
   cudaError_t e = cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn);
   if (e != cudaSuccess) return e;
   kfn<<<blocks, threads, dyn, st>>>(b);
@@ -816,8 +925,11 @@ static cudaError_t launch_batch_t(const BatchArgs &b, int blocks, int threads, s
 
 cudaError_t launch_batch(const BatchArgs &b, int precision, int shadow, int blocks, int threads, size_t dyn,
                          cudaStream_t st) {
-  if (dyn > (size_t)100 * 1024) return cudaErrorInvalidValue;  // two CTAs per SM must fit
-  if (threads < 64 || threads > 256 || threads % 32 || blocks < 1) return cudaErrorInvalidValue;
+  if (b.max_split < 0 || b.max_split > kMaxSplit || b.dyn_per_slot % 16 ||
+      dyn < ((size_t)b.dyn_per_slot << b.max_split) || dyn + kBatchStoreBytes > (size_t)180 * 1024)
+    return cudaErrorInvalidValue;
+  if (threads < 64 || threads > 512 || (threads >> b.max_split) % 32 || (threads >> b.max_split) < 64 || blocks < 1)
+    return cudaErrorInvalidValue;
   if (precision == PIMC_MIXED)
     return shadow ? launch_batch_t<PA_DAVID, float, true>(b, blocks, threads, dyn, st)
                   : launch_batch_t<PA_DAVID, float, false>(b, blocks, threads, dyn, st);
@@ -828,6 +940,7 @@ cudaError_t launch_batch(const BatchArgs &b, int precision, int shadow, int bloc
 template <int KIND, typename R, bool SHADOW>
 static cudaError_t batch_occupancy_t(int threads, size_t dyn, int *blocks_per_sm) {
   auto kfn = batch_kernel<KIND, R, SHADOW>;
+  dyn += kBatchStoreBytes;
   cudaError_t e = cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn);
   if (e != cudaSuccess) return e;
   return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, kfn, threads, dyn);

@@ -24,6 +24,8 @@ cudaError_t bisection_occupancy(const BisectionArgs &a, int precision, int shado
 // Many chains in one persistent launch: jobs[] (one sequential-schedule job
 // per chain, each with its own path, tables and ChainState), taken in the
 // order order[] through the atomic counter *queue (zero at launch).
+constexpr int kMaxSplit = 2;  // a CTA runs up to 2^kMaxSplit chains side by side
+
 struct BatchArgs {
   const BisectionArgs *jobs;
   const int *order;
@@ -32,6 +34,9 @@ struct BatchArgs {
   int n_blocks;                 // blocks of moves each chain runs in this launch
   pimc_move_record *trace;      // [chain][n_blocks * steps_per_block] or nullptr
   long long trace_per_chain;
+  int max_split;                // finest group level used, 0..kMaxSplit
+  int split[kMaxSplit];         // queue positions from which level k+1 groups run the chains
+  unsigned dyn_per_slot;        // shared-memory bytes of one slot's staged tables (multiple of 16)
 };
 
 cudaError_t launch_batch(const BatchArgs &b, int precision, int shadow, int blocks, int threads, size_t dyn,

@@ -53,14 +53,47 @@ struct SplineCell {
   int low, hi;
   R a, b, a3, b3, h26;
 };
+// Round to nearest even by the magic-constant addition (exact for
+// |t| < 2^22 in FP32, 2^51 in FP64; larger |t| only feeds the clamps below,
+// which send it to the first or last cell like the integer path does), and
+// the integer of an integral value in [0, 2^22).  These keep the cell search
+// on the FMA pipe instead of float-int conversions.
+__device__ __forceinline__ float round_even_magic(float t) {
+  return __fadd_rn(__fadd_rn(t, 12582912.0f), -12582912.0f);
+}
+__device__ __forceinline__ double round_even_magic(double t) {
+  return __dadd_rn(__dadd_rn(t, 6755399441055744.0), -6755399441055744.0);
+}
+__device__ __forceinline__ int int_of_integral(float v) { return __float_as_int(__fadd_rn(v, 12582912.0f)) - 0x4B400000; }
+__device__ __forceinline__ int int_of_integral(double v) {
+  return (int)(__double_as_longlong(__dadd_rn(v, 6755399441055744.0)) - 0x4338000000000000LL);
+}
+__device__ __forceinline__ float fmax_r(float a, float b) { return fmaxf(a, b); }
+__device__ __forceinline__ double fmax_r(double a, double b) { return fmax(a, b); }
+__device__ __forceinline__ float fmin_r(float a, float b) { return fminf(a, b); }
+__device__ __forceinline__ double fmin_r(double a, double b) { return fmin(a, b); }
+
 template <typename R>
 __device__ __forceinline__ SplineCell<R> spline_cell(const DGrid<R> &g, R x) {
   SplineCell<R> c;
-  int hi = reverse_map(g, x) + 1;
-  int low = hi - 1;
-  if (low < 0) { low = 0; hi = 1; }
-  if (hi > (g.n - 1)) { hi = g.n - 1; low = hi - 1; }
-  R xl = grid_x(g, low), xh = grid_x(g, hi);
+  int low, hi;
+  R xl, xh;
+  if (g.type == PIMC_GRID_LINEAR) {
+    // low = clamp(ReverseMap(x), 0, n-2), hi = low + 1, as integers held in R
+    const R rm = round_even_magic(rsub(rmul(rsub(x, g.start), g.deltainv), R(0.5)));
+    const R lowf = fmin_r(fmax_r(rm, R(0)), (R)(g.n - 2));
+    low = int_of_integral(lowf);
+    hi = low + 1;
+    xl = radd(g.start, rmul(lowf, g.delta));
+    xh = radd(g.start, rmul(radd(lowf, R(1)), g.delta));
+  } else {
+    hi = reverse_map(g, x) + 1;
+    low = hi - 1;
+    if (low < 0) { low = 0; hi = 1; }
+    if (hi > (g.n - 1)) { hi = g.n - 1; low = hi - 1; }
+    xl = grid_x(g, low);
+    xh = grid_x(g, hi);
+  }
   // A linear grid's cell width is delta (X(hi) - X(low) differs from it by a
   // rounding), so its inverse is the precomputed deltainv; a = 1 - b keeps the
   // two weights summing to one in either precision.
@@ -107,7 +140,7 @@ __device__ __forceinline__ R spline_pairs(const DGrid<R> &g, const typename Pair
 // ---- DavidPAClass::calcUsqzFast (DavidPAClass.cc:468-511) ----
 // diag: column 1 of ukj(level+TauPos) as (y, d2y) pairs (global or shared).
 template <typename R>
-__device__ __forceinline__ R david_U(const DDavid<R> &d, const typename Pair2<R>::T *diag, R s, R q, R z,
+__device__ __forceinline__ R david_U(const DDavid<R> &d, const typename Pair2<R>::T *diag, R s2, R q, R z,
                                      int level) {
   level = level + d.tau_pos;
   const DGrid<R> &g = d.grid;
@@ -118,7 +151,8 @@ __device__ __forceinline__ R david_U(const DDavid<R> &d, const typename Pair2<R>
   if (rprime > g.end) rprime = g.end;
   if ((rprime < rmin) || (r < rmin)) return spline_pairs(g, diag, rmin);
   R U = R(0.5) * (spline_pairs(g, diag, r) + spline_pairs(g, diag, rprime));
-  if (d.num_terms > 0 && s > R(0) && q < g.end) {
+  if (d.num_terms > 0 && s2 > R(0) && q < g.end) {
+    const R s = sqrt_r(s2);  // s is needed only by the off-diagonal terms
     const R *y = d.uy + (size_t)level * g.n * d.ncols;
     const R *d2 = d.ud2 + (size_t)level * g.n * d.ncols;
     SplineCell<R> c = spline_cell(g, q);
@@ -145,7 +179,7 @@ __device__ __forceinline__ R david_U(const DDavid<R> &d, const typename Pair2<R>
 
 // ---- DavidPAClass::calcUsqz, dU output (DavidPAClass.cc:291-463) ----
 template <typename R>
-__device__ __forceinline__ R david_dU(const DDavid<R> &d, R s, R q, R z, int level) {
+__device__ __forceinline__ R david_dU(const DDavid<R> &d, R s2, R q, R z, int level) {
   level = level + d.tau_pos;
   const DGrid<R> &g = d.grid;
   const R *uy = d.uy + (size_t)level * g.n * d.ncols;
@@ -162,7 +196,8 @@ __device__ __forceinline__ R david_dU(const DDavid<R> &d, R s, R q, R z, int lev
   R V = R(0.5) * (spline_col(g, uy, ud2, d.ncols, 0, r) + spline_col(g, uy, ud2, d.ncols, 0, rprime));
   R dU = R(0.5) * (spline_col(g, dy, dd2, d.ncols, 1, r) + spline_col(g, dy, dd2, d.ncols, 1, rprime));
   dU += V;
-  if (d.num_terms > 0 && s > R(0) && q < g.end) {
+  if (d.num_terms > 0 && s2 > R(0) && q < g.end) {
+    const R s = sqrt_r(s2);
     SplineCell<R> c = spline_cell(g, q);
     R zsquared = z * z;
     R ssquared = s * s;
@@ -344,7 +379,7 @@ __device__ __forceinline__ void put_in_box_fast(double v[3], const DevSystem &s)
 // forms them (ShortRangeClass.cc:217-220).
 template <typename R>
 struct LinkGeom {
-  R q, z, s2, s, rmag, rpmag;
+  R q, z, s2, rmag, rpmag;
 };
 template <typename R>
 __device__ __forceinline__ LinkGeom<R> link_geom(const double dA[3], const double dB[3]) {
@@ -357,7 +392,6 @@ __device__ __forceinline__ LinkGeom<R> link_geom(const double dA[3], const doubl
   g.s2 = d0 * d0 + d1 * d1 + d2 * d2;
   g.q = R(0.5) * (rmag + rpmag);
   g.z = (rmag - rpmag);
-  g.s = sqrt_r(g.s2);
   g.rmag = rmag;
   g.rpmag = rpmag;
   return g;
@@ -377,12 +411,12 @@ __device__ __forceinline__ R pa_U(const DevPA &pa, const typename Pair2<R>::T *d
 template <>
 __device__ __forceinline__ double pa_U<double, PA_DAVID>(const DevPA &pa, const double2 *diag,
                                                          const LinkGeom<double> &g, int level) {
-  return david_U<double>(pa.d64, diag, g.s, g.q, g.z, level);
+  return david_U<double>(pa.d64, diag, g.s2, g.q, g.z, level);
 }
 template <>
 __device__ __forceinline__ float pa_U<float, PA_DAVID>(const DevPA &pa, const float2 *diag,
                                                        const LinkGeom<float> &g, int level) {
-  return david_U<float>(pa.d32, diag, g.s, g.q, g.z, level);
+  return david_U<float>(pa.d32, diag, g.s2, g.q, g.z, level);
 }
 template <>
 __device__ __forceinline__ double pa_U<double, PA_TRICUBIC>(const DevPA &pa, const double2 *,
@@ -418,7 +452,7 @@ template <int KIND>
 __device__ __forceinline__ double pa_dU(const DevPA &pa, const LinkGeom<double> &g, int level);
 template <>
 __device__ __forceinline__ double pa_dU<PA_DAVID>(const DevPA &pa, const LinkGeom<double> &g, int level) {
-  return david_dU<double>(pa.d64, g.s, g.q, g.z, level);
+  return david_dU<double>(pa.d64, g.s2, g.q, g.z, level);
 }
 template <>
 __device__ __forceinline__ double pa_dU<PA_TRICUBIC>(const DevPA &pa, const LinkGeom<double> &g, int level) {
@@ -464,7 +498,7 @@ __device__ __forceinline__ void philox4x32_10(uint32_t c[4], uint32_t k0, uint32
   }
 }
 // Element `index` of stream `stream`: two 53-bit doubles per Philox block.
-__device__ __forceinline__ double philox_uniform(uint64_t seed, uint32_t stream, uint64_t index) {
+static __device__ __noinline__ double philox_uniform(uint64_t seed, uint32_t stream, uint64_t index) {
   uint64_t block = index >> 1;
   uint32_t c[4] = {(uint32_t)block, (uint32_t)(block >> 32), stream, 0x50494D43u};
   philox4x32_10(c, (uint32_t)seed, (uint32_t)(seed >> 32));
@@ -472,6 +506,20 @@ __device__ __forceinline__ double philox_uniform(uint64_t seed, uint32_t stream,
   uint32_t a = (h ? c[2] : c[0]) >> 5, b = (h ? c[3] : c[1]) >> 6;
   return ((double)a * 67108864.0 + (double)b) * (1.0 / 9007199254740992.0);
 }
+
+// Stream values precomputed for the positions [tb, tb + W) of one Local
+// stream (an even tb): the uniform u (u also holds position tb + W), log u,
+// and the polar-method pair (X1, X2, accepted) of the candidate pair starting
+// at each position.  A CTA fills it with all of its threads at once, so the
+// sampler warps, which draw sequentially, read these values instead of
+// computing Philox blocks, logarithms and square roots on their critical
+// path.  Entries are what the direct computation gives, bit for bit.
+struct RngTab {
+  double *u, *lu, *x1, *x2;
+  unsigned char *acc;
+  uint64_t tb;
+  int W;  // 0: no table
+};
 
 // RandomClass (Common/Random/Random.h:33-49,156-180): Local(), LocalInt(),
 // LocalGaussian() with the polar-method pair cache.  Every lane of a warp
@@ -481,9 +529,72 @@ struct DevRandom {
   uint32_t stream;
   int one_left;
   double x2;
-  __device__ __forceinline__ double Local() { return philox_uniform(seed, stream, n++); }
+  const RngTab *tab;
+  __device__ __forceinline__ double Local() {
+    if (tab) {
+      const uint64_t k = n - tab->tb;
+      if (k < (uint64_t)tab->W) {
+        n++;
+        return tab->u[k];
+      }
+    }
+    return philox_uniform(seed, stream, n++);
+  }
+  // log(Local()), the acceptance draw of a stage.
+  __device__ __forceinline__ double LocalLog() {
+    if (tab) {
+      const uint64_t k = n - tab->tb;
+      if (k < (uint64_t)tab->W) {
+        n++;
+        return tab->lu[k];
+      }
+    }
+    return log(philox_uniform(seed, stream, n++));
+  }
   __device__ __forceinline__ int LocalInt(int max) { return (int)floor(Local() * max); }
 };
+
+// The polar-method transform of one candidate pair (u1, u2).
+__device__ __forceinline__ void polar_pair(double u1, double u2, bool &acc, double &X1, double &X2) {
+  const double V1 = 2.0 * u1 - 1.0;
+  const double V2 = 2.0 * u2 - 1.0;
+  const double S = V1 * V1 + V2 * V2;
+  acc = !(S >= 1.0);
+  const double temp = sqrt((-2.0 * log(S)) / S);
+  X1 = V1 * temp;
+  X2 = V2 * temp;
+}
+
+// Fills t for the positions from (from & ~1), by the `size` threads whose
+// index in the group is `gtid`; `sync` is the group's barrier.
+template <typename Sync>
+__device__ void rng_tab_fill(RngTab &t, int W, uint64_t seed, uint32_t stream, uint64_t from, int gtid, int size,
+                             const Sync &sync) {
+  const uint64_t tb = from & ~1ull;
+  for (int i = gtid; i <= (W >> 1); i += size) {
+    const uint64_t blk = (tb >> 1) + (uint64_t)i;
+    uint32_t c[4] = {(uint32_t)blk, (uint32_t)(blk >> 32), stream, 0x50494D43u};
+    philox4x32_10(c, (uint32_t)seed, (uint32_t)(seed >> 32));
+    t.u[2 * i] = ((double)(c[0] >> 5) * 67108864.0 + (double)(c[1] >> 6)) * (1.0 / 9007199254740992.0);
+    t.u[2 * i + 1] = ((double)(c[2] >> 5) * 67108864.0 + (double)(c[3] >> 6)) * (1.0 / 9007199254740992.0);
+  }
+  sync();
+  for (int k = gtid; k < W; k += size) {
+    const double u1 = t.u[k], u2 = t.u[k + 1];
+    t.lu[k] = log(u1);
+    bool acc;
+    double X1, X2;
+    polar_pair(u1, u2, acc, X1, X2);
+    t.acc[k] = acc ? 1 : 0;
+    t.x1[k] = X1;
+    t.x2[k] = X2;
+  }
+  if (gtid == 0) {
+    t.tb = tb;
+    t.W = W;
+  }
+  sync();
+}
 
 // G unit Gaussians in stream order into out[0..G-1], drawn by one full warp.
 // Sequentially, LocalGaussian returns the cached X2 if one is left, else
@@ -491,8 +602,9 @@ struct DevRandom {
 // X1 = V1 t, caching X2 = V2 t, t = sqrt(-2 ln S / S).  Here lane j tests the
 // candidate pair at stream offset 2j; a ballot orders the accepted pairs, so
 // the values, the cache and the stream position come out exactly as the
-// sequential loop leaves them.  Bounded: at most 4096 rounds of 32 pairs.
-__device__ __forceinline__ void warp_gaussians(DevRandom &rng, int G, double *out, int lane) {
+// sequential loop leaves them.  Candidate pairs inside the precomputed table
+// are read from it.  Bounded: at most 4096 rounds of 32 pairs.
+static __device__ __noinline__ void warp_gaussians(DevRandom &rng, int G, double *out, int lane) {
   int k = 0;
   if (G > 0 && rng.one_left) {
     if (lane == 0) out[0] = rng.x2;
@@ -501,32 +613,37 @@ __device__ __forceinline__ void warp_gaussians(DevRandom &rng, int G, double *ou
   }
   for (int guard = 0; k < G && guard < 4096; guard++) {
     const int need = (G - k + 1) >> 1;
-    // Candidate pair j uses uniforms n+2j and n+2j+1.  Lane j computes the
-    // Philox block holding uniform n+2j (two uniforms per block); when n is
-    // odd the second uniform is the first half of the next lane's block.
-    const uint64_t b0 = (rng.n >> 1) + (uint64_t)lane;
-    uint32_t c[4] = {(uint32_t)b0, (uint32_t)(b0 >> 32), rng.stream, 0x50494D43u};
-    philox4x32_10(c, (uint32_t)rng.seed, (uint32_t)(rng.seed >> 32));
-    const double h0 = ((double)(c[0] >> 5) * 67108864.0 + (double)(c[1] >> 6)) * (1.0 / 9007199254740992.0);
-    const double h1 = ((double)(c[2] >> 5) * 67108864.0 + (double)(c[3] >> 6)) * (1.0 / 9007199254740992.0);
-    double u1, u2;
-    if ((rng.n & 1) == 0) {
-      u1 = h0;
-      u2 = h1;
+    bool acc;
+    double X1, X2;
+    const uint64_t kt = rng.tab ? rng.n + 2ull * (uint64_t)lane - rng.tab->tb : ~0ull;
+    const bool in_tab = rng.tab && kt < (uint64_t)rng.tab->W;
+    if (__all_sync(0xffffffffu, in_tab)) {
+      acc = rng.tab->acc[kt] != 0;
+      X1 = rng.tab->x1[kt];
+      X2 = rng.tab->x2[kt];
     } else {
-      u1 = h1;
-      u2 = __shfl_down_sync(0xffffffffu, h0, 1);
-      if (lane == 31) u2 = philox_uniform(rng.seed, rng.stream, rng.n + 2ull * 31 + 1);
+      // Candidate pair j uses uniforms n+2j and n+2j+1.  Lane j computes the
+      // Philox block holding uniform n+2j (two uniforms per block); when n is
+      // odd the second uniform is the first half of the next lane's block.
+      const uint64_t b0 = (rng.n >> 1) + (uint64_t)lane;
+      uint32_t c[4] = {(uint32_t)b0, (uint32_t)(b0 >> 32), rng.stream, 0x50494D43u};
+      philox4x32_10(c, (uint32_t)rng.seed, (uint32_t)(rng.seed >> 32));
+      const double h0 = ((double)(c[0] >> 5) * 67108864.0 + (double)(c[1] >> 6)) * (1.0 / 9007199254740992.0);
+      const double h1 = ((double)(c[2] >> 5) * 67108864.0 + (double)(c[3] >> 6)) * (1.0 / 9007199254740992.0);
+      double u1, u2;
+      if ((rng.n & 1) == 0) {
+        u1 = h0;
+        u2 = h1;
+      } else {
+        u1 = h1;
+        u2 = __shfl_down_sync(0xffffffffu, h0, 1);
+        if (lane == 31) u2 = philox_uniform(rng.seed, rng.stream, rng.n + 2ull * 31 + 1);
+      }
+      polar_pair(u1, u2, acc, X1, X2);
     }
-    const double V1 = 2.0 * u1 - 1.0;
-    const double V2 = 2.0 * u2 - 1.0;
-    const double S = V1 * V1 + V2 * V2;
-    const bool acc = !(S >= 1.0);
     const unsigned m = __ballot_sync(0xffffffffu, acc);
     const int before = __popc(m & ((1u << lane) - 1u));
     const int navail = __popc(m);
-    const double temp = sqrt((-2.0 * log(S)) / S);
-    const double X1 = V1 * temp, X2 = V2 * temp;
     if (acc && before < need) {
       const int idx = k + 2 * before;
       out[idx] = X1;

@@ -89,7 +89,7 @@ __global__ void __launch_bounds__(256) sr_single_noalloc_kernel(const double *__
     }
     dist_disp(a1, a2, b1, b2, sys, dA, dB);
     const LinkGeom<double> g = link_geom<double>(dA, dB);
-    acc += david_U<double>(d, diag, g.s, g.q, g.z, level);
+    acc += david_U<double>(d, diag, g.s2, g.q, g.z, level);
   }
   const double r = na_block_sum(acc, sh);
   if (threadIdx.x == 0) {

@@ -38,10 +38,14 @@ def oracle_run(c, n_blocks):
     return recs, s.get_path(0), pa
 
 
-@pytest.mark.parametrize("threads", [64, 128, 256])
-def test_batch_matches_oracle_per_chain(threads):
+@pytest.mark.parametrize("threads,max_split,ratio", [(64, 0, 0.5), (128, 0, 0.5), (256, 0, 0.5), (256, 2, 0.5),
+                                                     (512, 1, 0.5), (512, 2, 0.75)])
+def test_batch_matches_oracle_per_chain(threads, max_split, ratio):
+    """Whatever group size runs a chain (whole CTA, half or quarter), its
+    trace and final path equal the oracle's sequential run of that chain."""
     chains = make_chains()
-    b = P.BatchChains(chains, precision=P.FP64, threads_per_cta=threads, ctas=5)
+    b = P.BatchChains(chains, precision=P.FP64, threads_per_cta=threads, ctas=5, max_split=max_split,
+                      split_ratio=ratio)
     n_blocks = 25
     trace, stats = b.run(n_blocks, trace=True)
     total = 0
@@ -73,7 +77,8 @@ def test_batch_autotune_keeps_state_and_graph_replay_matches_oracle():
     chains = make_chains()
     b = P.BatchChains(chains, precision=P.FP64)
     tune = b.autotune(3)
-    assert tune["threads_per_cta"] in (64, 96, 128, 160, 192, 256) and tune["ctas"] >= 1
+    assert tune["threads_per_cta"] in (128, 256, 384, 512) and tune["ctas"] >= 1
+    assert tune["max_split"] in (0, 1, 2)
     for _ in range(3):  # the same launch replayed from its CUDA graph
         b.run_async(5)
     b.synchronize()
