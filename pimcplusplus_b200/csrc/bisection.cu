@@ -143,6 +143,19 @@ __device__ __forceinline__ double sample_level_warp(double (*w_old)[3], double (
   __syncwarp();
   return -ln + lo;
 }
+__device__ __noinline__ double sample_level_warp_outlined(double (*w_old)[3], double (*w_new)[3], double *gbuf,
+                                                          int num_levels, int level, const DevSystem &s,
+                                                          DevRandom &rng, int lane) {
+  return sample_level_warp(w_old, w_new, gbuf, num_levels, level, s, rng, lane);
+}
+// The level sampler: one out-of-line copy (OUTLINE: fewer cold instruction
+// lines per stage when a CTA runs many short jobs) or inlined at each call.
+template <bool OUTLINE>
+__device__ __forceinline__ double sample_level(double (*w_old)[3], double (*w_new)[3], double *gbuf, int num_levels,
+                                               int level, const DevSystem &s, DevRandom &rng, int lane) {
+  return OUTLINE ? sample_level_warp_outlined(w_old, w_new, gbuf, num_levels, level, s, rng, lane)
+                 : sample_level_warp(w_old, w_new, gbuf, num_levels, level, s, rng, lane);
+}
 
 }  // namespace
 
@@ -380,7 +393,7 @@ struct Group {
 // The moves of one job — one chain, or one window of a chain — on this CTA
 // (cluster rank `rank` of `CL`).  `phase` is the parity of the table-staging
 // mbarrier `bar`, flipped once per staging.
-template <int KIND, typename R, bool SHADOW>
+template <int KIND, typename R, bool SHADOW, bool OUTLINE>
 __device__ void run_job(const BisectionArgs &a, ChainState *cs, int window, unsigned rank, unsigned CL,
                         cg::cluster_group &cluster, const Group &G, unsigned char *dyn, unsigned dyn_cap,
                         KernelShared &S, uint64_t *bar_ptr, unsigned &phase, const RngTab &tab_mem) {
@@ -539,7 +552,7 @@ __device__ void run_job(const BisectionArgs &a, ChainState *cs, int window, unsi
       G.sync();
       if (warp == sampler) {
         DevRandom rng = rng_from(s_rng, seed, stream, &S.tab);
-        const double lsr = sample_level_warp(win_old[cur], win_new[cur], gbuf[0], L, L - 1, sys, rng, lane);
+        const double lsr = sample_level<OUTLINE>(win_old[cur], win_new[cur], gbuf[0], L, L - 1, sys, rng, lane);
         const double lu = rng.LocalLog();
         __syncwarp();
         if (lane == 0) {
@@ -587,7 +600,7 @@ __device__ void run_job(const BisectionArgs &a, ChainState *cs, int window, unsi
         if (warp == sampler && level > 0) {
           // speculative sampling of the next level (BisectionStage::Sample of stage level-1)
           DevRandom spec = rng_from(s_rng, seed, stream, &S.tab);
-          const double lsr = sample_level_warp(w_old, w_new, gbuf[0], L, level - 1, sys, spec, lane);
+          const double lsr = sample_level<OUTLINE>(w_old, w_new, gbuf[0], L, level - 1, sys, spec, lane);
           const double lu = spec.LocalLog();
           __syncwarp();
           if (lane == 0) {
@@ -608,7 +621,7 @@ __device__ void run_job(const BisectionArgs &a, ChainState *cs, int window, unsi
             for (int i = 0; i < 3; i++) wo[rel][i] = wn[rel][i] = __ldcg(q + i);
           }
           __syncwarp();
-          const double lsr = sample_level_warp(wo, wn, gbuf[1], L, L - 1, sys, spec, lane);
+          const double lsr = sample_level<OUTLINE>(wo, wn, gbuf[1], L, L - 1, sys, spec, lane);
           const double lu = spec.LocalLog();
           __syncwarp();
           if (lane == 0) {
@@ -769,7 +782,7 @@ __global__ void __launch_bounds__(512, 1) bisection_kernel(BisectionArgs a) {
   unsigned dyn_size;
   asm("mov.u32 %0, %%dynamic_smem_size;" : "=r"(dyn_size));
   const RngTab tab = store.part<2>(0, 2);
-  run_job<KIND, R, SHADOW>(a, cs, window, rank, CL, cluster, G, dyn, dyn_size, S, &s_bar, phase, tab);
+  run_job<KIND, R, SHADOW, false>(a, cs, window, rank, CL, cluster, G, dyn, dyn_size, S, &s_bar, phase, tab);
 }
 
 // Many independent chains in one persistent launch (the reference's clone
@@ -843,7 +856,7 @@ __global__ void __launch_bounds__(512, 1) batch_kernel(BatchArgs b) {
     }
     G.sync();
     const RngTab tab = store.part<kSlots>(p << (kMaxSplit - k), 1 << (kMaxSplit - k));
-    run_job<KIND, R, SHADOW>(job, job.chains, 0, 0, 1, cluster, G, dyn + (size_t)slot * b.dyn_per_slot,
+    run_job<KIND, R, SHADOW, true>(job, job.chains, 0, 0, 1, cluster, G, dyn + (size_t)slot * b.dyn_per_slot,
                              b.dyn_per_slot, S[slot], &s_bar[slot], phase, tab);
     c = -1;
   }

@@ -138,6 +138,36 @@ __device__ __forceinline__ R spline_pairs(const DGrid<R> &g, const typename Pair
 }
 
 // ---- DavidPAClass::calcUsqzFast (DavidPAClass.cc:468-511) ----
+// U plus the off-diagonal terms Ucof_kj(q) z^2j s^(2k-2j), k = 1..NumTerms,
+// j = 0..k, added one by one in the reference's order.  Out of line: the
+// diagonal-only tables never take it and the hot item loops stay compact.
+// Arguments are plain values so that no parameter-space struct is copied to
+// local memory for the call.
+template <typename R>
+__device__ __noinline__ R david_offdiag_add(DGrid<R> g, const R *y, const R *d2, int ncols, int num_terms, R U, R s2,
+                                            R q, R z) {
+  const R s = sqrt_r(s2);
+  SplineCell<R> c = spline_cell(g, q);
+  R zsquared = z * z;
+  R ssquared = s * s;
+  R ssquaredinverse = R(1.0) / ssquared;
+  R Sto2k = ssquared;
+  for (int k = 1; k <= num_terms; k++) {
+    R Zto2j = 1;
+    R currS = Sto2k;
+    for (int j = 0; j <= k; j++) {
+      int col = k * (k + 1) / 2 + j + 1;
+      R Ucof = spline_apply(c, __ldg(&y[c.low * ncols + col]), __ldg(&y[c.hi * ncols + col]),
+                            __ldg(&d2[c.low * ncols + col]), __ldg(&d2[c.hi * ncols + col]));
+      U += Ucof * Zto2j * currS;
+      Zto2j *= zsquared;
+      currS = currS * ssquaredinverse;
+    }
+    Sto2k = Sto2k * ssquared;
+  }
+  return U;
+}
+
 // diag: column 1 of ukj(level+TauPos) as (y, d2y) pairs (global or shared).
 template <typename R>
 __device__ __forceinline__ R david_U(const DDavid<R> &d, const typename Pair2<R>::T *diag, R s2, R q, R z,
@@ -151,29 +181,9 @@ __device__ __forceinline__ R david_U(const DDavid<R> &d, const typename Pair2<R>
   if (rprime > g.end) rprime = g.end;
   if ((rprime < rmin) || (r < rmin)) return spline_pairs(g, diag, rmin);
   R U = R(0.5) * (spline_pairs(g, diag, r) + spline_pairs(g, diag, rprime));
-  if (d.num_terms > 0 && s2 > R(0) && q < g.end) {
-    const R s = sqrt_r(s2);  // s is needed only by the off-diagonal terms
-    const R *y = d.uy + (size_t)level * g.n * d.ncols;
-    const R *d2 = d.ud2 + (size_t)level * g.n * d.ncols;
-    SplineCell<R> c = spline_cell(g, q);
-    R zsquared = z * z;
-    R ssquared = s * s;
-    R ssquaredinverse = R(1.0) / ssquared;
-    R Sto2k = ssquared;
-    for (int k = 1; k <= d.num_terms; k++) {
-      R Zto2j = 1;
-      R currS = Sto2k;
-      for (int j = 0; j <= k; j++) {
-        int col = k * (k + 1) / 2 + j + 1;
-        R Ucof = spline_apply(c, __ldg(&y[c.low * d.ncols + col]), __ldg(&y[c.hi * d.ncols + col]),
-                              __ldg(&d2[c.low * d.ncols + col]), __ldg(&d2[c.hi * d.ncols + col]));
-        U += Ucof * Zto2j * currS;
-        Zto2j *= zsquared;
-        currS = currS * ssquaredinverse;
-      }
-      Sto2k = Sto2k * ssquared;
-    }
-  }
+  if (d.num_terms > 0 && s2 > R(0) && q < g.end)
+    U = david_offdiag_add<R>(g, d.uy + (size_t)level * g.n * d.ncols, d.ud2 + (size_t)level * g.n * d.ncols, d.ncols,
+                             d.num_terms, U, s2, q, z);
   return U;
 }
 
@@ -568,7 +578,7 @@ __device__ __forceinline__ void polar_pair(double u1, double u2, bool &acc, doub
 // Fills t for the positions from (from & ~1), by the `size` threads whose
 // index in the group is `gtid`; `sync` is the group's barrier.
 template <typename Sync>
-__device__ void rng_tab_fill(RngTab &t, int W, uint64_t seed, uint32_t stream, uint64_t from, int gtid, int size,
+__device__ __noinline__ void rng_tab_fill(RngTab &t, int W, uint64_t seed, uint32_t stream, uint64_t from, int gtid, int size,
                              const Sync &sync) {
   const uint64_t tb = from & ~1ull;
   for (int i = gtid; i <= (W >> 1); i += size) {
