@@ -266,9 +266,6 @@ def run_ours(args):
         d.synchronize()
         s0 = bb.stats()
         times = []
-        sampler = ClockSampler(local) if rank == 0 else None
-        if sampler:
-            sampler.start()
         if dist:
             dist.barrier()
         torch.cuda.synchronize()
@@ -285,14 +282,13 @@ def run_ours(args):
         torch.cuda.synchronize()
         if dist:
             dist.barrier()
-        clocks = sampler.stop() if sampler else None
         s1 = bb.stats()
         if s1["status"]:
             raise RuntimeError(f"device status {s1['status']}")
         ms = float(np.sum(times))
         st = {k: s1[k] - s0[k] for k in ("moves", "accepted", "pair_evals", "stages_attempted")}
         d.close()
-        return ms, st, clocks
+        return ms, st
 
     def agg(ms, st):
         if not dist:
@@ -305,12 +301,17 @@ def run_ours(args):
         return float(t.item()), dict(pair_evals=int(v[0].item()), moves=int(v[1].item()),
                                      accepted=int(v[2].item()))
 
-    ms64, st64, _ = timed(P.FP64)
-    ms32, st32, clocks = timed(P.MIXED)
+    # nvidia-smi samples every 200 ms, so the clocks are sampled over all the
+    # timed legs together (C2 FP64 and mixed, the other schedule, C3)
+    sampler = ClockSampler(local) if rank == 0 else None
+    if sampler:
+        sampler.start()
+    ms64, st64 = timed(P.FP64)
+    ms32, st32 = timed(P.MIXED)
     ms64, st64 = agg(ms64, st64)
     ms32, st32 = agg(ms32, st32)
     other = "sequential" if args.schedule == "windows" else "windows"
-    ms_o, st_o, _ = timed(P.MIXED, schedule=other, steps=2)
+    ms_o, st_o = timed(P.MIXED, schedule=other, steps=2)
     ms_o, st_o = agg(ms_o, st_o)
 
     # dS accuracy of the mixed path: mixed decisions with the FP64 terms alongside
@@ -349,6 +350,9 @@ def run_ours(args):
         e2e_evals_timed = float(v.item())
 
     c3 = None if args.no_c3 else run_c3(args, P, torch, flush, local, rank, world, agg)
+    clocks = sampler.stop() if sampler else None
+    if clocks:
+        clocks["window"] = "all timed legs (C2 FP64, mixed, other schedule, accuracy, e2e, C3)"
 
     if rank == 0:
         peak, peak_kind = load_peaks()
@@ -421,7 +425,12 @@ def run_c3(args, P, torch, flush, local, rank, world, agg):
 
     def timed_batch(precision):
         b = P.BatchChains(chains, device=local, precision=precision)
-        tune = b.autotune(nb)
+        if args.c3_config:
+            t, sp, r = args.c3_config.split(",")
+            b.config(precision, False, int(t), 0, int(sp), float(r))
+            tune = dict(threads_per_cta=int(t), max_split=int(sp), split_ratio=float(r), fixed=True)
+        else:
+            tune = b.autotune(nb)
         stream = torch.cuda.ExternalStream(b.stream, device=f"cuda:{local}")
         for _ in range(args.warmup):
             b.run_async(nb)
@@ -491,11 +500,27 @@ def run_c3(args, P, torch, flush, local, rank, world, agg):
                 "pair_evals_per_s": st["pair_evals"] / s}
 
     r32, r64, p64, p32 = rates(ms32, st32), rates(ms64, st64), rates(pms64, pst64), rates(pms32, pst32)
+    # roofline of the batch kernel: one launch per step (persistent); 1-D pair
+    # evaluation = 56 B of algorithmic gathers in FP32 (partner at 2 slices
+    # 24 B + two spline cells 32 B)
+    peak, peak_kind = load_peaks()
+    evals_per_launch = st32["pair_evals"] / world / args.steps
+    ms_per_launch = ms32 / args.steps
+    achieved = evals_per_launch * 56 / (ms_per_launch / 1000.0) / 1e9
+    traffic = None
+    prof = os.path.join(ROOT, "profiles", "batch_c3_traffic.json")
+    if os.path.exists(prof):
+        with open(prof) as f:
+            traffic = json.load(f).get("dram_bytes_per_pair_eval_mixed", 0) * evals_per_launch
+    roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+            "traffic": traffic, "peak_kind": peak_kind, "bytes_per_eval": 56, "evals_per_launch": evals_per_launch,
+            "ms_per_launch": ms_per_launch, "kernel": "batch_kernel<PA_DAVID,float>",
+            "traffic_source": "profiles/batch_c3_traffic.json (ncu, one launch) scaled by evals"}
     return {
         "workload": f"{len(chains)} LJ He-4 chains, N in {{32..512}}, M in {{16..128}}, T in [1,4] K, "
                     f"rho in [0.018,0.024], primitive u00 on 1000 points, level <= 4, "
                     f"{nb * args.c3_steps_per_block} moves per chain per step",
-        "batched_mixed": dict(r32, ms_per_step=ms32 / args.steps, autotune=tune32),
+        "batched_mixed": dict(r32, ms_per_step=ms32 / args.steps, autotune=tune32, roofline=roof),
         "batched_fp64": dict(r64, ms_per_step=ms64 / args.steps, autotune=tune64),
         "plain_fp64": dict(p64, chains_sampled=len(sample), note="one chain at a time, single-chain driver"),
         "plain_mixed": dict(p32, chains_sampled=len(sample)),
@@ -529,6 +554,7 @@ def main():
     ap.add_argument("--c3-blocks", type=int, default=4)
     ap.add_argument("--c3-steps-per-block", type=int, default=4)
     ap.add_argument("--c3-plain-sample", type=int, default=32)
+    ap.add_argument("--c3-config", default="", help="threads,max_split,split_ratio instead of the autotuner")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)
