@@ -286,6 +286,32 @@ int pimc_batch_synchronize(pimc_batch *b);
 /* The batch's CUDA stream (cudaStream_t) for event timing and ordering. */
 void *pimc_batch_stream(pimc_batch *b);
 
+/* ---- observables (on the OLD copy) ---- */
+
+/* The terms of ActionsClass::Energy (ActionsClass.cc:812-871) for the whole
+ * path: kinetic = KineticClass::d_dBeta(0, M, 0), du_short =
+ * ShortRangeClass::d_dBeta(0, M, 0), du_long = LongRangeClass::d_dBeta
+ * (0 without pimc_set_longrange), v_short = sum over slices 0..M of
+ * ShortRangePotClass::V(slice) with weight 1/2 at slices 0 and M
+ * (ShortRangePotClass.cc:28-47), v_long = 0 (LongRangePotClass is not
+ * built), and total = (kinetic + du_short + du_long) / M, the per-slice
+ * sample EnergyClass::Accumulate adds (ObservableEnergy.cc:45-73). */
+typedef struct pimc_energy_terms {
+  double kinetic, du_short, du_long, v_short, v_long, total;
+} pimc_energy_terms;
+int pimc_energy(pimc_context *ctx, pimc_energy_terms *out);
+
+/* PairCorrelationClass (ObservableCorrelation.cc:36-224), one species: a
+ * linear grid {start, end, num_points} (end <= 0: the box side, the
+ * reference's default), num_points - 1 <= 12288 bins.  accumulate adds the
+ * OLD path's histogram of pair distances over slices 0..M-1 (enqueued, no
+ * sync); get returns the counts, g(r) normalised as WriteBlock does and the
+ * number of accumulated samples. */
+int pimc_gofr_setup(pimc_context *ctx, double start, double end, int num_points);
+int pimc_gofr_accumulate(pimc_context *ctx);
+int pimc_gofr_get(pimc_context *ctx, uint64_t *histogram, double *gofr, long long *total_counts);
+int pimc_gofr_reset(pimc_context *ctx);
+
 /* ---- allocation-free ShortRange SingleAction ----
  * No counterpart in the reference: it exists for callers that cannot call
  * cudaMalloc (an application whose memory pool owns every device

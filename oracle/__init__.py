@@ -88,6 +88,8 @@ def lib():
         "oracle_rng_seed": (None, [p, u64]),
         "oracle_run_bisection": (i, [p, i, C.POINTER(MoveRecord)]),
         "oracle_rng_position": (u64, [p]),
+        "oracle_energy": (None, [p, C.POINTER(d)]),
+        "oracle_gofr_accumulate": (None, [p, d, d, i, C.POINTER(u64)]),
         "oracle_run_windows": (i, [p, i, C.POINTER(MoveRecord)]),
     }
     for name, (res, args) in sig.items():
@@ -328,3 +330,16 @@ class System:
 
     def rng_position(self):
         return lib().oracle_rng_position(self.h)
+
+    def energy(self):
+        """ActionsClass::Energy terms of the OLD copy."""
+        out = np.zeros(6)
+        lib().oracle_energy(self.h, out.ctypes.data_as(C.POINTER(C.c_double)))
+        return dict(zip(("kinetic", "du_short", "du_long", "v_short", "v_long", "total"), out.tolist()))
+
+    def gofr_accumulate(self, start, end, num_points, hist=None):
+        """PairCorrelationClass::Accumulate of the OLD copy into hist (uint64)."""
+        if hist is None:
+            hist = np.zeros(num_points - 1, dtype=np.uint64)
+        lib().oracle_gofr_accumulate(self.h, start, end, num_points, hist.ctypes.data_as(C.POINTER(C.c_uint64)))
+        return hist

@@ -427,6 +427,18 @@ struct OraclePA {
     if (r <= pot.grid.End) return pot(r);
     return 0.0;
   }
+  // PairActionFitClass::V: DavidPAClass::V (DavidPAClass.cc:104-113) evaluates
+  // column 0 of the first tau table with r clamped to the grid; PAFitBase::V
+  // (PAFitBase.h:82) the potential; CoulombPot Z1Z2/r.
+  double V(double r) const {
+    if (kind == 1) {
+      if (r > ukj[0].grid->End) r = ukj[0].grid->End;
+      if (r < ukj[0].grid->Start) r = ukj[0].grid->Start;
+      return ukj[0](0, r);
+    }
+    if (kind == 2) return PotV(r);
+    return Z1Z2 / r;
+  }
   double U(double q, double z, double s2, int level) const {
     if (kind == 1) {  // DavidPAClass::U (DavidPAClass.cc:92-102)
       double s = sqrt(s2);
@@ -787,6 +799,23 @@ struct OracleSystem {
   double *P(int slice, int ptcl) { return P(mode, slice, ptcl); }
   int nk() const { return (int)(kVecs.size() / 3); }
 
+  // PathClass::DistDisp one-slice version (PathClass.h:637-660)
+  double Dist1(int slice, int ptcl1, int ptcl2) {
+    const double *a = P(slice, ptcl1), *b = P(slice, ptcl2);
+    double disp[3];
+    for (int i = 0; i < 3; i++) disp[i] = b[i] - a[i];
+    double n[3];
+    for (int i = 0; i < 3; i++) n[i] = nearbyint(disp[i] * BoxInv[i]);
+    for (int i = 0; i < 3; i++) disp[i] -= n[i] * IsPeriodic[i] * Box[i];
+    return sqrt(disp[0] * disp[0] + disp[1] * disp[1] + disp[2] * disp[2]);
+  }
+  // ShortRangePotClass::V(slice) (ShortRangePotClass.cc:28-47), no long range
+  double VSlice(int slice) {
+    double val = 0.0;
+    for (int ptcl1 = 0; ptcl1 < N; ptcl1++)
+      for (int ptcl2 = 0; ptcl2 < ptcl1; ptcl2++) val += pa->V(Dist1(slice, ptcl1, ptcl2));
+    return val;
+  }
   // PathClass::DistDisp two-slice version (PathClass.h:696-746)
   void DistDisp(int sliceA, int sliceB, int ptcl1, int ptcl2, double &distA, double &distB, dVec dispA,
                 dVec dispB) {
@@ -1362,5 +1391,50 @@ int oracle_run_bisection(OracleSystem *s, int n_blocks, OracleMoveRecord *record
   return 0;
 }
 uint64_t oracle_rng_position(OracleSystem *s) { return s->rng.nlocal; }
+
+// ActionsClass::Energy (ActionsClass.cc:812-871) on the OLD copy: out =
+// {kinetic, dUShort, dULong, vShort, vLong (0), total per slice}
+void oracle_energy(OracleSystem *s, double *out) {
+  const int M = s->NumSlices - 1;
+  const int mode = s->mode;
+  s->mode = 0;
+  const double kinetic = s->KineticDBeta(0, M, 0);
+  const double dUShort = s->ShortRangeDBeta(0, M, 0);
+  const double dULong = s->LRLevels > 0 ? s->LongRangeDBeta(0, M, 0) : 0.0;
+  double vShort = 0.0;
+  for (int slice = 0; slice <= M; slice++) {
+    double factor = ((slice == 0) || (slice == M)) ? 0.5 : 1.0;
+    vShort += factor * s->VSlice(slice);
+  }
+  s->mode = mode;
+  out[0] = kinetic;
+  out[1] = dUShort;
+  out[2] = dULong;
+  out[3] = vShort;
+  out[4] = 0.0;
+  out[5] = (kinetic + dUShort + dULong) / (double)M;  // ObservableEnergy.cc:45-73
+}
+
+// PairCorrelationClass::Accumulate (ObservableCorrelation.cc:191-207), one
+// species, on the OLD copy, into hist[num_points-1] on the LinearGrid
+// {start, end, num_points} (Grid.h:81-95).
+void oracle_gofr_accumulate(OracleSystem *s, double start, double end, int num_points, uint64_t *hist) {
+  const double delta = (end - start) / (double)(num_points - 1);
+  const double deltainv = 1.0 / delta;
+  const int mode = s->mode;
+  s->mode = 0;
+  for (int slice = 0; slice < s->NumSlices - 1; slice++)
+    for (int ptcl1 = 0; ptcl1 < s->N; ptcl1++)
+      for (int ptcl2 = ptcl1 + 1; ptcl2 < s->N; ptcl2++) {
+        const double dist = s->Dist1(slice, ptcl1, ptcl2);
+        if (dist < end) {
+          int index = (int)nearbyint((dist - start) * deltainv - 0.5);
+          // The reference indexes without a check; a grid starting above 0
+          // gives negative bins for closer pairs, which are skipped here.
+          if (index >= 0 && index < num_points - 1) hist[index]++;
+        }
+      }
+  s->mode = mode;
+}
 
 }  // extern "C"

@@ -125,6 +125,11 @@ int oracle_run_bisection(OracleSystem *s, int n_blocks, OracleMoveRecord *record
  * fit); returns windows = floor((slices-1)/2^L). */
 int oracle_run_windows(OracleSystem *s, int n_rounds, OracleMoveRecord *records);
 uint64_t oracle_rng_position(OracleSystem *s);
+/* ActionsClass::Energy terms on the OLD copy: {kinetic, dUShort, dULong,
+ * vShort, vLong (0), (kinetic+dUShort+dULong)/M}. */
+void oracle_energy(OracleSystem *s, double *out);
+/* PairCorrelationClass::Accumulate on the OLD copy into hist[num_points-1]. */
+void oracle_gofr_accumulate(OracleSystem *s, double start, double end, int num_points, uint64_t *hist);
 
 #ifdef __cplusplus
 }

@@ -98,6 +98,13 @@ class ChainDesc(C.Structure):
     ]
 
 
+class EnergyTerms(C.Structure):
+    _fields_ = [(n, C.c_double) for n in ("kinetic", "du_short", "du_long", "v_short", "v_long", "total")]
+
+    def as_dict(self):
+        return {n: getattr(self, n) for n, _ in self._fields_}
+
+
 class BisectionStats(C.Structure):
     _fields_ = [
         ("moves", C.c_int64),
@@ -143,6 +150,11 @@ _SIGS = {
     "pimc_calc_rhok": (_i, [_p]),
     "pimc_update_rhok": (_i, [_p, _i, _i, _ip, _i, _i]),
     "pimc_get_rhok": (_i, [_p, _i, _dp]),
+    "pimc_energy": (_i, [_p, C.POINTER(EnergyTerms)]),
+    "pimc_gofr_setup": (_i, [_p, _d, _d, _i]),
+    "pimc_gofr_accumulate": (_i, [_p]),
+    "pimc_gofr_get": (_i, [_p, C.POINTER(C.c_uint64), _dp, C.POINTER(C.c_longlong)]),
+    "pimc_gofr_reset": (_i, [_p]),
     "pimc_bisection_setup": (_i, [_p, C.POINTER(BisectionDesc)]),
     "pimc_rng_seed": (_i, [_p, C.c_uint64]),
     "pimc_bisection_windows": (_i, [_p, _ip]),
@@ -344,6 +356,32 @@ class PathData:
         out = np.empty((self.S, self.num_k, 2))
         self._check(_lib.pimc_get_rhok(self.h, copy, _dptr(out)), "get_rhok")
         return out[..., 0] + 1j * out[..., 1]
+
+    # ---- observables (EnergyClass, PairCorrelationClass) ----
+    def energy(self):
+        """ActionsClass::Energy terms of the OLD path; 'total' is the per-slice sample."""
+        e = EnergyTerms()
+        self._check(_lib.pimc_energy(self.h, C.byref(e)), "energy")
+        return e.as_dict()
+
+    def gofr_setup(self, start=0.0, end=0.0, num_points=101):
+        self._check(_lib.pimc_gofr_setup(self.h, start, end, num_points), "gofr_setup")
+        self._gofr_bins = num_points - 1
+
+    def gofr_accumulate(self):
+        self._check(_lib.pimc_gofr_accumulate(self.h), "gofr_accumulate")
+
+    def gofr_get(self):
+        """(histogram uint64, g(r) normalised like WriteBlock, number of samples)"""
+        h = np.zeros(self._gofr_bins, dtype=np.uint64)
+        g = np.zeros(self._gofr_bins)
+        n = C.c_longlong()
+        self._check(_lib.pimc_gofr_get(self.h, h.ctypes.data_as(C.POINTER(C.c_uint64)), _dptr(g), C.byref(n)),
+                    "gofr_get")
+        return h, g, n.value
+
+    def gofr_reset(self):
+        self._check(_lib.pimc_gofr_reset(self.h), "gofr_reset")
 
 
 class ActionBaseClass:

@@ -134,6 +134,87 @@ __global__ void __launch_bounds__(256) sr_dbeta_kernel(const double *__restrict_
   finish_sum(r, partials, counter, out, sh);
 }
 
+// ---- observables: ShortRangePotClass::V and PairCorrelationClass::Accumulate ----
+// PathClass::DistDisp one-slice form (PathClass.h:637-660): minimum image by
+// nearbyint(disp / L), then |disp|.
+__device__ __forceinline__ double dist_one_slice(const double a[3], const double b[3], const DevSystem &s) {
+  double d2 = 0.0;
+#pragma unroll
+  for (int i = 0; i < 3; i++) {
+    double d = b[i] - a[i];
+    const double n = rint(rmul(d, s.boxinv[i]));
+    d = rsub(d, rmul(n, s.box[i]));
+    d2 = radd(d2, rmul(d, d));
+  }
+  return sqrt(d2);
+}
+
+// V(r) of the pair action: DavidPAClass::V (DavidPAClass.cc:104-113), column 0
+// of the first tau table with r clamped to the grid; PAtricubicFit's
+// potential spline (PAFitBase.h:82).
+template <int KIND>
+__device__ __forceinline__ double pa_V(const DevPA &pa, double r) {
+  if (KIND == PA_DAVID) {
+    const DDavid<double> &d = pa.d64;
+    const DGrid<double> &g = d.grid;
+    if (r > g.end) r = g.end;
+    if (r < g.start) r = g.start;
+    return spline_col(g, d.uy, d.ud2, d.ncols, 0, r);
+  }
+  return pot_V(pa.t64, r);
+}
+
+// One pass over slices [0, S-1] x pairs p2 < p1 of the OLD path.
+//  DO_V: sum over slices of factor * sum_pairs V(r), factor 1/2 at the end
+//        slices (ActionsClass.cc:852-857 with ShortRangePotClass.cc:28-47).
+//  DO_G: histogram of the pair distances at slices [0, S-2] below the grid
+//        end, bin (int)nearbyint((r - start) * deltainv - 0.5)
+//        (ObservableCorrelation.cc:191-207, Grid.h:81-84); bins counted per
+//        block in shared memory, then added to the 64-bit histogram.
+template <int KIND, bool DO_V, bool DO_G>
+__global__ void __launch_bounds__(256) pair_obs_kernel(const double *__restrict__ path, DevSystem sys, DevPA pa,
+                                                       GofrGrid gg, unsigned long long *hist, double *partials,
+                                                       unsigned int *counter, double *out) {
+  extern __shared__ unsigned int s_hist[];
+  __shared__ double sh[32];
+  const int N = sys.N, S = sys.S;
+  const long long npairs = (long long)N * (N - 1) / 2;
+  const long long total = npairs * S;
+  if (DO_G) {
+    for (int i = threadIdx.x; i < gg.nbins; i += blockDim.x) s_hist[i] = 0u;
+    __syncthreads();
+  }
+  double acc = 0.0;
+  for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < total;
+       idx += (long long)gridDim.x * blockDim.x) {
+    const int slice = (int)(idx / npairs);
+    int p1, p2;
+    tri_decode(idx - (long long)slice * npairs, p1, p2);
+    if (!DO_V && slice == S - 1) continue;
+    double a[3], b[3];
+    load3(path + ((size_t)slice * N + p1) * 3, a);
+    load3(path + ((size_t)slice * N + p2) * 3, b);
+    const double dist = dist_one_slice(a, b, sys);
+    if (DO_V) {
+      const double f = (slice == 0 || slice == S - 1) ? 0.5 : 1.0;
+      acc += f * pa_V<KIND>(pa, dist);
+    }
+    if (DO_G && slice < S - 1 && dist < gg.end) {
+      const int bin = (int)rint(rsub(rmul(rsub(dist, gg.start), gg.deltainv), 0.5));
+      if (bin >= 0 && bin < gg.nbins) atomicAdd(&s_hist[bin], 1u);
+    }
+  }
+  if (DO_G) {
+    __syncthreads();
+    for (int i = threadIdx.x; i < gg.nbins; i += blockDim.x)
+      if (s_hist[i]) atomicAdd(&hist[i], (unsigned long long)s_hist[i]);
+  }
+  if (DO_V) {
+    const double r = block_sum(acc, sh);
+    finish_sum(r, partials, counter, out, sh);
+  }
+}
+
 __device__ __forceinline__ void velocity(const double *__restrict__ path, int N, int sa, int sb, int p,
                                          const DevSystem &sys, double v[3]) {
   double a[3], b[3];
@@ -289,6 +370,36 @@ cudaError_t launch_kin_dbeta(const ReduceTarget &t, const double *path, const De
   int blocks = grid_for((long long)sys.N * nlinks, 256, sm_count);
   kin_dbeta_kernel<<<blocks, 256, 0, t.stream>>>(path, sys, slice1, skip, nlinks, level, t.partials, t.counter,
                                                  t.out);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_pair_obs(const ReduceTarget &t, const double *path, const DevSystem &sys, const DevPA &pa,
+                            bool do_v, const GofrGrid *gg, unsigned long long *hist, int sm_count) {
+  const long long items = (long long)sys.N * (sys.N - 1) / 2 * sys.S;
+  const int blocks = grid_for(items, 256, sm_count);
+  const size_t dyn = gg ? (size_t)gg->nbins * sizeof(unsigned int) : 0;
+  const GofrGrid g0 = gg ? *gg : GofrGrid{0.0, 0.0, 0.0, 0};
+  const bool dav = pa.kind == PA_DAVID;
+  if (do_v && gg) {
+    if (dav)
+      pair_obs_kernel<PA_DAVID, true, true><<<blocks, 256, dyn, t.stream>>>(path, sys, pa, g0, hist, t.partials,
+                                                                            t.counter, t.out);
+    else
+      pair_obs_kernel<PA_TRICUBIC, true, true><<<blocks, 256, dyn, t.stream>>>(path, sys, pa, g0, hist, t.partials,
+                                                                               t.counter, t.out);
+  } else if (do_v) {
+    if (dav)
+      pair_obs_kernel<PA_DAVID, true, false><<<blocks, 256, 0, t.stream>>>(path, sys, pa, g0, hist, t.partials,
+                                                                           t.counter, t.out);
+    else
+      pair_obs_kernel<PA_TRICUBIC, true, false><<<blocks, 256, 0, t.stream>>>(path, sys, pa, g0, hist, t.partials,
+                                                                              t.counter, t.out);
+  } else if (gg) {
+    pair_obs_kernel<PA_DAVID, false, true><<<blocks, 256, dyn, t.stream>>>(path, sys, pa, g0, hist, t.partials,
+                                                                          t.counter, t.out);
+  } else {
+    return cudaErrorInvalidValue;
+  }
   return cudaGetLastError();
 }
 

@@ -256,6 +256,7 @@ int pimc_destroy(pimc_context *ctx) {
   cudaFree(ctx->d_rhok[1]);
   cudaFree(ctx->d_ulong_k);
   cudaFree(ctx->d_dulong_k);
+  cudaFree(ctx->d_gofr);
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
   delete ctx;
   return PIMC_OK;
@@ -866,6 +867,96 @@ int pimc_get_rhok(pimc_context *ctx, int copy, double *out) {
   if (ctx->num_k <= 0) return fail(ctx, PIMC_E_STATE, "pimc_setup_kvecs not called");
   CK(cudaSetDevice(ctx->device));
   CK(cudaMemcpy(out, ctx->d_rhok[copy], (size_t)ctx->sys.S * ctx->num_k * sizeof(double2), cudaMemcpyDeviceToHost));
+  return PIMC_OK;
+}
+
+// ---- observables ----
+
+int pimc_energy(pimc_context *ctx, pimc_energy_terms *out) {
+  if (!ctx || !out) return PIMC_E_ARG;
+  if (ctx->pa.kind == PA_NONE) return fail(ctx, PIMC_E_STATE, "no pair action set");
+  CK(cudaSetDevice(ctx->device));
+  const int M = ctx->sys.S - 1;
+  pimc_energy_terms e = {};
+  // ActionsClass::Energy (ActionsClass.cc:812-871) on the OLD path
+  int rc = pimc_d_dbeta(ctx, PIMC_ACTION_KINETIC, 0, M, 0, &e.kinetic);
+  if (!rc) rc = pimc_d_dbeta(ctx, PIMC_ACTION_SHORTRANGE, 0, M, 0, &e.du_short);
+  if (!rc && ctx->lr_ready) rc = pimc_d_dbeta(ctx, PIMC_ACTION_LONGRANGE, 0, M, 0, &e.du_long);
+  if (rc) return rc;
+  ReduceTarget t{ctx->stream, ctx->d_partials, ctx->d_counter, ctx->d_out};
+  CK(launch_pair_obs(t, ctx->d_path[PIMC_OLD], ctx->sys, ctx->pa, true, nullptr, nullptr, ctx->sm_count));
+  rc = finish_scalar(ctx, &e.v_short);
+  if (rc) return rc;
+  e.v_long = 0.0;
+  // EnergyClass::Accumulate's sample (ObservableEnergy.cc:45-73): per slice
+  e.total = (e.kinetic + e.du_short + e.du_long) / (double)M;
+  *out = e;
+  return PIMC_OK;
+}
+
+int pimc_gofr_setup(pimc_context *ctx, double start, double end, int num_points) {
+  if (!ctx) return PIMC_E_ARG;
+  if (end <= 0.0) end = ctx->sys.box[0];  // the reference's default grid end (ObservableCorrelation.cc:52-57)
+  if (num_points < 2 || num_points - 1 > 12288 || !(start >= 0.0) || !(end > start))
+    return fail(ctx, PIMC_E_ARG, "g(r) grid: 0 <= start < end and 2 <= NumPoints <= 12289");
+  CK(cudaSetDevice(ctx->device));
+  cudaFree(ctx->d_gofr);
+  ctx->d_gofr = nullptr;
+  CK(cudaMalloc(&ctx->d_gofr, (size_t)(num_points - 1) * sizeof(unsigned long long)));
+  CK(cudaMemsetAsync(ctx->d_gofr, 0, (size_t)(num_points - 1) * sizeof(unsigned long long), ctx->stream));
+  ctx->gofr_points = num_points;
+  ctx->gofr_start = start;
+  ctx->gofr_end = end;
+  // LinearGrid::Init (Grid.h:87-95)
+  ctx->gofr_delta = (end - start) / (double)(num_points - 1);
+  ctx->gofr_deltainv = 1.0 / ctx->gofr_delta;
+  ctx->gofr_counts = 0;
+  return PIMC_OK;
+}
+
+int pimc_gofr_accumulate(pimc_context *ctx) {
+  if (!ctx) return PIMC_E_ARG;
+  if (!ctx->d_gofr) return fail(ctx, PIMC_E_STATE, "pimc_gofr_setup not called");
+  CK(cudaSetDevice(ctx->device));
+  GofrGrid g{ctx->gofr_start, ctx->gofr_end, ctx->gofr_deltainv, ctx->gofr_points - 1};
+  ReduceTarget t{ctx->stream, ctx->d_partials, ctx->d_counter, ctx->d_out};
+  CK(launch_pair_obs(t, ctx->d_path[PIMC_OLD], ctx->sys, ctx->pa, false, &g, ctx->d_gofr, ctx->sm_count));
+  ctx->gofr_counts++;
+  return PIMC_OK;
+}
+
+int pimc_gofr_get(pimc_context *ctx, uint64_t *histogram, double *gofr, long long *total_counts) {
+  if (!ctx) return PIMC_E_ARG;
+  if (!ctx->d_gofr) return fail(ctx, PIMC_E_STATE, "pimc_gofr_setup not called");
+  CK(cudaSetDevice(ctx->device));
+  const int nb = ctx->gofr_points - 1;
+  std::vector<unsigned long long> h(nb);
+  CK(cudaMemcpyAsync(h.data(), ctx->d_gofr, nb * sizeof(unsigned long long), cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  if (histogram)
+    for (int i = 0; i < nb; i++) histogram[i] = h[i];
+  if (total_counts) *total_counts = ctx->gofr_counts;
+  if (gofr) {
+    // PairCorrelationClass::WriteBlock (ObservableCorrelation.cc:101-135), one species
+    const double N = ctx->sys.N, M = ctx->sys.S - 1;
+    const double vol = ctx->sys.box[0] * ctx->sys.box[1] * ctx->sys.box[2];
+    const double norm = 0.5 * (double)ctx->gofr_counts * M * (N * (N - 1.0)) / vol;
+    for (int i = 0; i < nb; i++) {
+      const double r1 = ctx->gofr_start + (double)i * ctx->gofr_delta;
+      const double r2 = ctx->gofr_start + (double)(i + 1) * ctx->gofr_delta;
+      const double binVol = 4.0 * M_PI / 3 * (r2 * r2 * r2 - r1 * r1 * r1);
+      gofr[i] = norm > 0.0 ? (double)h[i] / (binVol * norm) : 0.0;
+    }
+  }
+  return PIMC_OK;
+}
+
+int pimc_gofr_reset(pimc_context *ctx) {
+  if (!ctx) return PIMC_E_ARG;
+  if (!ctx->d_gofr) return fail(ctx, PIMC_E_STATE, "pimc_gofr_setup not called");
+  CK(cudaSetDevice(ctx->device));
+  CK(cudaMemsetAsync(ctx->d_gofr, 0, (size_t)(ctx->gofr_points - 1) * sizeof(unsigned long long), ctx->stream));
+  ctx->gofr_counts = 0;
   return PIMC_OK;
 }
 

@@ -159,5 +159,10 @@ struct pimc_context {
   int lr_levels = 0, use_background = 0;
   double *d_ulong_k = nullptr, *d_dulong_k = nullptr;  // [levels][k]
   std::vector<double> ulong_r0, ushort_k0, ulong_k0, dulong_r0, dushort_k0, dulong_k0;
+  // pair correlation accumulator (PairCorrelationClass)
+  unsigned long long *d_gofr = nullptr;
+  int gofr_points = 0;
+  double gofr_start = 0, gofr_end = 0, gofr_delta = 0, gofr_deltainv = 0;
+  long long gofr_counts = 0;
   std::string last_error;
 };

@@ -157,3 +157,29 @@ def test_bisection_oracle_deterministic(tmp_path):
     assert np.array_equal(outs[0][0], outs[1][0]) and outs[0][1] == outs[1][1]
     acc = np.mean([a for _, _, a in outs[0][1]])
     assert 0.02 < acc < 0.98
+
+
+def test_gofr_oracle_matches_numpy_histogram():
+    """PairCorrelationClass::Accumulate restated: slices 0..M-1, pairs p1 < p2,
+    minimum image by nearbyint, LinearGrid::ReverseMap binning; an
+    independent numpy computation gives the same integer counts."""
+    n, slices = 24, 9
+    box = np.array([9.0, 9.0, 9.0])
+    path = random_walk_path(n, slices, box, 0.7, 11, far=1.0)
+    o = O.System(n, slices, box, 0.01, W.HE4_LAMBDA, 0)
+    o.set_path(path)
+    pts, start, end = 61, 0.0, 9.0
+    got = o.gofr_accumulate(start, end, pts)
+    ref = np.zeros(pts - 1, dtype=np.uint64)
+    deltainv = 1.0 / ((end - start) / (pts - 1))
+    for s in range(slices - 1):
+        x = path[s]
+        i, j = np.triu_indices(n, 1)
+        d = x[j] - x[i]
+        d = d - np.rint(d * (1.0 / box)) * box
+        r = np.sqrt(d[:, 0] * d[:, 0] + d[:, 1] * d[:, 1] + d[:, 2] * d[:, 2])
+        r = r[r < end]
+        idx = np.rint((r - start) * deltainv - 0.5).astype(int)
+        np.add.at(ref, idx, 1)
+    assert np.array_equal(got, ref)
+    assert got.sum() == (slices - 1) * n * (n - 1) // 2  # the grid covers every distance up to L
