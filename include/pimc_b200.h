@@ -286,6 +286,36 @@ int pimc_batch_synchronize(pimc_batch *b);
 /* The batch's CUDA stream (cudaStream_t) for event timing and ordering. */
 void *pimc_batch_stream(pimc_batch *b);
 
+/* ---- classical Coulomb pair action and the optimized Ewald breakup ---- */
+
+/* PAclassicalFitClass with a CoulombPot (Common/PairAction/PAclassicalFit.cc:
+ * 57-75, 175-288): U = beta_l Z1Z2 / q, dU = Z1Z2 / q, beta_l = tau 2^l for
+ * l < num_levels.  Without pimc_longrange_coulomb nothing is subtracted. */
+int pimc_pa_coulomb(pimc_context *ctx, int sp1, int sp2, double z1z2, int num_levels);
+
+/* LongRangeClass::Init's OptimizedBreakup_U and _dU (PIMC++/src/Actions/
+ * LongRangeClass.cc:482-868) for the Coulomb pair action: LPQHI basis on
+ * num_knots knots to r_c = L/2, the k-space fit beyond the pimc_setup_kvecs
+ * cutoff, Ulong(r) / dUlong(r) natural quintic splines on the 1000-point
+ * LongGrid, and the k = 0 integrals (host, FP64).  Loads the long-range
+ * tables (as pimc_set_longrange) and turns on the 1/2 (Ulong(r) + Ulong(r'))
+ * subtraction in ShortRange (ShortRangeClass.cc:211-214, 282-286). */
+int pimc_longrange_coulomb(pimc_context *ctx, int num_knots, int use_background);
+
+/* The same breakup without a context (host only): tables for num_k
+ * k-vectors [num_k][3]; ulong_k/dulong_k [levels][num_k]; the per-level
+ * scalars [levels]; ulong_r/dulong_r [levels][1000][6] Taylor coefficients of
+ * the quintic splines on the grid [0, *rmax]. Any output may be NULL. */
+int pimc_coulomb_breakup(const double box[3], double z1z2, double smallest_beta, int num_levels, int num_knots,
+                         double kcutoff, int num_k, const double *kvecs, double *ulong_k, double *dulong_k,
+                         double *ulong_r0, double *dulong_r0, double *ushort_k0, double *dushort_k0,
+                         double *ulong_k0, double *dulong_k0, double *rmax, double *ulong_r, double *dulong_r);
+/* Natural quintic interpolating spline (third and fourth derivatives zero at
+ * both ends; QuinticSpline without end derivatives) of y[n] on a uniform
+ * grid of spacing h: coef[n][6] Taylor coefficients of each interval at its
+ * left knot, host only. */
+int pimc_quintic_spline(int n, double h, const double *y, double *coef);
+
 /* ---- observables (on the OLD copy) ---- */
 
 /* The terms of ActionsClass::Energy (ActionsClass.cc:812-871) for the whole

@@ -150,6 +150,10 @@ _SIGS = {
     "pimc_calc_rhok": (_i, [_p]),
     "pimc_update_rhok": (_i, [_p, _i, _i, _ip, _i, _i]),
     "pimc_get_rhok": (_i, [_p, _i, _dp]),
+    "pimc_pa_coulomb": (_i, [_p, _i, _i, _d, _i]),
+    "pimc_longrange_coulomb": (_i, [_p, _i, _i]),
+    "pimc_coulomb_breakup": (_i, [_dp, _d, _d, _i, _i, _d, _i, _dp] + [_dp] * 11),
+    "pimc_quintic_spline": (_i, [_i, _d, _dp, _dp]),
     "pimc_energy": (_i, [_p, C.POINTER(EnergyTerms)]),
     "pimc_gofr_setup": (_i, [_p, _d, _d, _i]),
     "pimc_gofr_accumulate": (_i, [_p]),
@@ -356,6 +360,14 @@ class PathData:
         out = np.empty((self.S, self.num_k, 2))
         self._check(_lib.pimc_get_rhok(self.h, copy, _dptr(out)), "get_rhok")
         return out[..., 0] + 1j * out[..., 1]
+
+    def pa_coulomb(self, z1z2, num_levels):
+        """PAclassicalFitClass with a Coulomb potential Z1Z2/r."""
+        self._check(_lib.pimc_pa_coulomb(self.h, 0, 0, z1z2, num_levels), "pa_coulomb")
+
+    def longrange_coulomb(self, num_knots, use_background=True):
+        """Optimized breakup of the Coulomb action (after setup_kvecs)."""
+        self._check(_lib.pimc_longrange_coulomb(self.h, num_knots, int(use_background)), "longrange_coulomb")
 
     # ---- observables (EnergyClass, PairCorrelationClass) ----
     def energy(self):
@@ -577,3 +589,35 @@ class BatchChains:
 
     def __del__(self):
         self.close()
+
+
+def coulomb_breakup(box, z1z2, smallest_beta, num_levels, num_knots, kcutoff, kvecs):
+    """Host-only optimized breakup of a Coulomb pair action; returns a dict of tables."""
+    kv = np.ascontiguousarray(kvecs, dtype=np.float64).reshape(-1, 3)
+    nk = kv.shape[0]
+    box = np.ascontiguousarray(box, dtype=np.float64)
+    out = dict(ulong_k=np.zeros((num_levels, nk)), dulong_k=np.zeros((num_levels, nk)))
+    for k in ("ulong_r0", "dulong_r0", "ushort_k0", "dushort_k0", "ulong_k0", "dulong_k0"):
+        out[k] = np.zeros(num_levels)
+    rmax = np.zeros(1)
+    out["ulong_r"] = np.zeros((num_levels, 1000, 6))
+    out["dulong_r"] = np.zeros((num_levels, 1000, 6))
+    rc = _lib.pimc_coulomb_breakup(_dptr(box), z1z2, smallest_beta, num_levels, num_knots, kcutoff, nk, _dptr(kv),
+                                   _dptr(out["ulong_k"]), _dptr(out["dulong_k"]), _dptr(out["ulong_r0"]),
+                                   _dptr(out["dulong_r0"]), _dptr(out["ushort_k0"]), _dptr(out["dushort_k0"]),
+                                   _dptr(out["ulong_k0"]), _dptr(out["dulong_k0"]), _dptr(rmax),
+                                   _dptr(out["ulong_r"]), _dptr(out["dulong_r"]))
+    if rc:
+        raise PimcError(rc, "pimc_coulomb_breakup")
+    out["rmax"] = float(rmax[0])
+    return out
+
+
+def quintic_spline(h, y):
+    """Natural quintic spline coefficients [n][6] of y on a uniform grid."""
+    y = np.ascontiguousarray(y, dtype=np.float64)
+    coef = np.zeros((len(y), 6))
+    rc = _lib.pimc_quintic_spline(len(y), h, _dptr(y), _dptr(coef))
+    if rc:
+        raise PimcError(rc, "pimc_quintic_spline")
+    return coef

@@ -161,6 +161,15 @@ __device__ __forceinline__ double pa_V(const DevPA &pa, double r) {
     if (r < g.start) r = g.start;
     return spline_col(g, d.uy, d.ud2, d.ncols, 0, r);
   }
+  if (KIND == PA_COULOMB) {
+    // CoulombPot V = Z1Z2 / r, less Vlong with the long-range breakup
+    // (ShortRangePotClass.cc:41-43); for the classical Coulomb action the V
+    // breakup fits the same X_k as the dU one, so Vlong is dUlong.
+    const DCoulomb<double> &c = pa.c64;
+    double v = c.z1z2 / r;
+    if (c.long_range) v -= quintic_at(c, c.dulong, r);
+    return v;
+  }
   return pot_V(pa.t64, r);
 }
 
@@ -333,6 +342,13 @@ cudaError_t launch_sr_single(const ReduceTarget &t, const double *path, const De
     else
       sr_single_kernel<PA_DAVID, double><<<blocks, 256, 0, t.stream>>>(path, sys, pa, act, slice1, skip, nlinks, level,
                                                                         t.partials, t.counter, t.out);
+  } else if (pa.kind == PA_COULOMB) {
+    if (precision == PIMC_MIXED)
+      sr_single_kernel<PA_COULOMB, float><<<blocks, 256, 0, t.stream>>>(path, sys, pa, act, slice1, skip, nlinks,
+                                                                         level, t.partials, t.counter, t.out);
+    else
+      sr_single_kernel<PA_COULOMB, double><<<blocks, 256, 0, t.stream>>>(path, sys, pa, act, slice1, skip, nlinks,
+                                                                          level, t.partials, t.counter, t.out);
   } else {
     if (precision == PIMC_MIXED)
       sr_single_kernel<PA_TRICUBIC, float><<<blocks, 256, 0, t.stream>>>(path, sys, pa, act, slice1, skip, nlinks,
@@ -351,6 +367,9 @@ cudaError_t launch_sr_dbeta(const ReduceTarget &t, const double *path, const Dev
   if (pa.kind == PA_DAVID)
     sr_dbeta_kernel<PA_DAVID><<<blocks, 256, 0, t.stream>>>(path, sys, pa, slice1, skip, nlinks, level, t.partials,
                                                             t.counter, t.out);
+  else if (pa.kind == PA_COULOMB)
+    sr_dbeta_kernel<PA_COULOMB><<<blocks, 256, 0, t.stream>>>(path, sys, pa, slice1, skip, nlinks, level, t.partials,
+                                                              t.counter, t.out);
   else
     sr_dbeta_kernel<PA_TRICUBIC><<<blocks, 256, 0, t.stream>>>(path, sys, pa, slice1, skip, nlinks, level, t.partials,
                                                                t.counter, t.out);
@@ -380,7 +399,14 @@ cudaError_t launch_pair_obs(const ReduceTarget &t, const double *path, const Dev
   const size_t dyn = gg ? (size_t)gg->nbins * sizeof(unsigned int) : 0;
   const GofrGrid g0 = gg ? *gg : GofrGrid{0.0, 0.0, 0.0, 0};
   const bool dav = pa.kind == PA_DAVID;
-  if (do_v && gg) {
+  if (do_v && pa.kind == PA_COULOMB) {
+    if (gg)
+      pair_obs_kernel<PA_COULOMB, true, true><<<blocks, 256, dyn, t.stream>>>(path, sys, pa, g0, hist, t.partials,
+                                                                              t.counter, t.out);
+    else
+      pair_obs_kernel<PA_COULOMB, true, false><<<blocks, 256, 0, t.stream>>>(path, sys, pa, g0, hist, t.partials,
+                                                                             t.counter, t.out);
+  } else if (do_v && gg) {
     if (dav)
       pair_obs_kernel<PA_DAVID, true, true><<<blocks, 256, dyn, t.stream>>>(path, sys, pa, g0, hist, t.partials,
                                                                             t.counter, t.out);

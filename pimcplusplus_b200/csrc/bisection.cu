@@ -920,6 +920,12 @@ cudaError_t bisection_occupancy(const BisectionArgs &a, int precision, int shado
     return shadow ? occupancy_t<PA_DAVID, double, true>(cl, threads, dyn, max_clusters)
                   : occupancy_t<PA_DAVID, double, false>(cl, threads, dyn, max_clusters);
   }
+  if (a.pa.kind == PA_COULOMB) {
+    if (mixed) return shadow ? occupancy_t<PA_COULOMB, float, true>(cl, threads, dyn, max_clusters)
+                             : occupancy_t<PA_COULOMB, float, false>(cl, threads, dyn, max_clusters);
+    return shadow ? occupancy_t<PA_COULOMB, double, true>(cl, threads, dyn, max_clusters)
+                  : occupancy_t<PA_COULOMB, double, false>(cl, threads, dyn, max_clusters);
+  }
   if (mixed) return shadow ? occupancy_t<PA_TRICUBIC, float, true>(cl, threads, dyn, max_clusters)
                            : occupancy_t<PA_TRICUBIC, float, false>(cl, threads, dyn, max_clusters);
   return shadow ? occupancy_t<PA_TRICUBIC, double, true>(cl, threads, dyn, max_clusters)
@@ -989,6 +995,12 @@ cudaError_t launch_bisection(const BisectionArgs &a, int precision, int shadow, 
                              : launch_t<PA_DAVID, float, false>(a, cl, clusters, threads, dyn, st);
     return shadow ? launch_t<PA_DAVID, double, true>(a, cl, clusters, threads, dyn, st)
                   : launch_t<PA_DAVID, double, false>(a, cl, clusters, threads, dyn, st);
+  }
+  if (a.pa.kind == PA_COULOMB) {
+    if (mixed) return shadow ? launch_t<PA_COULOMB, float, true>(a, cl, clusters, threads, dyn, st)
+                             : launch_t<PA_COULOMB, float, false>(a, cl, clusters, threads, dyn, st);
+    return shadow ? launch_t<PA_COULOMB, double, true>(a, cl, clusters, threads, dyn, st)
+                  : launch_t<PA_COULOMB, double, false>(a, cl, clusters, threads, dyn, st);
   }
   if (mixed) return shadow ? launch_t<PA_TRICUBIC, float, true>(a, cl, clusters, threads, dyn, st)
                            : launch_t<PA_TRICUBIC, float, false>(a, cl, clusters, threads, dyn, st);

@@ -146,7 +146,21 @@ LRDesc lr_desc(const pimc_context *ctx) {
 }
 
 // PairActionFitClass::IsLongRange of the context's pair action.
-bool pa_long_range(const pimc_context *ctx) { return ctx->pa.kind == PA_TRICUBIC; }
+// PairActionFitClass::IsLongRange: PAtricubicFit (PAtricubicFit.cc:869-872) and
+// a classical Coulomb action with Z1Z2 != 0 (PAclassicalFit.cc:112-117).
+bool pa_long_range(const pimc_context *ctx) {
+  return ctx->pa.kind == PA_TRICUBIC || (ctx->pa.kind == PA_COULOMB && ctx->pa.c64.z1z2 != 0.0);
+}
+
+int pa_levels_ok(pimc_context *ctx, int levels_needed) {
+  if (ctx->pa.kind == PA_DAVID && levels_needed + ctx->pa.d64.tau_pos > ctx->pa.d64.num_tau)
+    return fail(ctx, PIMC_E_ARG, "level beyond the pair action's tau levels");
+  if (ctx->pa.kind == PA_TRICUBIC && levels_needed > ctx->pa.t64.num_betas)
+    return fail(ctx, PIMC_E_ARG, "level beyond the pair action's beta levels");
+  if (ctx->pa.kind == PA_COULOMB && levels_needed > ctx->pa.c64.num_levels)
+    return fail(ctx, PIMC_E_ARG, "level beyond the pair action's beta levels");
+  return PIMC_OK;
+}
 
 // The constant (Madelung, k=0 / background) part of LongRangeClass's sum over
 // slices [slice1, slice2] step 2^level (LongRangeClass.cc:320-366).
@@ -458,10 +472,7 @@ int pimc_single_action(pimc_context *ctx, int action, int copy, int slice1, int 
   switch (action) {
     case PIMC_ACTION_SHORTRANGE:
       if (ctx->pa.kind == PA_NONE) return fail(ctx, PIMC_E_STATE, "no pair action set");
-      if (ctx->pa.kind == PA_DAVID && level + ctx->pa.d64.tau_pos >= ctx->pa.d64.num_tau)
-        return fail(ctx, PIMC_E_ARG, "level beyond the pair action's tau levels");
-      if (ctx->pa.kind == PA_TRICUBIC && level >= ctx->pa.t64.num_betas)
-        return fail(ctx, PIMC_E_ARG, "level beyond the pair action's beta levels");
+      if (int rc2 = pa_levels_ok(ctx, level + 1)) return rc2;
       CK(launch_sr_single(t, path, ctx->sys, ctx->pa, act, slice1, skip, nlinks, level, precision, ctx->sm_count));
       break;
     case PIMC_ACTION_KINETIC:
@@ -536,8 +547,7 @@ int pimc_d_dbeta(pimc_context *ctx, int action, int slice1, int slice2, int leve
   switch (action) {
     case PIMC_ACTION_SHORTRANGE:
       if (ctx->pa.kind == PA_NONE) return fail(ctx, PIMC_E_STATE, "no pair action set");
-      if (ctx->pa.kind == PA_DAVID && level + ctx->pa.d64.tau_pos >= ctx->pa.d64.num_tau)
-        return fail(ctx, PIMC_E_ARG, "level beyond the pair action's tau levels");
+      if (int rc2 = pa_levels_ok(ctx, level + 1)) return rc2;
       CK(launch_sr_dbeta(t, path, ctx->sys, ctx->pa, slice1, skip, nlinks, level, ctx->sm_count));
       break;
     case PIMC_ACTION_KINETIC:
@@ -599,10 +609,7 @@ int pimc_bisection_setup(pimc_context *ctx, const pimc_bisection_desc *d) {
   if (d->schedule == PIMC_SCHEDULE_WINDOWS && window_slots(ctx, d->num_levels) < 1)
     return fail(ctx, PIMC_E_ARG, "no window fits");
   if (d->use_longrange) return fail(ctx, PIMC_E_ARG, "long range inside device moves is not available");
-  if (ctx->pa.kind == PA_DAVID && d->num_levels + ctx->pa.d64.tau_pos > ctx->pa.d64.num_tau)
-    return fail(ctx, PIMC_E_ARG, "pair action has fewer tau levels than NumLevels");
-  if (ctx->pa.kind == PA_TRICUBIC && d->num_levels > ctx->pa.t64.num_betas)
-    return fail(ctx, PIMC_E_ARG, "pair action has fewer beta levels than NumLevels");
+  if (int rc2 = pa_levels_ok(ctx, d->num_levels)) return rc2;
   CK(cudaSetDevice(ctx->device));
   ctx->bis = *d;
   if (ctx->bis.cluster_ctas == 0) ctx->bis.cluster_ctas = ctx->sys.N >= 256 ? 8 : 1;
@@ -958,6 +965,90 @@ int pimc_gofr_reset(pimc_context *ctx) {
   CK(cudaMemsetAsync(ctx->d_gofr, 0, (size_t)(ctx->gofr_points - 1) * sizeof(unsigned long long), ctx->stream));
   ctx->gofr_counts = 0;
   return PIMC_OK;
+}
+
+// ---- classical Coulomb pair action and its optimized breakup ----
+
+int pimc_pa_coulomb(pimc_context *ctx, int sp1, int sp2, double z1z2, int num_levels) {
+  if (!ctx) return PIMC_E_ARG;
+  if (sp1 != 0 || sp2 != 0) return fail(ctx, PIMC_E_ARG, "one species pair (0, 0) is supported");
+  if (num_levels < 1 || num_levels > 16) return fail(ctx, PIMC_E_ARG, "num_levels must be in 1..16");
+  DCoulomb<double> c64{};
+  DCoulomb<float> c32{};
+  c64.z1z2 = z1z2;
+  c64.smallest_beta = ctx->sys.tau;
+  c64.num_levels = num_levels;
+  c64.long_range = 0;
+  c64.np = kLongGridPoints;
+  c32.z1z2 = (float)z1z2;
+  c32.smallest_beta = (float)ctx->sys.tau;
+  c32.num_levels = num_levels;
+  c32.long_range = 0;
+  c32.np = kLongGridPoints;
+  ctx->pa = DevPA{};
+  ctx->pa.kind = PA_COULOMB;
+  ctx->pa.c64 = c64;
+  ctx->pa.c32 = c32;
+  return PIMC_OK;
+}
+
+int pimc_longrange_coulomb(pimc_context *ctx, int num_knots, int use_background) {
+  if (!ctx) return PIMC_E_ARG;
+  if (ctx->pa.kind != PA_COULOMB) return fail(ctx, PIMC_E_STATE, "pimc_pa_coulomb not called");
+  if (ctx->num_k <= 0) return fail(ctx, PIMC_E_STATE, "pimc_setup_kvecs not called");
+  if (num_knots < 2 || num_knots > 1000) return fail(ctx, PIMC_E_ARG, "num_knots must be in 2..1000");
+  CK(cudaSetDevice(ctx->device));
+  DCoulomb<double> &c64 = ctx->pa.c64;
+  DCoulomb<float> &c32 = ctx->pa.c32;
+  BreakupTables bt;
+  int rc = coulomb_breakup(ctx->sys.box, c64.z1z2, c64.smallest_beta, c64.num_levels, num_knots, ctx->kcutoff,
+                           ctx->num_k, ctx->kvecs.data(), bt);
+  if (rc) return fail(ctx, rc, "breakup failed");
+  const double h = bt.rmax / (kLongGridPoints - 1);
+  c64.h = h;
+  c64.hinv = 1.0 / h;
+  c32.h = (float)h;
+  c32.hinv = (float)(1.0 / h);
+  if ((rc = upload(ctx, bt.ulong_r.data(), bt.ulong_r.size(), &c64.ulong))) return rc;
+  if ((rc = upload(ctx, bt.dulong_r.data(), bt.dulong_r.size(), &c64.dulong))) return rc;
+  std::vector<float> u32(bt.ulong_r.begin(), bt.ulong_r.end()), du32(bt.dulong_r.begin(), bt.dulong_r.end());
+  if ((rc = upload(ctx, u32.data(), u32.size(), &c32.ulong))) return rc;
+  if ((rc = upload(ctx, du32.data(), du32.size(), &c32.dulong))) return rc;
+  c64.long_range = 1;
+  c32.long_range = 1;
+  return pimc_set_longrange(ctx, c64.num_levels, bt.ulong_k.data(), bt.ulong_r0.data(), bt.ushort_k0.data(),
+                            bt.ulong_k0.data(), bt.dulong_k.data(), bt.dulong_r0.data(), bt.dushort_k0.data(),
+                            bt.dulong_k0.data(), use_background);
+}
+
+int pimc_coulomb_breakup(const double box[3], double z1z2, double smallest_beta, int num_levels, int num_knots,
+                         double kcutoff, int num_k, const double *kvecs, double *ulong_k, double *dulong_k,
+                         double *ulong_r0, double *dulong_r0, double *ushort_k0, double *dushort_k0,
+                         double *ulong_k0, double *dulong_k0, double *rmax, double *ulong_r, double *dulong_r) {
+  if (!box || num_levels < 1 || num_knots < 2 || num_k < 0 || (num_k > 0 && !kvecs)) return PIMC_E_ARG;
+  BreakupTables bt;
+  const int rc = coulomb_breakup(box, z1z2, smallest_beta, num_levels, num_knots, kcutoff, num_k, kvecs, bt);
+  if (rc) return rc;
+  auto put = [](double *dst, const std::vector<double> &src) {
+    if (dst) std::copy(src.begin(), src.end(), dst);
+  };
+  put(ulong_k, bt.ulong_k);
+  put(dulong_k, bt.dulong_k);
+  put(ulong_r0, bt.ulong_r0);
+  put(dulong_r0, bt.dulong_r0);
+  put(ushort_k0, bt.ushort_k0);
+  put(dushort_k0, bt.dushort_k0);
+  put(ulong_k0, bt.ulong_k0);
+  put(dulong_k0, bt.dulong_k0);
+  put(ulong_r, bt.ulong_r);
+  put(dulong_r, bt.dulong_r);
+  if (rmax) *rmax = bt.rmax;
+  return PIMC_OK;
+}
+
+int pimc_quintic_spline(int n, double h, const double *y, double *coef) {
+  if (n < 3 || !(h > 0.0) || !y || !coef) return PIMC_E_ARG;
+  return quintic_natural(n, h, y, coef) ? PIMC_OK : PIMC_E_ARG;
 }
 
 }  // extern "C"

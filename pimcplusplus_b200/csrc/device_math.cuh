@@ -415,9 +415,53 @@ template <>
 __device__ __forceinline__ const DTricubic<float> &tricubic_of<float>(const DevPA &pa) { return pa.t32; }
 
 // U(q, z, s^2, level) of the pair action (ActionBaseClass's PA.U).
+// QuinticSpline::operator() (QuinticSpline.h:204-221) on the LongGrid:
+// interval ReverseMap(x) clamped to [0, np-2], Horner in P = x - x_I.
+template <typename R>
+__device__ __forceinline__ R quintic_at(const DCoulomb<R> &c, const R *tab, R x) {
+  const R rm = round_even_magic(rsub(rmul(x, c.hinv), R(0.5)));
+  const R lowf = fmin_r(fmax_r(rm, R(0)), (R)(c.np - 2));
+  const int i = int_of_integral(lowf);
+  const R *t = tab + (size_t)i * 6;
+  const R P = x - rmul(lowf, c.h);
+  return ((((t[5] * P + t[4]) * P + t[3]) * P + t[2]) * P + t[1]) * P + t[0];
+}
+// PAclassicalFitClass::U with the long-range part taken out as
+// ShortRangeClass::SingleAction does (ShortRangeClass.cc:211-214).
+template <typename R>
+__device__ __forceinline__ R coulomb_U(const DCoulomb<R> &c, const LinkGeom<R> &g, int level) {
+  R beta = c.smallest_beta;
+  for (int i = 0; i < level; i++) beta *= R(2);
+  R U = beta * (c.z1z2 / g.q);
+  if (c.long_range) {
+    const R *tab = c.ulong + (size_t)level * c.np * 6;
+    U -= R(0.5) * (quintic_at(c, tab, g.rmag) + quintic_at(c, tab, g.rpmag));
+  }
+  return U;
+}
+// PAclassicalFitClass::dU with dUlong taken out (ShortRangeClass.cc:282-286).
+__device__ __forceinline__ double coulomb_dU(const DCoulomb<double> &c, const LinkGeom<double> &g, int level) {
+  double dU = c.z1z2 / g.q;
+  if (c.long_range) {
+    const double *tab = c.dulong + (size_t)level * c.np * 6;
+    dU -= 0.5 * (quintic_at(c, tab, g.rmag) + quintic_at(c, tab, g.rpmag));
+  }
+  return dU;
+}
+
 template <typename R, int KIND>
 __device__ __forceinline__ R pa_U(const DevPA &pa, const typename Pair2<R>::T *diag, const LinkGeom<R> &g,
                                   int level);
+template <>
+__device__ __forceinline__ double pa_U<double, PA_COULOMB>(const DevPA &pa, const double2 *,
+                                                           const LinkGeom<double> &g, int level) {
+  return coulomb_U<double>(pa.c64, g, level);
+}
+template <>
+__device__ __forceinline__ float pa_U<float, PA_COULOMB>(const DevPA &pa, const float2 *, const LinkGeom<float> &g,
+                                                         int level) {
+  return coulomb_U<float>(pa.c32, g, level);
+}
 template <>
 __device__ __forceinline__ double pa_U<double, PA_DAVID>(const DevPA &pa, const double2 *diag,
                                                          const LinkGeom<double> &g, int level) {
@@ -463,6 +507,10 @@ __device__ __forceinline__ double pa_dU(const DevPA &pa, const LinkGeom<double> 
 template <>
 __device__ __forceinline__ double pa_dU<PA_DAVID>(const DevPA &pa, const LinkGeom<double> &g, int level) {
   return david_dU<double>(pa.d64, g.s2, g.q, g.z, level);
+}
+template <>
+__device__ __forceinline__ double pa_dU<PA_COULOMB>(const DevPA &pa, const LinkGeom<double> &g, int level) {
+  return coulomb_dU(pa.c64, g, level);
 }
 template <>
 __device__ __forceinline__ double pa_dU<PA_TRICUBIC>(const DevPA &pa, const LinkGeom<double> &g, int level) {

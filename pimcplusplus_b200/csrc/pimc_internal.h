@@ -80,7 +80,26 @@ struct DTricubic {
   const R *pot_y, *pot_d2;  // SplinePot natural cubic spline
 };
 
-enum PAKind : int { PA_NONE = 0, PA_DAVID = 1, PA_TRICUBIC = 2 };
+enum PAKind : int { PA_NONE = 0, PA_DAVID = 1, PA_TRICUBIC = 2, PA_COULOMB = 3 };
+
+// Points of the long-range r grid, LongGrid of LongRangeClass (LongRangeClass.cc:547-549).
+constexpr int kLongGridPoints = 1000;
+
+// PAclassicalFitClass with a CoulombPot (PAclassicalFit.cc:57-75, 175-288):
+// U = beta_l Z1Z2 / q, dU = Z1Z2 / q, beta_l = smallest_beta 2^l.  With the
+// long-range breakup set, ShortRangeClass subtracts 1/2 (Ulong_l(r) +
+// Ulong_l(r')) (dUlong for d_dBeta), Ulong_l a natural quintic spline on the
+// LongGrid stored as the Taylor coefficients of each interval at its left
+// knot, {y, y', y''/2, y^(3)/6, y^(4)/24, y^(5)/120}: ulong[level][point][6].
+template <typename R>
+struct DCoulomb {
+  R z1z2, smallest_beta;
+  int num_levels;
+  int long_range;  // 1: subtract the long-range part
+  int np;
+  R h, hinv;       // LongGrid spacing (start 0)
+  const R *ulong, *dulong;
+};
 
 struct DevPA {
   int kind;
@@ -88,7 +107,22 @@ struct DevPA {
   DDavid<float> d32;
   DTricubic<double> t64;
   DTricubic<float> t32;
+  DCoulomb<double> c64;
+  DCoulomb<float> c32;
 };
+
+// The optimized breakup of a Coulomb pair action (breakup.cc).
+struct BreakupTables {
+  double rc = 0, rmax = 0, knots_delta = 0;
+  int levels = 0, num_k = 0, kpoints = 0;
+  std::vector<double> ulong_k, dulong_k;          // [level][k]
+  std::vector<double> ulong_r0, dulong_r0, ushort_k0, dushort_k0, ulong_k0, dulong_k0;  // [level]
+  std::vector<double> ulong_r, dulong_r;          // [level][kLongGridPoints][6]
+};
+int coulomb_breakup(const double box[3], double z1z2, double smallest_beta, int num_levels, int num_knots,
+                    double kcut, int num_k, const double *kvecs, BreakupTables &out);
+bool quintic_natural(int n, double h, const double *y, double *coef);
+double quintic_eval(int n, double start, double h, const double *coef, double x);
 
 struct DevSystem {
   int N, S;  // particles, path rows
