@@ -88,6 +88,7 @@ def lib():
         "oracle_rng_seed": (None, [p, u64]),
         "oracle_run_bisection": (i, [p, i, C.POINTER(MoveRecord)]),
         "oracle_rng_position": (u64, [p]),
+        "oracle_set_ulong": (None, [p, i, i, d, C.POINTER(d), C.POINTER(d)]),
         "oracle_energy": (None, [p, C.POINTER(d)]),
         "oracle_gofr_accumulate": (None, [p, d, d, i, C.POINTER(u64)]),
         "oracle_run_windows": (i, [p, i, C.POINTER(MoveRecord)]),
@@ -330,6 +331,14 @@ class System:
 
     def rng_position(self):
         return lib().oracle_rng_position(self.h)
+
+    def set_ulong(self, ulong_r, dulong_r, rmax):
+        """Ulong/dUlong quintic coefficient tables [levels][points][6] on [0, rmax]."""
+        u = np.ascontiguousarray(ulong_r, dtype=np.float64)
+        du = np.ascontiguousarray(dulong_r, dtype=np.float64)
+        self._keep_ulong = (u, du)
+        lib().oracle_set_ulong(self.h, u.shape[0], u.shape[1], rmax / (u.shape[1] - 1),
+                               u.ctypes.data_as(C.POINTER(C.c_double)), du.ctypes.data_as(C.POINTER(C.c_double)))
 
     def energy(self):
         """ActionsClass::Energy terms of the OLD copy."""

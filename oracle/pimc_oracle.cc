@@ -809,11 +809,16 @@ struct OracleSystem {
     for (int i = 0; i < 3; i++) disp[i] -= n[i] * IsPeriodic[i] * Box[i];
     return sqrt(disp[0] * disp[0] + disp[1] * disp[1] + disp[2] * disp[2]);
   }
-  // ShortRangePotClass::V(slice) (ShortRangePotClass.cc:28-47), no long range
+  // ShortRangePotClass::V(slice) (ShortRangePotClass.cc:28-47); Vlong of the
+  // classical Coulomb action is its dUlong(0) (the V breakup fits the same X_k).
   double VSlice(int slice) {
     double val = 0.0;
     for (int ptcl1 = 0; ptcl1 < N; ptcl1++)
-      for (int ptcl2 = 0; ptcl2 < ptcl1; ptcl2++) val += pa->V(Dist1(slice, ptcl1, ptcl2));
+      for (int ptcl2 = 0; ptcl2 < ptcl1; ptcl2++) {
+        const double dist = Dist1(slice, ptcl1, ptcl2);
+        val += pa->V(dist);
+        if (pa->IsLongRange() && UseLongRange) val -= dUlong(0, dist);
+      }
     return val;
   }
   // PathClass::DistDisp two-slice version (PathClass.h:696-746)
@@ -875,8 +880,16 @@ struct OracleSystem {
           double q = 0.5 * (rmag + rpmag);
           double z = (rmag - rpmag);
           double U = pa->U(q, z, s2, level);
-          if (pa->IsLongRange() && UseLongRange) U -= 0.5 * (Ulong(level, rmag) + Ulong(level, rpmag));
-          TotalU += absolute ? fabs(U) : U;
+          // The absolute variant (a scale for the mixed-precision tolerance)
+          // adds the magnitudes of the pair action and of the long-range part
+          // separately: the difference cancels, their rounding does not.
+          double mag = fabs(U);
+          if (pa->IsLongRange() && UseLongRange) {
+            const double ul = 0.5 * (Ulong(level, rmag) + Ulong(level, rpmag));
+            U -= ul;
+            mag += fabs(ul);
+          }
+          TotalU += absolute ? mag : U;
         }
       }
     }
@@ -901,10 +914,32 @@ struct OracleSystem {
         }
     return dU;
   }
-  // The long-range r-space pieces are not part of this oracle yet; the
-  // configurations here run with UseLongRange=false for the short-range sum.
-  double Ulong(int, double) { return 0.0; }
-  double dUlong(int, double) { return 0.0; }
+  // PairActionFitClass::Ulong(level) / dUlong(level): QuinticSpline objects on
+  // the LongGrid [0, rmax] (LongRangeClass.cc:547-549, 629, 818); here given
+  // as Taylor coefficients per interval [level][point][6], evaluated as
+  // QuinticSpline::operator() does (QuinticSpline.h:164-221).
+  std::vector<double> ULongTab, dULongTab;
+  int ULongPoints = 0;
+  double ULongDelta = 0.0;
+  double Quintic(const std::vector<double> &tab, int level, double x) const {
+    if (ULongPoints == 0) return 0.0;
+    const double deltainv = 1.0 / ULongDelta;
+    int J = (int)nearbyint((x - 0.0) * deltainv - 0.5) + 1;
+    int I = J - 1;
+    if (I < 0) {
+      I = 0;
+      J = 1;
+    }
+    if (J > (ULongPoints - 1)) {
+      J = ULongPoints - 1;
+      I = J - 1;
+    }
+    const double *c = &tab[((size_t)level * ULongPoints + I) * 6];
+    double P = (x - (0.0 + (double)I * ULongDelta));
+    return ((((c[5] * P + c[4]) * P + c[3]) * P + c[2]) * P + c[1]) * P + c[0];
+  }
+  double Ulong(int level, double r) { return Quintic(ULongTab, level, r); }
+  double dUlong(int level, double r) { return Quintic(dULongTab, level, r); }
 
   // KineticClass::SingleAction (KineticClass.cc:33-90)
   double KineticSingle(int slice1, int slice2, const int *changed, int nchanged, int level) {
@@ -1391,6 +1426,18 @@ int oracle_run_bisection(OracleSystem *s, int n_blocks, OracleMoveRecord *record
   return 0;
 }
 uint64_t oracle_rng_position(OracleSystem *s) { return s->rng.nlocal; }
+
+// Ulong / dUlong quintic tables [levels][points][6] on [0, (points-1) delta];
+// turns on Actions.UseLongRange (the short-range subtraction, and the long-range
+// action in the bisection's lowest stage when k-vectors are set).
+void oracle_set_ulong(OracleSystem *s, int levels, int points, double delta, const double *ulong,
+                      const double *dulong) {
+  s->ULongTab.assign(ulong, ulong + (size_t)levels * points * 6);
+  s->dULongTab.assign(dulong, dulong + (size_t)levels * points * 6);
+  s->ULongPoints = points;
+  s->ULongDelta = delta;
+  s->UseLongRange = 1;
+}
 
 // ActionsClass::Energy (ActionsClass.cc:812-871) on the OLD copy: out =
 // {kinetic, dUShort, dULong, vShort, vLong (0), total per slice}

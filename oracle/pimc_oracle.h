@@ -125,6 +125,9 @@ int oracle_run_bisection(OracleSystem *s, int n_blocks, OracleMoveRecord *record
  * fit); returns windows = floor((slices-1)/2^L). */
 int oracle_run_windows(OracleSystem *s, int n_rounds, OracleMoveRecord *records);
 uint64_t oracle_rng_position(OracleSystem *s);
+/* Ulong / dUlong quintic tables [levels][points][6]; sets UseLongRange. */
+void oracle_set_ulong(OracleSystem *s, int levels, int points, double delta, const double *ulong,
+                      const double *dulong);
 /* ActionsClass::Energy terms on the OLD copy: {kinetic, dUShort, dULong,
  * vShort, vLong (0), (kinetic+dUShort+dULong)/M}. */
 void oracle_energy(OracleSystem *s, double *out);
