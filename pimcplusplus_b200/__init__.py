@@ -448,13 +448,14 @@ class BisectionBlock:
     """
 
     def __init__(self, path_data: PathData, num_levels, steps_per_block=1, shortrange_at_higher_levels=True,
-                 precision=FP64, shadow=False, cluster_ctas=0, threads_per_cta=0, schedule=SEQUENTIAL):
+                 precision=FP64, shadow=False, cluster_ctas=0, threads_per_cta=0, schedule=SEQUENTIAL,
+                 use_longrange=False):
         self.PathData = path_data
         d = BisectionDesc()
         d.num_levels = num_levels
         d.steps_per_block = steps_per_block
         d.shortrange_at_higher_levels = int(shortrange_at_higher_levels)
-        d.use_longrange = 0
+        d.use_longrange = int(use_longrange)
         d.precision = precision
         d.shadow = int(shadow)
         d.cluster_ctas = cluster_ctas

@@ -159,6 +159,38 @@ __device__ __forceinline__ double sample_level(double (*w_old)[3], double (*w_ne
 
 }  // namespace
 
+// e^{i k.r} of one k-vector: the phase in FP64, its sine and cosine in R (the
+// FP32 path reduces the phase to [-pi, pi] in FP64 first).
+template <typename R>
+__device__ __forceinline__ double2 cis_k(const double *kv, const double r[3]);
+template <>
+__device__ __forceinline__ double2 cis_k<double>(const double *kv, const double r[3]) {
+  const double th = radd(radd(rmul(kv[0], r[0]), rmul(kv[1], r[1])), rmul(kv[2], r[2]));
+  double sn, cs;
+  sincos(th, &sn, &cs);
+  return make_double2(cs, sn);
+}
+template <>
+__device__ __forceinline__ double2 cis_k<float>(const double *kv, const double r[3]) {
+  const double th = radd(radd(rmul(kv[0], r[0]), rmul(kv[1], r[1])), rmul(kv[2], r[2]));
+  const double n = rint(th * 0.15915494309189535);  // 1 / (2 pi)
+  const float red = (float)(th - n * 6.283185307179586);
+  float sn, cs;
+  sincosf(red, &sn, &cs);
+  return make_double2((double)cs, (double)sn);
+}
+// rho_k of the NEW path at one slice after the moved particle's update
+// (PathClass::UpdateRho_ks, PathClass.cc:649-707): NEW = OLD, + e^{ik.r_new},
+// - e^{ik.r_old}, in that order.
+template <typename R>
+__device__ __forceinline__ double2 rho_new_k(double2 ro, const double *kv, const double rn[3], const double rold[3]) {
+  const double2 cn = cis_k<R>(kv, rn), co = cis_k<R>(kv, rold);
+  double2 r = make_double2(ro.x + cn.x, ro.y + cn.y);
+  r.x -= co.x;
+  r.y -= co.y;
+  return r;
+}
+
 // OLD and NEW action sums of one stage level over this CTA's share of the
 // (partner, link) items, plus the moved particle's kinetic links on cluster
 // rank 0.  Partner positions are read once and serve both copies.  Returns
@@ -296,6 +328,33 @@ __device__ __forceinline__ double4 stage_sums(const BisectionArgs &a, const doub
           so += v;
           so2 += v2;
         }
+      }
+    }
+  }
+  if (a.use_lr && lv == 0) {
+    // LongRangeClass::SingleAction (LongRangeClass.cc:273-371) over the
+    // window's slices [slice1, slice1 + 2^L] with weight 1/2 at both ends:
+    // sum_k Ulong_k |rho_k|^2 of the OLD and of the updated NEW rho_k.  The
+    // Madelung and background terms are the same in both and cancel in dS.
+    const int nk = a.nk;
+    const int total = (span + 1) * nk;
+    const int chunk = (total + (int)CL - 1) / (int)CL;
+    const int beg = chunk * (int)rank;
+    const int end = min(total, beg + chunk);
+    for (int it = beg + etid; it < end; it += ethreads) {
+      const int rel = it / nk, k = it - rel * nk;
+      const double f = (rel == 0 || rel == span) ? 0.5 : 1.0;
+      const double2 ro = __ldcg(&a.rhok[(size_t)(slice1 + rel) * nk + k]);
+      const double *kv = a.kvec + 3 * k;
+      const double u = __ldg(&a.ulong_k0[k]);
+      const double2 rn = rho_new_k<R>(ro, kv, w_new[rel], w_old[rel]);
+      const double o2 = ro.x * ro.x + ro.y * ro.y, n2 = rn.x * rn.x + rn.y * rn.y;
+      so += f * o2 * u;
+      sn += f * n2 * u;
+      if (SHADOW) {
+        const double2 rs = rho_new_k<RS>(ro, kv, w_new[rel], w_old[rel]);
+        so2 += f * o2 * u;
+        sn2 += f * (rs.x * rs.x + rs.y * rs.y) * u;
       }
     }
   }
@@ -710,6 +769,22 @@ __device__ void run_job(const BisectionArgs &a, ChainState *cs, int window, unsi
     have_next = s_next[0] != 0;
     // ---- AcceptCopy (PathClass.cc:797-863); a rejected move left HBM untouched ----
     if (acc_all) {
+      if (a.use_lr) {
+        // AcceptCopy of rho_k (PathClass.cc:797-863): the NEW rho_k of the
+        // window, recomputed with the arithmetic of the stage sums, from the
+        // positions before PutInBoxFast as UpdateRho_ks saw them.  Split over
+        // the cluster's CTAs; with concurrent windows only interior slices are
+        // written (end slices are shared with the neighbouring windows, and
+        // their update is rounding only).
+        const int lo = a.concurrent ? 1 : 0, hi = a.concurrent ? span - 1 : span;
+        const int nk = a.nk, total = (hi - lo + 1) * nk;
+        for (int it = (int)rank * G.size + tid; it < total; it += (int)CL * G.size) {
+          const int rel = lo + it / nk, k = it - (it / nk) * nk;
+          double2 *p2 = &a.rhok[(size_t)(slice1 + rel) * nk + k];
+          const double2 rn = rho_new_k<R>(__ldcg(p2), a.kvec + 3 * k, w_new[rel], w_old[rel]);
+          __stcg(p2, rn);
+        }
+      }
       if (rank == 0)
         for (int rel = tid; rel <= span; rel += G.size) {
           double v[3] = {w_new[rel][0], w_new[rel][1], w_new[rel][2]};

@@ -17,6 +17,12 @@ struct BisectionArgs {
   int num_levels, steps_per_block, n_blocks, sr_higher;
   int concurrent;             // 0: sequential schedule; 1: concurrent windows, one round per launch
   unsigned long long round;   // Common-stream index of this round (concurrent)
+  // LongRangeClass::SingleAction in the lowest stage (BisectionBlock.cc:92-103):
+  // rho_k of the OLD path [slice][k], the k-vectors [k][3] and Ulong_k of level 0
+  double2 *rhok;
+  const double *kvec;
+  const double *ulong_k0;
+  int nk, use_lr;
 };
 
 cudaError_t bisection_occupancy(const BisectionArgs &a, int precision, int shadow, int cluster_ctas, int threads,

@@ -271,6 +271,7 @@ int pimc_destroy(pimc_context *ctx) {
   cudaFree(ctx->d_ulong_k);
   cudaFree(ctx->d_dulong_k);
   cudaFree(ctx->d_gofr);
+  cudaFree(ctx->d_kvec);
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
   delete ctx;
   return PIMC_OK;
@@ -425,6 +426,7 @@ int pimc_set_path(pimc_context *ctx, int copy, const double *path) {
     if (copy == PIMC_BOTH || copy == c)
       CK(cudaMemcpyAsync(ctx->d_path[c], path, ctx->path_elems * sizeof(double), cudaMemcpyHostToDevice,
                          ctx->stream));
+  if (copy != PIMC_NEW) ctx->rhok_valid = false;  // the device moves recompute rho_k of the new OLD path
   CK(cudaStreamSynchronize(ctx->stream));
   return PIMC_OK;
 }
@@ -608,7 +610,13 @@ int pimc_bisection_setup(pimc_context *ctx, const pimc_bisection_desc *d) {
     return fail(ctx, PIMC_E_ARG, "bad schedule");
   if (d->schedule == PIMC_SCHEDULE_WINDOWS && window_slots(ctx, d->num_levels) < 1)
     return fail(ctx, PIMC_E_ARG, "no window fits");
-  if (d->use_longrange) return fail(ctx, PIMC_E_ARG, "long range inside device moves is not available");
+  if (d->use_longrange) {
+    // LongRange joins the lowest stage (BisectionBlock.cc:92-103); its short-range
+    // counterpart must subtract the same Ulong
+    if (!ctx->lr_ready || ctx->num_k <= 0) return fail(ctx, PIMC_E_STATE, "long range needs k-vectors and tables");
+    if (!(ctx->pa.kind == PA_COULOMB && ctx->pa.c64.long_range))
+      return fail(ctx, PIMC_E_ARG, "long range in device moves needs the Coulomb action's breakup (pimc_longrange_coulomb)");
+  }
   if (int rc2 = pa_levels_ok(ctx, d->num_levels)) return rc2;
   CK(cudaSetDevice(ctx->device));
   ctx->bis = *d;
@@ -671,6 +679,15 @@ static int run_bisection(pimc_context *ctx, int n_blocks, pimc_move_record *devi
   a.sr_higher = ctx->bis.shortrange_at_higher_levels;
   a.concurrent = ctx->bis.schedule == PIMC_SCHEDULE_WINDOWS;
   a.round = ctx->rounds;
+  a.use_lr = ctx->bis.use_longrange ? 1 : 0;
+  a.rhok = ctx->d_rhok[0];
+  a.kvec = ctx->d_kvec;
+  a.ulong_k0 = ctx->d_ulong_k;  // level 0 row
+  a.nk = ctx->num_k;
+  if (a.use_lr && !ctx->rhok_valid) {  // PathClass::UpdateRho_ks() of the current OLD path
+    CK(launch_rhok_full(ctx->stream, ctx->d_path[0], ctx->sys.N, ctx->sys.S, lr_desc(ctx), ctx->d_rhok[0]));
+    ctx->rhok_valid = true;
+  }
   const int cl = ctx->bis.cluster_ctas, thr = ctx->bis.threads_per_cta;
   if (!a.concurrent) {
     CK(launch_bisection(a, ctx->bis.precision, ctx->bis.shadow, cl, 1, thr, ctx->stream));
@@ -710,6 +727,9 @@ int pimc_run_bisection(pimc_context *ctx, int n_blocks, pimc_move_record *trace,
   // The device moves advance OLD only; bring NEW back in sync (MirroredClass invariant).
   CK(cudaMemcpyAsync(ctx->d_path[1], ctx->d_path[0], ctx->path_elems * sizeof(double), cudaMemcpyDeviceToDevice,
                      ctx->stream));
+  if (ctx->bis.use_longrange)
+    CK(cudaMemcpyAsync(ctx->d_rhok[1], ctx->d_rhok[0], (size_t)ctx->sys.S * ctx->num_k * sizeof(double2),
+                       cudaMemcpyDeviceToDevice, ctx->stream));
   if (trace && nrec)
     CK(cudaMemcpyAsync(trace, ctx->d_trace, nrec * sizeof(pimc_move_record), cudaMemcpyDeviceToHost, ctx->stream));
   CK(cudaStreamSynchronize(ctx->stream));
@@ -790,6 +810,11 @@ int pimc_setup_kvecs(pimc_context *ctx, double kcutoff, int *num_k) {
   if (kidx.size() > 1024) return fail(ctx, PIMC_E_ARG, "more than 1024 k-vectors");
   ctx->num_k = (int)kidx.size();
   ctx->kcutoff = kcutoff;
+  ctx->rhok_valid = false;
+  cudaFree(ctx->d_kvec);
+  ctx->d_kvec = nullptr;
+  CK(cudaMalloc(&ctx->d_kvec, ctx->kvecs.size() * sizeof(double) + 16));
+  CK(cudaMemcpy(ctx->d_kvec, ctx->kvecs.data(), ctx->kvecs.size() * sizeof(double), cudaMemcpyHostToDevice));
   cudaFree(ctx->d_kidx);
   cudaFree(ctx->d_rhok[0]);
   cudaFree(ctx->d_rhok[1]);
@@ -852,6 +877,7 @@ int pimc_calc_rhok(pimc_context *ctx) {
   CK(cudaMemcpyAsync(ctx->d_rhok[1], ctx->d_rhok[0], (size_t)ctx->sys.S * ctx->num_k * sizeof(double2),
                      cudaMemcpyDeviceToDevice, ctx->stream));
   CK(cudaStreamSynchronize(ctx->stream));
+  ctx->rhok_valid = true;
   return PIMC_OK;
 }
 

@@ -189,6 +189,8 @@ struct pimc_context {
   std::vector<double> kvecs;  // [k][3]
   int3 *d_kidx = nullptr;
   double2 *d_rhok[2] = {nullptr, nullptr};
+  double *d_kvec = nullptr;  // [k][3] for the device moves
+  bool rhok_valid = false;   // d_rhok[OLD] holds rho_k of the OLD path
   bool lr_ready = false;
   int lr_levels = 0, use_background = 0;
   double *d_ulong_k = nullptr, *d_dulong_k = nullptr;  // [levels][k]

@@ -88,3 +88,84 @@ def test_energy_terms_coulomb():
     for k in ("kinetic", "du_short", "du_long", "v_short", "total"):
         assert rel_err(got[k], ref[k], max(abs(ref[k]), 1e-8)) < 1e-12, (k, got[k], ref[k])
     d.close()
+
+
+def jellium_moves(seed=21, **kw):
+    o, d, m, levels = jellium(**kw)
+    start = o.get_path(0)
+    o.set_path(start, 1)
+    d.set_path(start)
+    o.calc_rhok_all()
+    return o, d, m, levels
+
+
+def compare(ref, got, stats, tol=1e-9):
+    assert len(ref) == len(got)
+    n_acc = 0
+    for i, (r, g) in enumerate(zip(ref, got)):
+        assert (r.slice1, r.ptcl, r.accepted, r.stages_passed) == (
+            int(g["slice1"]), int(g["ptcl"]), int(g["accepted"]), int(g["stages_passed"])), i
+        for k in range(8):
+            assert abs(r.dS[k] - g["dS"][k]) <= tol * max(1.0, abs(r.dS[k])), (i, k, r.dS[k], g["dS"][k])
+        n_acc += r.accepted
+    assert stats["status"] == 0 and stats["accepted"] == n_acc
+    return n_acc
+
+
+@pytest.mark.parametrize("cluster", [1, 2])
+def test_bisection_jellium_longrange_trace(cluster):
+    """Device moves with LongRange in the lowest stage (rho_k updated per
+    moved slice, written back on acceptance) replay the oracle's trace."""
+    o, d, m, levels = jellium_moves()
+    L, spb = 3, 4
+    o.bisection_config(L, spb, use_longrange=True)
+    o.rng_seed(5)
+    ref = o.run_bisection(40)
+    bb = P.BisectionBlock(d, L, spb, cluster_ctas=cluster, threads_per_cta=128, use_longrange=True)
+    bb.seed(5)
+    got, stats = bb.MakeMoves(40)
+    assert compare(ref, got, stats) > 10
+    assert np.max(np.abs(d.get_path(P.OLDMODE) - o.get_path(0))) < 1e-9
+    rk_o, rk_d = o.rhok(0), d.get_rhok(P.OLDMODE)
+    assert np.max(np.abs(rk_d - rk_o)) < 1e-9 * np.max(np.abs(rk_o))
+    # the rho_k the moves maintained is that of the final path
+    o.calc_rhok_all()
+    assert np.max(np.abs(rk_d - o.rhok(0))) < 1e-9 * np.max(np.abs(rk_o))
+    d.close()
+
+
+def test_bisection_jellium_longrange_windows():
+    o, d, m, levels = jellium_moves(seed=23)
+    L, spb = 2, 3
+    o.bisection_config(L, spb, use_longrange=True)
+    o.rng_seed(9)
+    ref = o.run_windows(6)
+    bb = P.BisectionBlock(d, L, spb, cluster_ctas=1, threads_per_cta=128, use_longrange=True, schedule=P.WINDOWS)
+    bb.seed(9)
+    got, stats = bb.MakeMoves(6)
+    live = [(r, g) for r, g in zip(ref, got) if r.slice1 >= 0]
+    assert len(live) > 10
+    for i, (r, g) in enumerate(live):
+        assert (r.slice1, r.ptcl, r.accepted, r.stages_passed) == (
+            int(g["slice1"]), int(g["ptcl"]), int(g["accepted"]), int(g["stages_passed"])), i
+        for k in range(8):
+            assert abs(r.dS[k] - g["dS"][k]) <= 1e-9 * max(1.0, abs(r.dS[k])), (i, k)
+    assert np.max(np.abs(d.get_path(P.OLDMODE) - o.get_path(0))) < 1e-9
+    o.calc_rhok_all()
+    assert np.max(np.abs(d.get_rhok(P.OLDMODE) - o.rhok(0))) < 1e-9 * np.max(np.abs(o.rhok(0)))
+    d.close()
+
+
+def test_bisection_jellium_mixed_shadow():
+    """Mixed path (FP32 pair terms and FP32 sincos of reduced phases, FP64
+    sums): per-stage dS relative error against the FP64 terms, and flips."""
+    o, d, m, levels = jellium_moves(seed=29)
+    bb = P.BisectionBlock(d, 3, 4, precision=P.MIXED, shadow=True, cluster_ctas=1, threads_per_cta=128,
+                          use_longrange=True)
+    bb.seed(3)
+    rec, stats = bb.MakeMoves(100)
+    mask = rec["dS_shadow"] != 0.0
+    rel = np.abs(rec["dS"][mask] - rec["dS_shadow"][mask]) / np.maximum(np.abs(rec["dS_shadow"][mask]), 1e-3)
+    assert np.median(rel) < 1e-5, np.median(rel)
+    assert stats["flips"] <= 0.01 * stats["stages_attempted"] + 1
+    d.close()
