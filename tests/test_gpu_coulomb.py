@@ -169,3 +169,33 @@ def test_bisection_jellium_mixed_shadow():
     assert np.median(rel) < 1e-5, np.median(rel)
     assert stats["flips"] <= 0.01 * stats["stages_attempted"] + 1
     d.close()
+
+
+def test_jellium_energy_within_2sigma_mixed_vs_oracle():
+    """Independent chains sample the same distribution: the mixed device
+    chain (concurrent windows, long range in the moves) and the FP64 oracle
+    chain agree on the energy within 2 combined sigma (blocking)."""
+    o, d, m, levels = jellium_moves(seed=31)
+    L = 2
+    windows = m >> L
+    per_sweep = 32 * windows
+    o.bisection_config(L, per_sweep, use_longrange=True)
+    o.rng_seed(111)
+    bb = P.BisectionBlock(d, L, 32, precision=P.MIXED, cluster_ctas=1, threads_per_cta=128, use_longrange=True,
+                          schedule=P.WINDOWS)
+    bb.seed(8)
+    # small bisection moves accept ~98 %: long chains for independent blocks
+    burn, sweeps, nb = 200, 4000, 20
+    e_o, e_d = [], []
+    for sw in range(burn + sweeps):
+        o.run_bisection(1)
+        bb.MakeMoves(1, trace=False)
+        if sw >= burn:
+            e_o.append(o.energy()["total"])
+            e_d.append(d.energy()["total"])
+    k = len(e_o) // nb
+    bo = np.asarray(e_o)[: k * nb].reshape(nb, k).mean(1)
+    bd = np.asarray(e_d)[: k * nb].reshape(nb, k).mean(1)
+    so, sd = bo.std(ddof=1) / np.sqrt(nb), bd.std(ddof=1) / np.sqrt(nb)
+    assert abs(bo.mean() - bd.mean()) <= 2.0 * np.hypot(so, sd), (bo.mean(), so, bd.mean(), sd)
+    d.close()
