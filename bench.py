@@ -350,6 +350,7 @@ def run_ours(args):
         e2e_evals_timed = float(v.item())
 
     c3 = None if args.no_c3 else run_c3(args, P, torch, flush, local, rank, world, agg)
+    c4 = None if args.no_c4 else run_c4(args, P, torch, flush, local, rank, world, agg)
     clocks = sampler.stop() if sampler else None
     if clocks:
         clocks["window"] = "all timed legs (C2 FP64, mixed, other schedule, accuracy, e2e, C3)"
@@ -405,6 +406,9 @@ def run_ours(args):
         if c3:
             line["c3"] = c3
             line["gpu_launches"] += c3.pop("_launches")
+        if c4:
+            line["c4"] = c4
+            line["gpu_launches"] += c4.pop("_launches")
         if cpu:
             line["cpu_baseline"] = {"value": cpu["value"], "unit": UNIT, "cores": cpu["cores"], "kind": "port",
                                     "sample": cpu["sample"]}
@@ -530,6 +534,101 @@ def run_c3(args, P, torch, flush, local, rank, world, agg):
     }
 
 
+def run_c4(args, P, torch, flush, local, rank, world, agg):
+    """Jellium (C4): 128 electrons at r_s = 4 bohr, beta = 8 Ry^-1, M = 64,
+    classical Coulomb pair action with the optimized breakup (49 knots,
+    k cutoff 1.2 bohr^-1: 510 k-vectors), bisection level 3, concurrent
+    windows, LongRange with the rho_k update in every move's lowest stage."""
+    n, m, L, levels = 128, 64, 3, 3
+    boxl = (4.0 * math.pi / 3.0 * n) ** (1.0 / 3.0) * 4.0
+    box = np.array([boxl] * 3)
+    tau = 8.0 / m
+    start = initial_path(n, m + 1, box, 41 + rank, 0.0)
+    spb = 16
+
+    def make(precision, shadow=False, schedule=None):
+        d = P.PathData(n, m + 1, box, tau, 1.0, 0, device=local)
+        d.pa_coulomb(2.0, levels)
+        nk = d.setup_kvecs(1.2)
+        d.longrange_coulomb(49, use_background=True)
+        d.set_path(start)
+        bb = P.BisectionBlock(d, L, spb, precision=precision, shadow=shadow, cluster_ctas=args.c4_cluster,
+                              threads_per_cta=256, schedule=schedule if schedule is not None else P.WINDOWS,
+                              use_longrange=True)
+        bb.seed(500 + rank)
+        return d, bb, nk
+
+    rounds = max(1, 2048 // (spb * ((m) >> L)))
+
+    def timed(precision):
+        d, bb, nk = make(precision)
+        stream = torch.cuda.ExternalStream(P.lib().pimc_stream(d.h), device=f"cuda:{local}")
+        for _ in range(args.warmup):
+            bb.launch_async(rounds)
+        d.synchronize()
+        s0 = bb.stats()
+        times = []
+        for _ in range(args.steps):
+            with torch.cuda.stream(stream):
+                flush.zero_()
+                e0 = torch.cuda.Event(enable_timing=True)
+                e1 = torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                bb.launch_async(rounds)
+                e1.record(stream)
+            e1.synchronize()
+            times.append(e0.elapsed_time(e1))
+        s1 = bb.stats()
+        if s1["status"]:
+            raise RuntimeError(f"C4 device status {s1['status']}")
+        # share of moves that reach the lowest stage (its rho_k update covers 2^L + 1 slices)
+        rec, _ = bb.MakeMoves(rounds, trace=True)
+        live = rec["slice1"] >= 0
+        frac0 = float(np.mean(rec["stages_passed"][live] >= L - 1)) if live.any() else 0.0
+        d.close()
+        st = {k: s1[k] - s0[k] for k in ("moves", "accepted", "pair_evals", "stages_attempted")}
+        ms, st = agg(float(np.sum(times)), st)
+        return ms, st, frac0, nk
+
+    ms32, st32, f32, nk = timed(P.MIXED)
+    ms64, st64, f64, _ = timed(P.FP64)
+    d, bb, _ = make(P.MIXED, shadow=True, schedule=P.SEQUENTIAL)
+    bb.MakeMoves(20, trace=False)
+    rec, sh = bb.MakeMoves(max(1, args.accuracy_moves // spb), trace=True)
+    d.close()
+    mask = rec["dS_shadow"] != 0.0
+    rel = np.abs(rec["dS"][mask] - rec["dS_shadow"][mask]) / np.abs(rec["dS_shadow"][mask])
+
+    def rates(ms, st, frac0):
+        s = ms / 1000.0
+        upd = st["moves"] * frac0 * ((1 << L) + 1)
+        return {"pair_evals_per_s": st["pair_evals"] / s, "moves_per_s": st["moves"] / s,
+                "accepted_moves_per_s": st["accepted"] / s, "rhok_updates_per_s": upd / s,
+                "ms_per_step": ms / args.steps}
+
+    r32, r64 = rates(ms32, st32, f32), rates(ms64, st64, f64)
+    peak, peak_kind = load_peaks()
+    # algorithmic bytes: 1-D Coulomb pair eval in FP32 = partner at 2 slices (24 B) + two
+    # Ulong quintic cells (2 x 24 B); rho_k update = OLD read + NEW write, 32 B per k
+    secs = ms32 / 1000.0 / args.steps
+    achieved = ((st32["pair_evals"] / world / args.steps) * 72 +
+                r32["rhok_updates_per_s"] / world * secs * 32 * nk) / secs / 1e9
+    return {
+        "workload": f"jellium N={n}, r_s=4 bohr, beta=8 Ry^-1, M={m}, classical Coulomb action with optimized "
+                    f"breakup (49 knots), {nk} k-vectors, bisection level {L}, concurrent windows, "
+                    f"{args.c4_cluster}-CTA clusters",
+        "mixed": r32, "fp64": r64,
+        "mixed_over_fp64": r32["accepted_moves_per_s"] / r64["accepted_moves_per_s"],
+        "dS_relerr": {"median": float(np.median(rel)) if rel.size else None,
+                      "p99": float(np.quantile(rel, 0.99)) if rel.size else None, "stages": int(rel.size),
+                      "flip_rate": sh["flips"] / max(1, sh["stages_attempted"])},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": None, "peak_kind": peak_kind,
+                     "kernel": "bisection_kernel<PA_COULOMB,float> with LongRange"},
+        "_launches": 2 * args.steps * rounds,
+    }
+
+
 def nb_launches(schedule, blocks):
     """Bisection-kernel launches per timed step (FP64 + mixed counted by the caller)."""
     return blocks if schedule == "windows" else 1
@@ -550,6 +649,8 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-c3", action="store_true")
+    ap.add_argument("--no-c4", action="store_true")
+    ap.add_argument("--c4-cluster", type=int, default=8)
     ap.add_argument("--c3-chains", type=int, default=1024)
     ap.add_argument("--c3-blocks", type=int, default=4)
     ap.add_argument("--c3-steps-per-block", type=int, default=4)
