@@ -171,11 +171,12 @@ def lj_chain(n, m, temp, rho, levels, seed, steps_per_block=1, npts=200, r_min=1
 
 
 def lattice_path(n, slices, box, rng, jitter=0.1):
-    """n particles on the first n sites of a simple-cubic lattice filling the
-    box, each displaced by up to +-jitter of the lattice spacing, copied to
-    every slice (a classical start: no overlaps at liquid densities)."""
+    """n particles spread evenly over the sites of the smallest simple-cubic
+    lattice with at least n sites filling the box, each displaced by up to
+    +-jitter of the lattice spacing, copied to every slice (a classical
+    start: no overlaps at liquid densities)."""
     side = int(np.ceil(n ** (1.0 / 3.0) - 1e-9))
-    idx = np.arange(side ** 3)[:n]
+    idx = (np.arange(n) * side ** 3) // n
     ijk = np.stack([idx // (side * side), (idx // side) % side, idx % side], axis=1).astype(np.float64)
     a = np.asarray(box, dtype=np.float64) / side
     pts = (ijk + 0.5 + jitter * (rng.random((n, 3)) * 2.0 - 1.0)) * a - 0.5 * np.asarray(box)

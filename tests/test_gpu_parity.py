@@ -304,3 +304,43 @@ def test_bisection_trace_windows_tricubic():
     got, stats = bb.MakeMoves(50)
     compare_window_traces(ref, got, stats)
     assert np.max(np.abs(d.get_path(P.OLDMODE) - o.get_path(0))) < 1e-9
+
+
+@pytest.mark.parametrize("schedule", ["sequential", "windows"])
+def test_bisection_trace_level5_truncated_lj(tmp_path, schedule):
+    """Bisection level 5 (32-slice windows, 16 midpoints at the top level) on
+    the C5 table (LJ truncated and shifted to zero at 2.5 sigma)."""
+    cfg = dict(W.CONFIGS["C5"])
+    cfg.update(N=128, M=128)
+    tau, box = W.derived(cfg)
+    dm = W.make_dm_for(cfg, str(tmp_path))
+    n, slices, L = cfg["N"], cfg["M"] + 1, cfg["levels"]
+    o = O.System(n, slices, box, tau, W.HE4_LAMBDA, 0)
+    o.set_pa(O.PairAction.from_dm(dm, tau, 0))
+    start = W.lattice_path(n, slices, box, np.random.default_rng(51))
+    o.set_path(start, 0)
+    o.set_path(start, 1)
+    d = P.PathData(n, slices, box, tau, W.HE4_LAMBDA, 0)
+    d.set_path(start)
+    d.pa_david_from_dm(dm, 0)
+    o.bisection_config(L, 4)
+    o.rng_seed(77)
+    if schedule == "sequential":
+        ref = o.run_bisection(60)
+        bb = P.BisectionBlock(d, L, 4, cluster_ctas=4, threads_per_cta=256)
+    else:
+        ref = o.run_windows(15)
+        bb = P.BisectionBlock(d, L, 4, cluster_ctas=4, threads_per_cta=256, schedule=P.WINDOWS)
+    bb.seed(77)
+    got, stats = bb.MakeMoves(60 if schedule == "sequential" else 15)
+    live = [(r, g) for r, g in zip(ref, got) if r.slice1 >= 0]
+    assert len(live) > 20
+    acc = 0
+    for i, (r, g) in enumerate(live):
+        assert (r.slice1, r.ptcl, r.accepted, r.stages_passed) == (
+            int(g["slice1"]), int(g["ptcl"]), int(g["accepted"]), int(g["stages_passed"])), i
+        for k in range(8):
+            assert abs(r.dS[k] - g["dS"][k]) <= 1e-9 * max(1.0, abs(r.dS[k])), (i, k)
+        acc += r.accepted
+    assert 0 < acc < len(live)
+    assert np.max(np.abs(d.get_path(P.OLDMODE) - o.get_path(0))) < 1e-9
