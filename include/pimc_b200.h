@@ -181,6 +181,14 @@ typedef struct pimc_bisection_desc {
   int cluster_ctas;                 /* CTAs cooperating on one chain (1..16), 0 = auto */
   int threads_per_cta;              /* 0 = auto */
   int schedule;                     /* PIMC_SCHEDULE_SEQUENTIAL or PIMC_SCHEDULE_WINDOWS */
+  /* Neighbour lists for the short-range sum (the role of ShortRangeOnClass's
+   * cells, Actions/ShortRangeOnClass.cc:35-240), DavidPA only: > 0 turns
+   * them on with this skin (length units of the box) around each particle's
+   * path; results equal the all-partner sum, since a DavidPA table is zero
+   * beyond its grid end.  neighbor_max: list capacity per particle (0 = 1024);
+   * a particle with more partners uses all of them. */
+  double neighbor_skin;
+  int neighbor_max;
 } pimc_bisection_desc;
 
 /* One move: the fields the accept trace is compared on. */

@@ -74,6 +74,8 @@ class BisectionDesc(C.Structure):
         ("cluster_ctas", C.c_int),
         ("threads_per_cta", C.c_int),
         ("schedule", C.c_int),
+        ("neighbor_skin", C.c_double),
+        ("neighbor_max", C.c_int),
     ]
 
 
@@ -449,7 +451,7 @@ class BisectionBlock:
 
     def __init__(self, path_data: PathData, num_levels, steps_per_block=1, shortrange_at_higher_levels=True,
                  precision=FP64, shadow=False, cluster_ctas=0, threads_per_cta=0, schedule=SEQUENTIAL,
-                 use_longrange=False):
+                 use_longrange=False, neighbor_skin=0.0, neighbor_max=0):
         self.PathData = path_data
         d = BisectionDesc()
         d.num_levels = num_levels
@@ -461,6 +463,8 @@ class BisectionBlock:
         d.cluster_ctas = cluster_ctas
         d.threads_per_cta = threads_per_cta
         d.schedule = schedule
+        d.neighbor_skin = neighbor_skin
+        d.neighbor_max = neighbor_max
         self.desc = d
         self.steps_per_block = steps_per_block
         path_data._check(_lib.pimc_bisection_setup(path_data.h, C.byref(d)), "bisection_setup")

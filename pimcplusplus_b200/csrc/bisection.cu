@@ -200,7 +200,7 @@ template <int KIND, typename R, bool SHADOW>
 __device__ __forceinline__ double4 stage_sums(const BisectionArgs &a, const double (*w_old)[3],
                                               const double (*w_new)[3], const typename Pair2<R>::T *dg,
                                               const void *dgs, int lv, int slice1, int ptcl, unsigned rank,
-                                              unsigned CL, int etid, int ethreads) {
+                                              unsigned CL, int etid, int ethreads, const int *plist, int np) {
   typedef typename std::conditional<std::is_same<R, double>::value, float, double>::type RS;
   typedef typename Pair2<RS>::T P2S;
   const DevSystem &sys = a.sys;
@@ -228,7 +228,8 @@ __device__ __forceinline__ double4 stage_sums(const BisectionArgs &a, const doub
     }
   }
   if (lv == 0 || a.sr_higher) {  // ShortRangeClass::SingleAction over partners x links
-    const int np = N - 1;
+    // partners: all others (plist null, np = N - 1) or the moved particle's
+    // neighbour list (np entries, ascending)
     const int total = np * nlinks;  // < 2^31: N <= 2^20, 2^L <= 64 (host-checked)
     const int chunk = (total + (int)CL - 1) / (int)CL;
     const int beg = chunk * (int)rank;
@@ -265,7 +266,7 @@ __device__ __forceinline__ double4 stage_sums(const BisectionArgs &a, const doub
           live[u] = it < end;
           const int link = live[u] ? lk[u] : lk[0];
           const int j = live[u] ? jj[u] : jj[0];
-          const int p2 = j < ptcl ? j : j + 1;
+          const int p2 = plist ? __ldg(&plist[j]) : (j < ptcl ? j : j + 1);
           r0s[u] = link * skip;
           const double *pa_ = path + ((size_t)(slice1 + r0s[u]) * N + p2) * 3;
           const double *pb_ = path + ((size_t)(slice1 + r0s[u] + skip) * N + p2) * 3;
@@ -308,7 +309,7 @@ __device__ __forceinline__ double4 stage_sums(const BisectionArgs &a, const doub
       for (int it = beg + team; it < end; it += nteams) {
         const int link = it / np;
         const int j = it - link * np;
-        const int p2 = j < ptcl ? j : j + 1;
+        const int p2 = plist ? __ldg(&plist[j]) : (j < ptcl ? j : j + 1);
         const int r0 = link * skip;
         const double *pa_ = path + ((size_t)(slice1 + r0) * N + p2) * 3;
         const double *pb_ = path + ((size_t)(slice1 + r0 + skip) * N + p2) * 3;
@@ -413,7 +414,30 @@ struct KernelShared {
   RngSnap s_rng, s_spec1, s_spec2;
   int s_ok;
   RngTab tab;
+  // neighbour lists: bounding sphere of the moved particle (and of the
+  // speculated next one), whether a NEW position of the current stage lies
+  // outside it, and whether this job evaluates all partners from now on
+  double4 s_cb, s_next_cb;
+  int s_far, s_next_far, s_allpairs;
 };
+
+// Whether any of the window's span+1 NEW positions lies outside the moved
+// particle's bounding sphere cb (minimum image), by one warp.
+__device__ __forceinline__ int window_outside(const double (*w)[3], int span, double4 cb, const DevSystem &sys,
+                                              int lane) {
+  int out = 0;
+  for (int rel = lane; rel <= span; rel += 32) {
+    double d[3] = {w[rel][0] - cb.x, w[rel][1] - cb.y, w[rel][2] - cb.z};
+    double r2 = 0.0;
+    for (int i = 0; i < 3; i++) {
+      const double n = rint(d[i] * sys.boxinv[i]);
+      d[i] -= n * sys.box[i];
+      r2 += d[i] * d[i];
+    }
+    out |= r2 > cb.w * cb.w;
+  }
+  return __any_sync(0xffffffffu, out);
+}
 
 // Storage of the precomputed stream tables of a CTA: NF parts of kTabFine
 // positions; a group uses a contiguous run of parts.
@@ -551,6 +575,8 @@ __device__ void run_job(const BisectionArgs &a, ChainState *cs, int window, unsi
     s_rng.x2 = cs->x2;
     s_ctl[3] = 0;
     s_next[0] = 0;
+    S.s_far = 0;
+    S.s_allpairs = 0;
     S.tab = tab_mem;
     S.tab.W = 0;  // filled below
   }
@@ -613,11 +639,20 @@ __device__ void run_job(const BisectionArgs &a, ChainState *cs, int window, unsi
         DevRandom rng = rng_from(s_rng, seed, stream, &S.tab);
         const double lsr = sample_level<OUTLINE>(win_old[cur], win_new[cur], gbuf[0], L, L - 1, sys, rng, lane);
         const double lu = rng.LocalLog();
+        int far = 0;
+        double4 cb = make_double4(0.0, 0.0, 0.0, 0.0);
+        if (a.nbr_on) {
+          cb = a.nbr_cb[s_ctl[1]];
+          __syncwarp();
+          far = window_outside(win_new[cur], span, cb, sys, lane);
+        }
         __syncwarp();
         if (lane == 0) {
           s_logsr[L - 1] = lsr;
           s_logu[L - 1] = lu;
           rng_store(s_rng, rng);
+          S.s_cb = cb;
+          S.s_far = far;
         }
       }
       G.sync();
@@ -632,6 +667,7 @@ __device__ void run_job(const BisectionArgs &a, ChainState *cs, int window, unsi
     double prevDS = 0.0, prevDS_s = 0.0;
     bool acc_all = true;
     int passed = 0;
+    int move_far = 0;  // some stage of this move sampled outside the moved particle's sphere
     pimc_move_record rec;
     if (lead) {
       rec.slice1 = slice1;
@@ -641,12 +677,27 @@ __device__ void run_job(const BisectionArgs &a, ChainState *cs, int window, unsi
     int si = 0;
     for (int level = L - 1; level >= 0; level--, si++) {
       // ---- LocalStageClass::Attempt (StageClass.cc:49-95) ----
+      // Partners: the moved particle's neighbour list while its NEW positions
+      // stay inside its sphere and no earlier move of this job left one;
+      // otherwise all particles (the same sum: pairs beyond the table's end
+      // add exact zeros).
+      const int far = S.s_far;
+      move_far |= far;
+      int np = N - 1;
+      const int *plist = nullptr;
+      if (a.nbr_on && !far && !S.s_allpairs) {
+        const int cnt = __ldcg(&a.nbr_cnt[ptcl]);
+        if (cnt >= 0) {
+          np = cnt;
+          plist = a.nbr_idx + (size_t)ptcl * a.nbr_kmax;
+        }
+      }
       if (evaluator) {
         const size_t st = KIND == PA_DAVID ? (size_t)david_of<R>(a.pa).diag_stride : 0;
         const size_t sts = (KIND == PA_DAVID && SHADOW) ? (size_t)david_of<RS>(a.pa).diag_stride : 0;
         const double4 v = stage_sums<KIND, R, SHADOW>(a, w_old, w_new, diag_smem ? diag_smem + level * st : nullptr,
                                                       diag_smem_s ? diag_smem_s + level * sts : nullptr, level,
-                                                      slice1, ptcl, rank, CL, tid, ethreads);
+                                                      slice1, ptcl, rank, CL, tid, ethreads, plist, np);
         const double o1 = warp_sum(v.x), n1 = warp_sum(v.y);
         const double o2 = SHADOW ? warp_sum(v.z) : 0.0, n2 = SHADOW ? warp_sum(v.w) : 0.0;
         if (lane == 0) {
@@ -682,19 +733,28 @@ __device__ void run_job(const BisectionArgs &a, ChainState *cs, int window, unsi
           __syncwarp();
           const double lsr = sample_level<OUTLINE>(wo, wn, gbuf[1], L, L - 1, sys, spec, lane);
           const double lu = spec.LocalLog();
+          int far = 0;
+          double4 cb = make_double4(0.0, 0.0, 0.0, 0.0);
+          if (a.nbr_on) {
+            cb = a.nbr_cb[np_];
+            __syncwarp();
+            far = window_outside(wn, span, cb, sys, lane);
+          }
           __syncwarp();
           if (lane == 0) {
             s_next[1] = ns1;
             s_next[2] = np_;
             s_next_f[0] = lsr;
             s_next_f[1] = lu;
+            S.s_next_cb = cb;
+            S.s_next_far = far;
             rng_store(s_spec2, spec);
           }
         }
         if (lane < 4) sh_red[warp][lane] = 0.0;
       }
       // Counted as the reference performs them: OLD + NEW of the stage's links.
-      if (lead && (level == 0 || a.sr_higher)) pair_evals += 2ull * (unsigned long long)(N - 1) * (span >> level);
+      if (lead && (level == 0 || a.sr_higher)) pair_evals += 2ull * (unsigned long long)np * (span >> level);
       G.sync();
       // ---- reduce: warps -> CTA (warp 0) -> cluster (DSMEM, rank order) ----
       const int par = xc & 1;
@@ -741,18 +801,24 @@ __device__ void run_job(const BisectionArgs &a, ChainState *cs, int window, unsi
         if (lead && si < 8) rec.dS[si] = currActionChange;
         // commit the stream position the outcome selects
         const bool ends = !toAccept || level == 0 || status != 0;
+        // neighbour lists: whether the next stage's NEW positions (the level
+        // sampled speculatively into w_new) leave the moved particle's sphere
+        const int far_next = (a.nbr_on && !ends) ? window_outside(w_new, span, S.s_cb, sys, lane) : 0;
         if (lane == 0) {
           s_ctl[2] = toAccept ? 1 : 0;
           s_ctl[3] = status;
           int nv = 0;
           if (!ends) {
             s_rng = s_spec1;
+            S.s_far = far_next;
           } else if (status == 0 && more && specwarp >= 0 && !(toAccept && s_next[2] == ptcl)) {
             s_rng = s_spec2;
             s_ctl[0] = s_next[1];
             s_ctl[1] = s_next[2];
             s_logsr[L - 1] = s_next_f[0];
             s_logu[L - 1] = s_next_f[1];
+            S.s_cb = S.s_next_cb;
+            S.s_far = S.s_next_far;
             nv = 1;
           }
           s_next[0] = nv;
@@ -768,6 +834,12 @@ __device__ void run_job(const BisectionArgs &a, ChainState *cs, int window, unsi
     }
     have_next = s_next[0] != 0;
     // ---- AcceptCopy (PathClass.cc:797-863); a rejected move left HBM untouched ----
+    if (acc_all && move_far) {
+      // this move left its sphere: the lists no longer bound this job's
+      // positions; all partners from here on, and a rebuild before the next launch
+      if (tid == 0) S.s_allpairs = 1;
+      if (lead) atomicExch(a.nbr_dirty, 1);
+    }
     if (acc_all) {
       if (a.use_lr) {
         // AcceptCopy of rho_k (PathClass.cc:797-863): the NEW rho_k of the

@@ -23,7 +23,19 @@ struct BisectionArgs {
   const double *kvec;
   const double *ulong_k0;
   int nk, use_lr;
+  // Neighbour lists of the short-range sum (0: all partners): per particle the
+  // bounding sphere of its path {c, B} and the partners j with
+  // |c_i - c_j| <= range + B_i + B_j in ascending order (count -1: overflow)
+  int nbr_on, nbr_kmax;
+  const double4 *nbr_cb;
+  const int *nbr_cnt, *nbr_idx;
+  int *nbr_dirty;
 };
+
+// Neighbour lists for the device moves (neighbors.cu): rebuilt from the
+// current path when *dirty is set, then *dirty cleared.
+cudaError_t launch_nbr_rebuild(cudaStream_t st, const double *path, const DevSystem &sys, double range, double skin,
+                               int kmax, double4 *cb, int *cnt, int *idx, int *dirty);
 
 cudaError_t bisection_occupancy(const BisectionArgs &a, int precision, int shadow, int cluster_ctas, int threads,
                                 int *max_clusters);

@@ -272,6 +272,10 @@ int pimc_destroy(pimc_context *ctx) {
   cudaFree(ctx->d_dulong_k);
   cudaFree(ctx->d_gofr);
   cudaFree(ctx->d_kvec);
+  cudaFree(ctx->d_nbr_cb);
+  cudaFree(ctx->d_nbr_cnt);
+  cudaFree(ctx->d_nbr_idx);
+  cudaFree(ctx->d_nbr_dirty);
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
   delete ctx;
   return PIMC_OK;
@@ -426,7 +430,10 @@ int pimc_set_path(pimc_context *ctx, int copy, const double *path) {
     if (copy == PIMC_BOTH || copy == c)
       CK(cudaMemcpyAsync(ctx->d_path[c], path, ctx->path_elems * sizeof(double), cudaMemcpyHostToDevice,
                          ctx->stream));
-  if (copy != PIMC_NEW) ctx->rhok_valid = false;  // the device moves recompute rho_k of the new OLD path
+  if (copy != PIMC_NEW) {
+    ctx->rhok_valid = false;  // the device moves recompute rho_k of the new OLD path
+    if (ctx->d_nbr_dirty) CK(cudaMemsetAsync(ctx->d_nbr_dirty, 0xff, sizeof(int), ctx->stream));  // and the lists
+  }
   CK(cudaStreamSynchronize(ctx->stream));
   return PIMC_OK;
 }
@@ -618,6 +625,26 @@ int pimc_bisection_setup(pimc_context *ctx, const pimc_bisection_desc *d) {
       return fail(ctx, PIMC_E_ARG, "long range in device moves needs the Coulomb action's breakup (pimc_longrange_coulomb)");
   }
   if (int rc2 = pa_levels_ok(ctx, d->num_levels)) return rc2;
+  if (d->neighbor_skin < 0.0 || d->neighbor_max < 0) return fail(ctx, PIMC_E_ARG, "bad neighbour-list settings");
+  if (d->neighbor_skin > 0.0) {
+    if (ctx->pa.kind != PA_DAVID) return fail(ctx, PIMC_E_ARG, "neighbour lists need a DavidPA table");
+    if (ctx->sys.N > 65536) return fail(ctx, PIMC_E_ARG, "neighbour lists support up to 65536 particles");
+    CK(cudaSetDevice(ctx->device));
+    const int kmax = d->neighbor_max ? std::min(d->neighbor_max, ctx->sys.N) : std::min(1024, ctx->sys.N);
+    cudaFree(ctx->d_nbr_cb);
+    cudaFree(ctx->d_nbr_cnt);
+    cudaFree(ctx->d_nbr_idx);
+    cudaFree(ctx->d_nbr_dirty);
+    ctx->d_nbr_cb = nullptr;
+    ctx->d_nbr_cnt = ctx->d_nbr_idx = ctx->d_nbr_dirty = nullptr;
+    CK(cudaMalloc(&ctx->d_nbr_cb, (size_t)ctx->sys.N * sizeof(double4)));
+    CK(cudaMalloc(&ctx->d_nbr_cnt, (size_t)ctx->sys.N * sizeof(int)));
+    CK(cudaMalloc(&ctx->d_nbr_idx, (size_t)ctx->sys.N * kmax * sizeof(int)));
+    CK(cudaMalloc(&ctx->d_nbr_dirty, sizeof(int)));
+    CK(cudaMemset(ctx->d_nbr_dirty, 0xff, sizeof(int)));
+    ctx->nbr_kmax = kmax;
+    ctx->nbr_range = ctx->pa.d64.grid.end;  // the table is zero from its last point on
+  }
   CK(cudaSetDevice(ctx->device));
   ctx->bis = *d;
   if (ctx->bis.cluster_ctas == 0) ctx->bis.cluster_ctas = ctx->sys.N >= 256 ? 8 : 1;
@@ -684,12 +711,25 @@ static int run_bisection(pimc_context *ctx, int n_blocks, pimc_move_record *devi
   a.kvec = ctx->d_kvec;
   a.ulong_k0 = ctx->d_ulong_k;  // level 0 row
   a.nk = ctx->num_k;
+  a.nbr_on = ctx->bis.neighbor_skin > 0.0 ? 1 : 0;
+  a.nbr_kmax = ctx->nbr_kmax;
+  a.nbr_cb = ctx->d_nbr_cb;
+  a.nbr_cnt = ctx->d_nbr_cnt;
+  a.nbr_idx = ctx->d_nbr_idx;
+  a.nbr_dirty = ctx->d_nbr_dirty;
   if (a.use_lr && !ctx->rhok_valid) {  // PathClass::UpdateRho_ks() of the current OLD path
     CK(launch_rhok_full(ctx->stream, ctx->d_path[0], ctx->sys.N, ctx->sys.S, lr_desc(ctx), ctx->d_rhok[0]));
     ctx->rhok_valid = true;
   }
   const int cl = ctx->bis.cluster_ctas, thr = ctx->bis.threads_per_cta;
+  auto rebuild = [&]() {  // no-op unless a move or set_path marked the lists stale
+    return a.nbr_on ? launch_nbr_rebuild(ctx->stream, ctx->d_path[0], ctx->sys, ctx->nbr_range,
+                                         ctx->bis.neighbor_skin, ctx->nbr_kmax, ctx->d_nbr_cb, ctx->d_nbr_cnt,
+                                         ctx->d_nbr_idx, ctx->d_nbr_dirty)
+                    : cudaSuccess;
+  };
   if (!a.concurrent) {
+    CK(rebuild());
     CK(launch_bisection(a, ctx->bis.precision, ctx->bis.shadow, cl, 1, thr, ctx->stream));
     return PIMC_OK;
   }
@@ -697,6 +737,7 @@ static int run_bisection(pimc_context *ctx, int n_blocks, pimc_move_record *devi
   for (int r = 0; r < n_blocks; r++) {
     a.round = ctx->rounds + r;
     a.trace_offset = (long long)r * W * ctx->bis.steps_per_block;
+    CK(rebuild());
     CK(launch_bisection(a, ctx->bis.precision, ctx->bis.shadow, cl, W, thr, ctx->stream));
   }
   ctx->rounds += n_blocks;

@@ -190,6 +190,11 @@ struct pimc_context {
   int3 *d_kidx = nullptr;
   double2 *d_rhok[2] = {nullptr, nullptr};
   double *d_kvec = nullptr;  // [k][3] for the device moves
+  // neighbour lists of the device moves
+  double4 *d_nbr_cb = nullptr;
+  int *d_nbr_cnt = nullptr, *d_nbr_idx = nullptr, *d_nbr_dirty = nullptr;
+  int nbr_kmax = 0;
+  double nbr_range = 0.0;
   bool rhok_valid = false;   // d_rhok[OLD] holds rho_k of the OLD path
   bool lr_ready = false;
   int lr_levels = 0, use_background = 0;

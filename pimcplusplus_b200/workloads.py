@@ -139,7 +139,9 @@ def make_dm_for(cfg, directory, r_min=1.5):
     rc = cfg.get("rcut")
     pot = (lambda r: lj_truncated(r, rc)) if rc else lj
     path = os.path.join(directory, f"lj_{cfg['N']}_{cfg['M']}.dm")
-    write_primitive_dm(path, r_min, box[0] / 2.0, cfg["npts"], tau, cfg["levels"] + 1, pot)
+    # a truncated table ends at its cutoff: the reader zeroes the last row, so
+    # every pair at or beyond rc contributes exactly zero
+    write_primitive_dm(path, r_min, rc if rc else box[0] / 2.0, cfg["npts"], tau, cfg["levels"] + 1, pot)
     return path
 
 

@@ -344,3 +344,56 @@ def test_bisection_trace_level5_truncated_lj(tmp_path, schedule):
         acc += r.accepted
     assert 0 < acc < len(live)
     assert np.max(np.abs(d.get_path(P.OLDMODE) - o.get_path(0))) < 1e-9
+
+
+@pytest.mark.parametrize("schedule,skin,cluster", [("sequential", 3.0, 4), ("windows", 3.0, 2), ("sequential", 0.02, 1),
+                                                   ("windows", 0.02, 2)])
+def test_bisection_neighbor_lists_match_all_partner_oracle(tmp_path, schedule, skin, cluster):
+    """Neighbour lists (bounding spheres of each particle's path + skin) give
+    the all-partner sums of the oracle: the truncated table is zero beyond its
+    end.  A tiny skin makes moves leave their spheres, exercising the
+    all-partner fallback and the rebuild between launches."""
+    cfg = dict(W.CONFIGS["C5"])
+    cfg.update(N=256, M=128)
+    tau, box = W.derived(cfg)
+    dm = W.make_dm_for(cfg, str(tmp_path))
+    n, slices, L = cfg["N"], cfg["M"] + 1, cfg["levels"]
+    o = O.System(n, slices, box, tau, W.HE4_LAMBDA, 0)
+    o.set_pa(O.PairAction.from_dm(dm, tau, 0))
+    start = W.lattice_path(n, slices, box, np.random.default_rng(61))
+    o.set_path(start, 0)
+    o.set_path(start, 1)
+    d = P.PathData(n, slices, box, tau, W.HE4_LAMBDA, 0)
+    d.set_path(start)
+    d.pa_david_from_dm(dm, 0)
+    o.bisection_config(L, 4)
+    o.rng_seed(83)
+    kw = dict(cluster_ctas=cluster, threads_per_cta=256, neighbor_skin=skin)
+    if schedule == "sequential":
+        ref = list(o.run_bisection(30)) + list(o.run_bisection(30))
+        bb = P.BisectionBlock(d, L, 4, **kw)
+        bb.seed(83)
+        g1, _ = bb.MakeMoves(30)
+        g2, stats = bb.MakeMoves(30)
+    else:
+        ref = list(o.run_windows(8)) + list(o.run_windows(8))
+        bb = P.BisectionBlock(d, L, 4, schedule=P.WINDOWS, **kw)
+        bb.seed(83)
+        g1, _ = bb.MakeMoves(8)
+        g2, stats = bb.MakeMoves(8)
+    got = np.concatenate([g1, g2])
+    live = [(r, g) for r, g in zip(ref, got) if r.slice1 >= 0]
+    acc = 0
+    for i, (r, g) in enumerate(live):
+        assert (r.slice1, r.ptcl, r.accepted, r.stages_passed) == (
+            int(g["slice1"]), int(g["ptcl"]), int(g["accepted"]), int(g["stages_passed"])), i
+        for k in range(8):
+            assert abs(r.dS[k] - g["dS"][k]) <= 1e-9 * max(1.0, abs(r.dS[k])), (i, k, r.dS[k], g["dS"][k])
+        acc += r.accepted
+    assert acc > 5
+    assert np.max(np.abs(d.get_path(P.OLDMODE) - o.get_path(0))) < 1e-9
+    # with a skin above the moves' excursions the lists cut the pair evaluations
+    full = sum(2 * (n - 1) * sum((1 << L) >> lv for lv in range(L - 1, L - 2 - r.stages_passed, -1) if lv >= 0)
+               for r, _ in live)
+    if skin >= 1.0:
+        assert stats["pair_evals"] < 0.8 * full, (stats["pair_evals"], full)
