@@ -351,6 +351,7 @@ def run_ours(args):
 
     c3 = None if args.no_c3 else run_c3(args, P, torch, flush, local, rank, world, agg)
     c4 = None if args.no_c4 else run_c4(args, P, torch, flush, local, rank, world, agg)
+    c5 = None if args.no_c5 else run_c5(args, P, torch, flush, local, rank, world, agg)
     clocks = sampler.stop() if sampler else None
     if clocks:
         clocks["window"] = "all timed legs (C2 FP64, mixed, other schedule, accuracy, e2e, C3)"
@@ -409,6 +410,9 @@ def run_ours(args):
         if c4:
             line["c4"] = c4
             line["gpu_launches"] += c4.pop("_launches")
+        if c5:
+            line["c5"] = c5
+            line["gpu_launches"] += c5.pop("_launches")
         if cpu:
             line["cpu_baseline"] = {"value": cpu["value"], "unit": UNIT, "cores": cpu["cores"], "kind": "port",
                                     "sample": cpu["sample"]}
@@ -629,6 +633,82 @@ def run_c4(args, P, torch, flush, local, rank, world, agg):
     }
 
 
+def run_c5(args, P, torch, flush, local, rank, world, agg):
+    """C5: one large chain, 4096 LJ He-4 at 0.02186 A^-3, T = 1 K, M = 256,
+    LJ truncated and shifted to zero at 2.5 sigma (table to the cutoff),
+    bisection level 5, concurrent windows, neighbour lists (skin 2.5 A)
+    against the all-partner sum, mixed and FP64."""
+    import tempfile
+
+    from pimcplusplus_b200 import workloads as W
+
+    cfg = dict(W.CONFIGS["C5"])
+    tau, box = W.derived(cfg)
+    n, m, L = cfg["N"], cfg["M"], cfg["levels"]
+    dm = W.make_dm_for(cfg, tempfile.mkdtemp())
+    spb = 16
+    start = W.lattice_path(n, m + 1, box, np.random.default_rng(5 + rank))
+
+    def make(precision, skin, path):
+        d = P.PathData(n, m + 1, box, tau, W.HE4_LAMBDA, 0, device=local)
+        d.pa_david_from_dm(dm, 0)
+        d.set_path(path)
+        bb = P.BisectionBlock(d, L, spb, precision=precision, cluster_ctas=args.c5_cluster, threads_per_cta=512,
+                              schedule=P.WINDOWS, neighbor_skin=skin)
+        bb.seed(900 + rank)
+        return d, bb
+
+    # a short all-partner run gives the path its quantum spread first (untimed)
+    d, bb = make(P.MIXED, 0.0, start)
+    bb.MakeMoves(args.c5_equil, trace=False)
+    eq = d.get_path(P.OLDMODE)
+    d.close()
+    rounds = args.c5_rounds
+
+    def timed(precision, skin):
+        d, bb = make(precision, skin, eq)
+        stream = torch.cuda.ExternalStream(P.lib().pimc_stream(d.h), device=f"cuda:{local}")
+        for _ in range(args.warmup):
+            bb.launch_async(rounds)
+        d.synchronize()
+        s0 = bb.stats()
+        times = []
+        for _ in range(args.steps):
+            with torch.cuda.stream(stream):
+                flush.zero_()
+                e0 = torch.cuda.Event(enable_timing=True)
+                e1 = torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                bb.launch_async(rounds)
+                e1.record(stream)
+            e1.synchronize()
+            times.append(e0.elapsed_time(e1))
+        s1 = bb.stats()
+        if s1["status"]:
+            raise RuntimeError(f"C5 device status {s1['status']}")
+        d.close()
+        st = {k: s1[k] - s0[k] for k in ("moves", "accepted", "pair_evals", "stages_attempted")}
+        ms, st = agg(float(np.sum(times)), st)
+        s = ms / 1000.0
+        return {"pair_evals_per_s": st["pair_evals"] / s, "moves_per_s": st["moves"] / s,
+                "accepted_moves_per_s": st["accepted"] / s, "pair_evals_per_move": st["pair_evals"] / st["moves"],
+                "ms_per_step": ms / args.steps}
+
+    lists32 = timed(P.MIXED, args.c5_skin)
+    lists64 = timed(P.FP64, args.c5_skin)
+    plain32 = timed(P.MIXED, 0.0)
+    return {
+        "workload": f"{n} LJ He-4, rho 0.02186/A^3, T=1 K, M={m}, LJ truncated/shifted at 2.5 sigma, level {L}, "
+                    f"{m >> L} concurrent windows x {args.c5_cluster}-CTA clusters, {spb * rounds} moves per "
+                    f"window per step",
+        "neighbor_lists_mixed": lists32, "neighbor_lists_fp64": lists64, "all_partners_mixed": plain32,
+        "lists_over_all_partners": lists32["accepted_moves_per_s"] / plain32["accepted_moves_per_s"],
+        "mixed_over_fp64": lists32["accepted_moves_per_s"] / lists64["accepted_moves_per_s"],
+        "skin": args.c5_skin,
+        "_launches": 3 * args.steps * rounds,
+    }
+
+
 def nb_launches(schedule, blocks):
     """Bisection-kernel launches per timed step (FP64 + mixed counted by the caller)."""
     return blocks if schedule == "windows" else 1
@@ -650,6 +730,11 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-c3", action="store_true")
     ap.add_argument("--no-c4", action="store_true")
+    ap.add_argument("--no-c5", action="store_true")
+    ap.add_argument("--c5-cluster", type=int, default=16)
+    ap.add_argument("--c5-skin", type=float, default=2.5)
+    ap.add_argument("--c5-rounds", type=int, default=4)
+    ap.add_argument("--c5-equil", type=int, default=60)
     ap.add_argument("--c4-cluster", type=int, default=8)
     ap.add_argument("--c3-chains", type=int, default=1024)
     ap.add_argument("--c3-blocks", type=int, default=4)
