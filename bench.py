@@ -140,8 +140,11 @@ def _pair_evals_of(records, n, levels):
     return total
 
 
-def _cpu_worker(args):
-    seed, seconds, nq, ny, nt = args
+_WORKER = {}
+
+
+def _cpu_init(seed, nq, ny, nt):
+    """One oracle chain per worker process, built once (C2 tables, FP64)."""
     import oracle as O
     cfg, tau, box, tabs = c2_setup(nq, ny, nt)
     qg, yg, tg, umat, dumat, pg, pot = tabs
@@ -149,10 +152,16 @@ def _cpu_worker(args):
     s = O.System(n, slices, box, tau, 6.0596, 0)
     pa = O.PairAction.tricubic(qg, yg, tg, tau, umat, dumat, pg, pot)
     s.set_pa(pa)
+    seed = seed + os.getpid() % 1000
     s.set_path(initial_path(n, slices, box, seed, 0.45 * 2.556))
     s.bisection_config(L, 1)
     s.rng_seed(seed)
     s.run_bisection(20)  # warm-up
+    _WORKER.update(s=s, pa=pa, n=n, L=L)
+
+
+def _cpu_run(seconds):
+    s, n, L = _WORKER["s"], _WORKER["n"], _WORKER["L"]
     evals = moves = acc = 0
     t0 = time.perf_counter()
     while time.perf_counter() - t0 < seconds:
@@ -160,40 +169,76 @@ def _cpu_worker(args):
         evals += _pair_evals_of(recs, n, L)
         moves += len(recs)
         acc += sum(r.accepted for r in recs)
-    dt = time.perf_counter() - t0
-    return evals, moves, acc, dt
+    return evals, moves, acc, time.perf_counter() - t0
+
+
+def cpu_workers(cores):
+    """Worker count: the host cores, capped by memory (each chain holds ~0.4 GB of
+    FP64 tables and buffers) and at 64."""
+    try:
+        import psutil
+        avail = psutil.virtual_memory().available
+        cores = min(cores, max(1, int(avail * 0.5 // (600 << 20))))
+    except Exception:
+        cores = min(cores, 8)
+    return max(1, min(cores, 64))
+
+
+class CpuChains:
+    """The oracle on `cores` host cores, one chain per core (clone parallelism)."""
+
+    def __init__(self, cores):
+        import oracle as O
+        O.build()
+        self.cores = cores
+        self.pool = None
+        if cores == 1:
+            _cpu_init(1000, 200, 50, 50)
+        else:
+            ctx = mp.get_context("spawn")
+            self.pool = ctx.Pool(cores, initializer=_cpu_init, initargs=(1000, 200, 50, 50))
+
+    def sample(self, seconds):
+        if self.pool is None:
+            res = [_cpu_run(seconds)]
+        else:
+            res = self.pool.map(_cpu_run, [seconds] * self.cores, chunksize=1)
+        evals = sum(r[0] for r in res)
+        moves = sum(r[1] for r in res)
+        acc = sum(r[2] for r in res)
+        dt = max(r[3] for r in res)
+        return dict(value=evals / dt, moves_per_s=moves / dt, accepted_per_s=acc / dt, cores=self.cores,
+                    sample=f"{moves} moves of C2 (FP64 oracle, {self.cores} independent chain(s), {dt:.1f} s)")
+
+    def close(self):
+        if self.pool is not None:
+            self.pool.close()
+            self.pool.join()
 
 
 def cpu_baseline(cores, seconds):
-    import oracle as O
-    O.build()
-    if cores == 1:
-        res = [_cpu_worker((1000, seconds, 200, 50, 50))]
-    else:
-        ctx = mp.get_context("spawn")
-        with ctx.Pool(cores) as pool:
-            res = pool.map(_cpu_worker, [(1000 + i, seconds, 200, 50, 50) for i in range(cores)])
-    evals = sum(r[0] for r in res)
-    moves = sum(r[1] for r in res)
-    acc = sum(r[2] for r in res)
-    dt = max(r[3] for r in res)
-    return dict(value=evals / dt, moves_per_s=moves / dt, accepted_per_s=acc / dt, cores=cores,
-                sample=f"{moves} moves of C2 (FP64 oracle, {cores} independent chain(s), {dt:.1f} s)")
+    c = CpuChains(cores)
+    try:
+        return c.sample(seconds)
+    finally:
+        c.close()
 
 
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    cores = os.cpu_count() or 1
+    cores = cpu_workers(os.cpu_count() or 1)
     seconds = max(2.0, min(20.0, 60.0 / max(1, args.steps + args.warmup)))
+    chains = CpuChains(cores)
     for _ in range(args.warmup):
-        cpu_baseline(cores, 1.0)
+        chains.sample(1.0)
     vals = []
     last = None
     for _ in range(args.steps):
-        last = cpu_baseline(cores, seconds)
+        last = chains.sample(seconds)
         vals.append(last["value"])
+    chains.close()
     value = float(np.mean(vals))
     cfg, tau, box, _ = c2_setup(8, 4, 4)
     line = {
@@ -216,6 +261,24 @@ W_NAME = "C2: 512 LJ He-4, rho 0.02186/A^3, T=1.5 K, M=128, PAtricubicFit 200x50
 # ---------------------------------------------------------------------------
 # GPU arm
 # ---------------------------------------------------------------------------
+COUNTERS = ("pair_evals", "moves", "accepted", "stages_attempted")
+
+
+def aggregate_ranks(ms, st, dist, device):
+    """Replicas: the job's time is the slowest rank's, its work the sum of the
+    ranks' counters (one all-reduce each; every rank calls this in the same
+    order)."""
+    if not dist:
+        return ms, st
+    import torch
+    t = torch.tensor([ms], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    keys = [k for k in COUNTERS if k in st]
+    v = torch.tensor([float(st[k]) for k in keys], dtype=torch.float64, device=device)
+    dist.all_reduce(v)
+    return float(t.item()), {k: int(round(float(x))) for k, x in zip(keys, v.tolist())}
+
+
 def run_ours(args):
     import torch
     rank = int(os.environ.get("RANK", "0"))
@@ -291,15 +354,7 @@ def run_ours(args):
         return ms, st
 
     def agg(ms, st):
-        if not dist:
-            return ms, st
-        t = torch.tensor([ms], dtype=torch.float64, device=f"cuda:{local}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        v = torch.tensor([st["pair_evals"], st["moves"], st["accepted"]], dtype=torch.float64,
-                         device=f"cuda:{local}")
-        dist.all_reduce(v)
-        return float(t.item()), dict(pair_evals=int(v[0].item()), moves=int(v[1].item()),
-                                     accepted=int(v[2].item()))
+        return aggregate_ranks(ms, st, dist, f"cuda:{local}")
 
     # nvidia-smi samples every 200 ms, so the clocks are sampled over all the
     # timed legs together (C2 FP64 and mixed, the other schedule, C3)
