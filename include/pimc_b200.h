@@ -167,9 +167,16 @@ int pimc_get_rhok(pimc_context *ctx, int copy, double *out /* [slices][num_k][2]
  * window start drawn from the Local stream (ChooseTimeSlices).  WINDOWS runs
  * one round per block: a Common-stream offset o in [0, 2^L) and concurrent
  * BisectionBlocks on the disjoint windows [o + w 2^L, o + (w+1) 2^L], each
- * with its own Local stream (PIMC++'s time-slice parallelism on one GPU). */
+ * with its own Local stream (PIMC++'s time-slice parallelism on one GPU).
+ * PROPOSALS is WINDOWS with P = cluster_ctas concurrent moved-particle
+ * proposals per window: every step of a window is slots 0..P-1 each making
+ * one move from its own Local stream, with the result of making them one
+ * after another in slot order (a slot whose move read a particle that an
+ * earlier slot's accepted move changed is made again).  Short range only
+ * (use_longrange 0); with neighbour lists most slots are independent. */
 #define PIMC_SCHEDULE_SEQUENTIAL 0
 #define PIMC_SCHEDULE_WINDOWS 1
+#define PIMC_SCHEDULE_PROPOSALS 2
 
 typedef struct pimc_bisection_desc {
   int num_levels;                   /* Move{NumLevels} */
@@ -178,9 +185,10 @@ typedef struct pimc_bisection_desc {
   int use_longrange;                /* LongRange pushed at the lowest level */
   int precision;                    /* PIMC_FP64 or PIMC_MIXED */
   int shadow;                       /* also evaluate the other precision, for dS error */
-  int cluster_ctas;                 /* CTAs cooperating on one chain (1..16), 0 = auto */
+  int cluster_ctas;                 /* CTAs cooperating on one chain (1..16), 0 = auto;
+                                       PROPOSALS: proposal slots per window (2..16), one CTA each */
   int threads_per_cta;              /* 0 = auto */
-  int schedule;                     /* PIMC_SCHEDULE_SEQUENTIAL or PIMC_SCHEDULE_WINDOWS */
+  int schedule;                     /* PIMC_SCHEDULE_SEQUENTIAL, _WINDOWS or _PROPOSALS */
   /* Neighbour lists for the short-range sum (the role of ShortRangeOnClass's
    * cells, Actions/ShortRangeOnClass.cc:35-240), DavidPA only: > 0 turns
    * them on with this skin (length units of the box) around each particle's
@@ -209,18 +217,22 @@ typedef struct pimc_bisection_stats {
   int64_t flips;          /* shadow mode: stage decisions the other precision would flip */
   int32_t status;         /* device status word: 0, PIMC_E_NAN, PIMC_E_STAGING, PIMC_E_CAP */
   int32_t pad;
+  int64_t redone;         /* PROPOSALS: moves discarded and made again (not in moves) */
 } pimc_bisection_stats;
 
 int pimc_bisection_setup(pimc_context *ctx, const pimc_bisection_desc *desc);
 /* Seeds the chain's streams (Philox-4x32-10 key; counters reset): the Local
  * stream of the sequential schedule and the per-window streams. */
 int pimc_rng_seed(pimc_context *ctx, uint64_t seed);
-/* Window slots per round of the WINDOWS schedule: floor((slices-1) / 2^L). */
+/* Window slots per round of the WINDOWS and PROPOSALS schedules:
+ * min(floor((slices-1) / 2^L), 64). */
 int pimc_bisection_windows(pimc_context *ctx, int *windows);
 /* Runs n_blocks BisectionBlocks on the device (OLD copy is the state; NEW is
  * brought back in sync afterwards).  SEQUENTIAL: n_blocks*steps_per_block
  * moves.  WINDOWS: n_blocks rounds of windows*steps_per_block moves; the
  * trace slots of windows that do not fit a round have slice1 = -1.
+ * PROPOSALS: n_blocks rounds of windows*steps_per_block*P moves, records
+ * [round][window][step][slot].
  * trace: that many records or NULL.  stats: accumulated since setup. */
 int pimc_run_bisection(pimc_context *ctx, int n_blocks, pimc_move_record *trace,
                        pimc_bisection_stats *stats);

@@ -92,6 +92,7 @@ def lib():
         "oracle_energy": (None, [p, C.POINTER(d)]),
         "oracle_gofr_accumulate": (None, [p, d, d, i, C.POINTER(u64)]),
         "oracle_run_windows": (i, [p, i, C.POINTER(MoveRecord)]),
+        "oracle_run_proposals": (i, [p, i, i, C.POINTER(MoveRecord)]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
@@ -327,6 +328,15 @@ class System:
         w = min((self.S - 1) >> self.num_levels, 64)
         recs = (MoveRecord * (n_rounds * w * self.steps_per_block))()
         lib().oracle_run_windows(self.h, n_rounds, recs)
+        return recs
+
+    def run_proposals(self, n_rounds, proposals):
+        """Concurrent windows with `proposals` slots per window, replayed in
+        slot order; records [round][window][step][slot]."""
+        w = min((self.S - 1) >> self.num_levels, 64)
+        recs = (MoveRecord * (n_rounds * w * self.steps_per_block * proposals))()
+        if lib().oracle_run_proposals(self.h, n_rounds, proposals, recs) < 0:
+            raise ValueError("proposals must be 1..16")
         return recs
 
     def rng_position(self):

@@ -1257,26 +1257,32 @@ struct OracleSystem {
   // replayed sequentially: round r draws o = floor(Common() * 2^L) at
   // Common-stream index r and runs one block per window [o + w 2^L, ...],
   // window w drawing from its own Local stream.  The windows commute, so the
-  // order here is immaterial.
-  void MakeRound(OracleMoveRecord *recs) {
+  // order here is immaterial.  With P proposal slots per window
+  // (PIMC_SCHEDULE_PROPOSALS) every step of a window is slot 0, 1, ..., P-1
+  // making one move each in that order, slot p drawing from Local stream
+  // 0x100 + 64 p + w; records [window][step][slot].
+  void MakeRound(OracleMoveRecord *recs, int P = 1) {
     const int span = 1 << NumLevels;
     const int W = std::min((NumSlices - 1) >> NumLevels, 64);
     const int o = (int)floor(philox_uniform(rng.seed, STREAM_COMMON, rounds) * span);
     rounds++;
     for (int w = 0; w < W; w++) {
-      OracleMoveRecord *r = recs + (size_t)w * StepsPerBlock;
+      OracleMoveRecord *r = recs + (size_t)w * StepsPerBlock * P;
       const int slice1 = o + w * span;
       if (slice1 + span > NumSlices - 1) {
-        for (int st = 0; st < StepsPerBlock; st++) {
+        for (int st = 0; st < StepsPerBlock * P; st++) {
           memset(&r[st], 0, sizeof(OracleMoveRecord));
           r[st].slice1 = -1;
           r[st].ptcl = -1;
         }
         continue;
       }
-      std::swap(rng, wrng[w]);
-      for (int st = 0; st < StepsPerBlock; st++) MakeMove(slice1, slice1 + span, &r[st]);
-      std::swap(rng, wrng[w]);
+      for (int st = 0; st < StepsPerBlock; st++)
+        for (int p = 0; p < P; p++) {
+          std::swap(rng, wrng[(size_t)p * 64 + w]);
+          MakeMove(slice1, slice1 + span, &r[(size_t)st * P + p]);
+          std::swap(rng, wrng[(size_t)p * 64 + w]);
+        }
     }
   }
   void MakeBlock(OracleMoveRecord *recs) {
@@ -1409,8 +1415,8 @@ void oracle_rng_seed(OracleSystem *s, uint64_t seed) {
   s->rng.stream = STREAM_LOCAL;
   s->rng.nlocal = 0;
   s->rng.one_left = false;
-  s->wrng.assign(64, Random());
-  for (int w = 0; w < 64; w++) {
+  s->wrng.assign(64 * 16, Random());  // [slot][window]
+  for (int w = 0; w < 64 * 16; w++) {
     s->wrng[w].seed = seed;
     s->wrng[w].stream = 0x100u + (uint32_t)w;
   }
@@ -1419,6 +1425,13 @@ void oracle_rng_seed(OracleSystem *s, uint64_t seed) {
 int oracle_run_windows(OracleSystem *s, int n_rounds, OracleMoveRecord *records) {
   const int W = std::min((s->NumSlices - 1) >> s->NumLevels, 64);
   for (int r = 0; r < n_rounds; r++) s->MakeRound(records + (size_t)r * W * s->StepsPerBlock);
+  return W;
+}
+int oracle_run_proposals(OracleSystem *s, int n_rounds, int proposals, OracleMoveRecord *records) {
+  const int W = std::min((s->NumSlices - 1) >> s->NumLevels, 64);
+  if (proposals < 1 || proposals > 16) return -1;
+  for (int r = 0; r < n_rounds; r++)
+    s->MakeRound(records + (size_t)r * W * s->StepsPerBlock * proposals, proposals);
   return W;
 }
 int oracle_run_bisection(OracleSystem *s, int n_blocks, OracleMoveRecord *records) {

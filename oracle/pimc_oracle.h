@@ -124,6 +124,10 @@ int oracle_run_bisection(OracleSystem *s, int n_blocks, OracleMoveRecord *record
  * windows*steps_per_block records (slice1 = -1 for a window that does not
  * fit); returns windows = floor((slices-1)/2^L). */
 int oracle_run_windows(OracleSystem *s, int n_rounds, OracleMoveRecord *records);
+/* The same with `proposals` (1..16) slots per window: every step of a window
+ * is slots 0..proposals-1 making one move each, in slot order, slot p from
+ * Local stream 0x100 + 64 p + w; records [round][window][step][slot]. */
+int oracle_run_proposals(OracleSystem *s, int n_rounds, int proposals, OracleMoveRecord *records);
 uint64_t oracle_rng_position(OracleSystem *s);
 /* Ulong / dUlong quintic tables [levels][points][6]; sets UseLongRange. */
 void oracle_set_ulong(OracleSystem *s, int levels, int points, double delta, const double *ulong,

@@ -34,7 +34,7 @@ OLDMODE, NEWMODE, BOTH = 0, 1, 2
 FP64, MIXED = 0, 1
 ACTION_SHORTRANGE, ACTION_KINETIC, ACTION_LONGRANGE = 0, 1, 2
 GRID_LINEAR, GRID_LOG = 0, 1
-SEQUENTIAL, WINDOWS = 0, 1
+SEQUENTIAL, WINDOWS, PROPOSALS = 0, 1, 2
 
 STATUS = {
     0: "ok", 1: "invalid argument", 2: "CUDA error", 3: "non-finite action", 4: "index out of range",
@@ -116,6 +116,7 @@ class BisectionStats(C.Structure):
         ("flips", C.c_int64),
         ("status", C.c_int32),
         ("pad", C.c_int32),
+        ("redone", C.c_int64),
     ]
 
     def as_dict(self):
@@ -447,6 +448,9 @@ class BisectionBlock:
 
     One call of `MakeMoves(n_blocks)` runs n_blocks blocks of StepsPerBlock
     moves each; the Local RNG stream is Philox-4x32-10 keyed by `seed`.
+    schedule WINDOWS: a block is one round of concurrent slice windows;
+    PROPOSALS: a round of windows with `cluster_ctas` concurrent proposal
+    slots each, trace records [round][window][step][slot].
     """
 
     def __init__(self, path_data: PathData, num_levels, steps_per_block=1, shortrange_at_higher_levels=True,
@@ -471,13 +475,16 @@ class BisectionBlock:
         w = C.c_int()
         path_data._check(_lib.pimc_bisection_windows(path_data.h, C.byref(w)), "bisection_windows")
         self.windows = w.value
+        # PROPOSALS: cluster_ctas proposal slots per window (0 = the library's default, 8)
+        self.proposals = (cluster_ctas or 8) if schedule == PROPOSALS else 1
 
     def seed(self, seed):
         self.PathData._check(_lib.pimc_rng_seed(self.PathData.h, C.c_uint64(seed)), "rng_seed")
 
     def MakeMoves(self, n_blocks, trace=True):
         st = BisectionStats()
-        rec = np.zeros(n_blocks * self.windows * self.steps_per_block, dtype=MOVE_RECORD) if trace else None
+        rec = (np.zeros(n_blocks * self.windows * self.steps_per_block * self.proposals, dtype=MOVE_RECORD)
+               if trace else None)
         ptr = rec.ctypes.data_as(_p) if trace else None
         self.PathData._check(_lib.pimc_run_bisection(self.PathData.h, n_blocks, ptr, C.byref(st)), "run_bisection")
         return rec, st.as_dict()

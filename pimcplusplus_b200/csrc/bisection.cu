@@ -419,6 +419,12 @@ struct KernelShared {
   // outside it, and whether this job evaluates all partners from now on
   double4 s_cb, s_next_cb;
   int s_far, s_next_far, s_allpairs;
+  // concurrent proposals: the stream position at the start of this slot's
+  // move (restored when the move is redone), the outcome every slot of the
+  // window published for the in-order commit, and the commit's verdict
+  RngSnap s_rng0;
+  int4 s_pub[kMaxCluster];
+  int s_commit[4];  // first slot to redo, stop, any committed move left its sphere
 };
 
 // Whether any of the window's span+1 NEW positions lies outside the moved
@@ -437,6 +443,23 @@ __device__ __forceinline__ int window_outside(const double (*w)[3], int span, do
     out |= r2 > cb.w * cb.w;
   }
   return __any_sync(0xffffffffu, out);
+}
+
+// Whether particle j is in particle i's neighbour list (ascending, cnt >= 0).
+__device__ __forceinline__ bool in_nbr_list(const BisectionArgs &a, int i, int j) {
+  const int cnt = __ldcg(&a.nbr_cnt[i]);
+  const int *l = a.nbr_idx + (size_t)i * a.nbr_kmax;
+  int lo = 0, hi = cnt;  // search [lo, hi)
+  while (lo < hi) {
+    const int mid = (lo + hi) >> 1;
+    const int v = __ldg(&l[mid]);
+    if (v == j) return true;
+    if (v < j)
+      lo = mid + 1;
+    else
+      hi = mid;
+  }
+  return false;
 }
 
 // Storage of the precomputed stream tables of a CTA: NF parts of kTabFine
@@ -476,7 +499,7 @@ struct Group {
 // The moves of one job — one chain, or one window of a chain — on this CTA
 // (cluster rank `rank` of `CL`).  `phase` is the parity of the table-staging
 // mbarrier `bar`, flipped once per staging.
-template <int KIND, typename R, bool SHADOW, bool OUTLINE>
+template <int KIND, typename R, bool SHADOW, bool OUTLINE, bool PROP = false>
 __device__ void run_job(const BisectionArgs &a, ChainState *cs, int window, unsigned rank, unsigned CL,
                         cg::cluster_group &cluster, const Group &G, unsigned char *dyn, unsigned dyn_cap,
                         KernelShared &S, uint64_t *bar_ptr, unsigned &phase, const RngTab &tab_mem) {
@@ -501,14 +524,21 @@ __device__ void run_job(const BisectionArgs &a, ChainState *cs, int window, unsi
   const int lane = tid & 31, warp = tid >> 5;
   const int nwarps = G.size >> 5;
   const int sampler = nwarps - 1;
-  const int specwarp = nwarps >= 4 ? nwarps - 2 : -1;  // next-move speculator (needs >= 4 warps)
+  // Concurrent proposals: each CTA of the window's cluster is one proposal
+  // slot and evaluates its moves alone (evaluation rank 0 of 1); the cluster
+  // only meets to commit the slots' moves in order.
+  constexpr bool prop = PROP;
+  const unsigned erank = prop ? 0u : rank, ECL = prop ? 1u : CL;
+  // next-move speculator (needs >= 4 warps; not with proposals, whose next
+  // move may start from a window another slot is about to write)
+  const int specwarp = (nwarps >= 4 && !prop) ? nwarps - 2 : -1;
   const int ethreads = (nwarps - (specwarp >= 0 ? 2 : 1)) * 32;  // evaluating threads: warps below the samplers
   const bool evaluator = tid < ethreads;
   const DevSystem &sys = a.sys;
   const int N = sys.N;
   const int L = a.num_levels;
   const int span = 1 << L;
-  const bool lead = (rank == 0 && tid == 0);
+  const bool lead = (erank == 0 && tid == 0);
 
   // ---- stage the diagonal DavidPA columns into shared memory (bulk TMA) ----
   // Each level's column is diag_stride pairs long, padded so every level and
@@ -580,7 +610,7 @@ __device__ void run_job(const BisectionArgs &a, ChainState *cs, int window, unsi
     S.tab = tab_mem;
     S.tab.W = 0;  // filled below
   }
-  unsigned long long moves = 0, accepted = 0, stages = 0, pair_evals = 0, flips = 0;
+  unsigned long long moves = 0, accepted = 0, stages = 0, pair_evals = 0, flips = 0, redone = 0;
   int status = 0;
   double *path = a.path;
   unsigned xc = 0;  // exchange parity counter
@@ -597,7 +627,8 @@ __device__ void run_job(const BisectionArgs &a, ChainState *cs, int window, unsi
           pimc_move_record r = {};
           r.slice1 = -1;
           r.ptcl = -1;
-          a.trace[a.trace_offset + (long long)window * a.steps_per_block + st] = r;
+          const long long at = (long long)window * a.steps_per_block + st;
+          a.trace[a.trace_offset + (prop ? at * a.proposals + rank : at)] = r;
         }
       if (KIND == PA_DAVID && CL > 1) cluster.sync();  // xchg[1] no longer read by peers
       return;
@@ -611,236 +642,266 @@ __device__ void run_job(const BisectionArgs &a, ChainState *cs, int window, unsi
   const int total_moves = (a.concurrent ? 1 : a.n_blocks) * a.steps_per_block;
   int cur = 0;
   bool have_next = false;
+  // Concurrent proposals.  Step `pstep` of the round is slot 0, 1, ..., P-1
+  // of the window each making one move from its own Local stream, with the
+  // result of making them in that order.  A pass runs slots pfirst..P-1 at
+  // once on the positions at the start of the pass; then, in slot order, a
+  // slot's move is kept unless an earlier slot of the pass accepted a move
+  // of a particle the slot's sums read (or of the slot's own particle).  The
+  // first slot that fails this is redone, with the slots after it, in the
+  // next pass from the positions the kept moves wrote and from its stream
+  // position at the start of the move.
+  const int P = prop ? a.proposals : 1;
+  int pstep = 0, pfirst = 0;
 
-  for (int m = 0; m < total_moves; m++) {
-    const int blk = m / a.steps_per_block, step = m - blk * a.steps_per_block;
-    if (!have_next) {
-      // ChooseTimeSlices (BisectionBlock.cc:362-374), ChooseParticle (NoPermuteClass.cc:61-68)
-      if (warp == sampler) {
-        DevRandom rng = rng_from(s_rng, seed, stream, &S.tab);
-        if (!a.concurrent && step == 0) slice1 = rng.LocalInt(numLeft);
-        const int p = rng.LocalInt(N);
-        __syncwarp();
-        if (lane == 0) {
-          s_ctl[0] = slice1;
-          s_ctl[1] = p;
-          rng_store(s_rng, rng);
-        }
-      }
-      G.sync();
-      slice1 = s_ctl[0];
-      const int p = s_ctl[1];
-      for (int rel = tid; rel <= span; rel += G.size) {
-        const double *q = path + ((size_t)(slice1 + rel) * N + p) * 3;
-        for (int i = 0; i < 3; i++) win_old[cur][rel][i] = win_new[cur][rel][i] = __ldcg(q + i);
-      }
-      G.sync();
-      if (warp == sampler) {
-        DevRandom rng = rng_from(s_rng, seed, stream, &S.tab);
-        const double lsr = sample_level<OUTLINE>(win_old[cur], win_new[cur], gbuf[0], L, L - 1, sys, rng, lane);
-        const double lu = rng.LocalLog();
-        int far = 0;
-        double4 cb = make_double4(0.0, 0.0, 0.0, 0.0);
-        if (a.nbr_on) {
-          cb = a.nbr_cb[s_ctl[1]];
-          __syncwarp();
-          far = window_outside(win_new[cur], span, cb, sys, lane);
-        }
-        __syncwarp();
-        if (lane == 0) {
-          s_logsr[L - 1] = lsr;
-          s_logu[L - 1] = lu;
-          rng_store(s_rng, rng);
-          S.s_cb = cb;
-          S.s_far = far;
-        }
-      }
-      G.sync();
-    }
-    slice1 = s_ctl[0];
-    const int ptcl = s_ctl[1];
-    const bool more = m + 1 < total_moves;
-    const bool next_new_block = !a.concurrent && ((m + 1) % a.steps_per_block == 0);
-    double(*w_old)[3] = win_old[cur];
-    double(*w_new)[3] = win_new[cur];
-
-    double prevDS = 0.0, prevDS_s = 0.0;
+  for (int m = 0; prop ? pstep < a.steps_per_block : m < total_moves; m++) {
+    const int blk = prop ? 0 : m / a.steps_per_block, step = prop ? pstep : m - blk * a.steps_per_block;
+    const bool active = !prop || (int)rank >= pfirst;
+    // this move's work: counted at once, or with proposals when the move is kept
+    unsigned long long mv_stages = 0, mv_pairs = 0, mv_flips = 0;
+    unsigned long long &c_stages = PROP ? mv_stages : stages, &c_pairs = PROP ? mv_pairs : pair_evals,
+                       &c_flips = PROP ? mv_flips : flips;
+    int reads_all = 0, reads_list = 0;  // the partner sums read all particles / the neighbour list
     bool acc_all = true;
-    int passed = 0;
     int move_far = 0;  // some stage of this move sampled outside the moved particle's sphere
+    int mptcl = 0;     // the moved particle
     pimc_move_record rec;
-    if (lead) {
-      rec.slice1 = slice1;
-      rec.ptcl = ptcl;
-      for (int i = 0; i < 8; i++) rec.dS[i] = rec.dS_shadow[i] = 0.0;
-    }
-    int si = 0;
-    for (int level = L - 1; level >= 0; level--, si++) {
-      // ---- LocalStageClass::Attempt (StageClass.cc:49-95) ----
-      // Partners: the moved particle's neighbour list while its NEW positions
-      // stay inside its sphere and no earlier move of this job left one;
-      // otherwise all particles (the same sum: pairs beyond the table's end
-      // add exact zeros).
-      const int far = S.s_far;
-      move_far |= far;
-      int np = N - 1;
-      const int *plist = nullptr;
-      if (a.nbr_on && !far && !S.s_allpairs) {
-        const int cnt = __ldcg(&a.nbr_cnt[ptcl]);
-        if (cnt >= 0) {
-          np = cnt;
-          plist = a.nbr_idx + (size_t)ptcl * a.nbr_kmax;
-        }
-      }
-      if (evaluator) {
-        const size_t st = KIND == PA_DAVID ? (size_t)david_of<R>(a.pa).diag_stride : 0;
-        const size_t sts = (KIND == PA_DAVID && SHADOW) ? (size_t)david_of<RS>(a.pa).diag_stride : 0;
-        const double4 v = stage_sums<KIND, R, SHADOW>(a, w_old, w_new, diag_smem ? diag_smem + level * st : nullptr,
-                                                      diag_smem_s ? diag_smem_s + level * sts : nullptr, level,
-                                                      slice1, ptcl, rank, CL, tid, ethreads, plist, np);
-        const double o1 = warp_sum(v.x), n1 = warp_sum(v.y);
-        const double o2 = SHADOW ? warp_sum(v.z) : 0.0, n2 = SHADOW ? warp_sum(v.w) : 0.0;
-        if (lane == 0) {
-          sh_red[warp][0] = o1;
-          sh_red[warp][1] = n1;
-          sh_red[warp][2] = o2;
-          sh_red[warp][3] = n2;
-        }
-      } else {
-        if (warp == sampler && level > 0) {
-          // speculative sampling of the next level (BisectionStage::Sample of stage level-1)
-          DevRandom spec = rng_from(s_rng, seed, stream, &S.tab);
-          const double lsr = sample_level<OUTLINE>(w_old, w_new, gbuf[0], L, level - 1, sys, spec, lane);
-          const double lu = spec.LocalLog();
+    if (active) {
+      if (!have_next) {
+        // ChooseTimeSlices (BisectionBlock.cc:362-374), ChooseParticle (NoPermuteClass.cc:61-68)
+        if (warp == sampler) {
+          DevRandom rng = rng_from(s_rng, seed, stream, &S.tab);
+          if (!a.concurrent && step == 0) slice1 = rng.LocalInt(numLeft);
+          const int p = rng.LocalInt(N);
           __syncwarp();
           if (lane == 0) {
-            s_logsr[level - 1] = lsr;
-            s_logu[level - 1] = lu;
-            rng_store(s_spec1, spec);
+            if (prop) S.s_rng0 = s_rng;
+            s_ctl[0] = slice1;
+            s_ctl[1] = p;
+            rng_store(s_rng, rng);
           }
         }
-        if (warp == specwarp && more) {
-          // speculative start of the next move, as if this move ends here
-          DevRandom spec = rng_from(s_rng, seed, stream, &S.tab);
-          const int ns1 = next_new_block ? spec.LocalInt(numLeft) : slice1;
-          const int np_ = spec.LocalInt(N);
-          double(*wo)[3] = win_old[cur ^ 1];
-          double(*wn)[3] = win_new[cur ^ 1];
-          for (int rel = lane; rel <= span; rel += 32) {
-            const double *q = path + ((size_t)(ns1 + rel) * N + np_) * 3;
-            for (int i = 0; i < 3; i++) wo[rel][i] = wn[rel][i] = __ldcg(q + i);
-          }
-          __syncwarp();
-          const double lsr = sample_level<OUTLINE>(wo, wn, gbuf[1], L, L - 1, sys, spec, lane);
-          const double lu = spec.LocalLog();
+        G.sync();
+        slice1 = s_ctl[0];
+        const int p = s_ctl[1];
+        for (int rel = tid; rel <= span; rel += G.size) {
+          const double *q = path + ((size_t)(slice1 + rel) * N + p) * 3;
+          for (int i = 0; i < 3; i++) win_old[cur][rel][i] = win_new[cur][rel][i] = __ldcg(q + i);
+        }
+        G.sync();
+        if (warp == sampler) {
+          DevRandom rng = rng_from(s_rng, seed, stream, &S.tab);
+          const double lsr = sample_level<OUTLINE>(win_old[cur], win_new[cur], gbuf[0], L, L - 1, sys, rng, lane);
+          const double lu = rng.LocalLog();
           int far = 0;
           double4 cb = make_double4(0.0, 0.0, 0.0, 0.0);
           if (a.nbr_on) {
-            cb = a.nbr_cb[np_];
+            cb = a.nbr_cb[s_ctl[1]];
             __syncwarp();
-            far = window_outside(wn, span, cb, sys, lane);
+            far = window_outside(win_new[cur], span, cb, sys, lane);
           }
           __syncwarp();
           if (lane == 0) {
-            s_next[1] = ns1;
-            s_next[2] = np_;
-            s_next_f[0] = lsr;
-            s_next_f[1] = lu;
-            S.s_next_cb = cb;
-            S.s_next_far = far;
-            rng_store(s_spec2, spec);
+            s_logsr[L - 1] = lsr;
+            s_logu[L - 1] = lu;
+            rng_store(s_rng, rng);
+            S.s_cb = cb;
+            S.s_far = far;
           }
         }
-        if (lane < 4) sh_red[warp][lane] = 0.0;
+        G.sync();
       }
-      // Counted as the reference performs them: OLD + NEW of the stage's links.
-      if (lead && (level == 0 || a.sr_higher)) pair_evals += 2ull * (unsigned long long)np * (span >> level);
-      G.sync();
-      // ---- reduce: warps -> CTA (warp 0) -> cluster (DSMEM, rank order) ----
-      const int par = xc & 1;
-      xc++;
-      if (warp == 0 && lane < 4) {
-        double v = 0.0;
-        for (int w = 0; w < nwarps; w++) v += sh_red[w][lane];
-        if (CL > 1)
-          for (unsigned r = 0; r < CL; r++) cluster.map_shared_rank(&xchg[par][rank][0], r)[lane] = v;
+      slice1 = s_ctl[0];
+      const int ptcl = s_ctl[1];
+      mptcl = ptcl;
+      const bool more = m + 1 < total_moves;
+      const bool next_new_block = !a.concurrent && ((m + 1) % a.steps_per_block == 0);
+      double(*w_old)[3] = win_old[cur];
+      double(*w_new)[3] = win_new[cur];
+
+      double prevDS = 0.0, prevDS_s = 0.0;
+      int passed = 0;
+      if (lead) {
+        rec.slice1 = slice1;
+        rec.ptcl = ptcl;
+        for (int i = 0; i < 8; i++) rec.dS[i] = rec.dS_shadow[i] = 0.0;
+      }
+      int si = 0;
+      for (int level = L - 1; level >= 0; level--, si++) {
+        // ---- LocalStageClass::Attempt (StageClass.cc:49-95) ----
+        // Partners: the moved particle's neighbour list while its NEW positions
+        // stay inside its sphere and no earlier move of this job left one;
+        // otherwise all particles (the same sum: pairs beyond the table's end
+        // add exact zeros).
+        const int far = S.s_far;
+        move_far |= far;
+        int np = N - 1;
+        const int *plist = nullptr;
+        if (a.nbr_on && !far && !S.s_allpairs) {
+          const int cnt = __ldcg(&a.nbr_cnt[ptcl]);
+          if (cnt >= 0) {
+            np = cnt;
+            plist = a.nbr_idx + (size_t)ptcl * a.nbr_kmax;
+          }
+        }
+        if (evaluator) {
+          const size_t st = KIND == PA_DAVID ? (size_t)david_of<R>(a.pa).diag_stride : 0;
+          const size_t sts = (KIND == PA_DAVID && SHADOW) ? (size_t)david_of<RS>(a.pa).diag_stride : 0;
+          const double4 v = stage_sums<KIND, R, SHADOW>(a, w_old, w_new, diag_smem ? diag_smem + level * st : nullptr,
+                                                        diag_smem_s ? diag_smem_s + level * sts : nullptr, level,
+                                                        slice1, ptcl, erank, ECL, tid, ethreads, plist, np);
+          const double o1 = warp_sum(v.x), n1 = warp_sum(v.y);
+          const double o2 = SHADOW ? warp_sum(v.z) : 0.0, n2 = SHADOW ? warp_sum(v.w) : 0.0;
+          if (lane == 0) {
+            sh_red[warp][0] = o1;
+            sh_red[warp][1] = n1;
+            sh_red[warp][2] = o2;
+            sh_red[warp][3] = n2;
+          }
+        } else {
+          if (warp == sampler && level > 0) {
+            // speculative sampling of the next level (BisectionStage::Sample of stage level-1)
+            DevRandom spec = rng_from(s_rng, seed, stream, &S.tab);
+            const double lsr = sample_level<OUTLINE>(w_old, w_new, gbuf[0], L, level - 1, sys, spec, lane);
+            const double lu = spec.LocalLog();
+            __syncwarp();
+            if (lane == 0) {
+              s_logsr[level - 1] = lsr;
+              s_logu[level - 1] = lu;
+              rng_store(s_spec1, spec);
+            }
+          }
+          if (warp == specwarp && more) {
+            // speculative start of the next move, as if this move ends here
+            DevRandom spec = rng_from(s_rng, seed, stream, &S.tab);
+            const int ns1 = next_new_block ? spec.LocalInt(numLeft) : slice1;
+            const int np_ = spec.LocalInt(N);
+            double(*wo)[3] = win_old[cur ^ 1];
+            double(*wn)[3] = win_new[cur ^ 1];
+            for (int rel = lane; rel <= span; rel += 32) {
+              const double *q = path + ((size_t)(ns1 + rel) * N + np_) * 3;
+              for (int i = 0; i < 3; i++) wo[rel][i] = wn[rel][i] = __ldcg(q + i);
+            }
+            __syncwarp();
+            const double lsr = sample_level<OUTLINE>(wo, wn, gbuf[1], L, L - 1, sys, spec, lane);
+            const double lu = spec.LocalLog();
+            int far = 0;
+            double4 cb = make_double4(0.0, 0.0, 0.0, 0.0);
+            if (a.nbr_on) {
+              cb = a.nbr_cb[np_];
+              __syncwarp();
+              far = window_outside(wn, span, cb, sys, lane);
+            }
+            __syncwarp();
+            if (lane == 0) {
+              s_next[1] = ns1;
+              s_next[2] = np_;
+              s_next_f[0] = lsr;
+              s_next_f[1] = lu;
+              S.s_next_cb = cb;
+              S.s_next_far = far;
+              rng_store(s_spec2, spec);
+            }
+          }
+          if (lane < 4) sh_red[warp][lane] = 0.0;
+        }
+        // Counted as the reference performs them: OLD + NEW of the stage's links.
+        if (level == 0 || a.sr_higher) {
+          if (lead) c_pairs += 2ull * (unsigned long long)np * (span >> level);
+          if (PROP) {
+            if (plist)
+              reads_list = 1;
+            else
+              reads_all = 1;
+          }
+        }
+        G.sync();
+        // ---- reduce: warps -> CTA (warp 0) -> cluster (DSMEM, rank order) ----
+        const int par = xc & 1;
+        xc++;
+        if (warp == 0 && lane < 4) {
+          double v = 0.0;
+          for (int w = 0; w < nwarps; w++) v += sh_red[w][lane];
+          if (ECL > 1)
+            for (unsigned r = 0; r < CL; r++) cluster.map_shared_rank(&xchg[par][rank][0], r)[lane] = v;
+          else
+            xchg[par][0][lane] = v;
+        }
+        if (ECL > 1)
+          cluster.sync();
         else
-          xchg[par][0][lane] = v;
-      }
-      if (CL > 1)
-        cluster.sync();
-      else
-        __syncwarp();
-      if (warp == 0) {
-        double v = 0.0;
-        if (lane < 4)
-          for (unsigned r = 0; r < CL; r++) v += xchg[par][r][lane];
-        const double so = __shfl_sync(0xffffffffu, v, 0);
-        const double sn = __shfl_sync(0xffffffffu, v, 1);
-        const double so2 = __shfl_sync(0xffffffffu, v, 2);
-        const double sn2 = __shfl_sync(0xffffffffu, v, 3);
-        // ---- Metropolis test, identical in every CTA ----
-        const double currActionChange = sn - so;
-        const double logsr = s_logsr[level];
-        const double logAcceptProb = logsr - currActionChange + prevDS;
-        const double logu = s_logu[level];
-        bool toAccept = logAcceptProb >= logu;
-        if (toAccept && (fabs(sn) > 1e50 || fabs(so) > 1e50)) {  // StageClass.cc:74-85
-          toAccept = false;
-          status = PIMC_E_STAGING;
-        }
-        if (!isfinite(currActionChange)) status = PIMC_E_NAN;
-        if (SHADOW) {
-          const double dss = sn2 - so2;
-          const bool other = (logsr - dss + prevDS_s) >= logu;
-          if (other != toAccept && lead) flips++;
-          prevDS_s = dss;
-          if (lead && si < 8) rec.dS_shadow[si] = dss;
-        }
-        prevDS = currActionChange;
-        if (lead && si < 8) rec.dS[si] = currActionChange;
-        // commit the stream position the outcome selects
-        const bool ends = !toAccept || level == 0 || status != 0;
-        // neighbour lists: whether the next stage's NEW positions (the level
-        // sampled speculatively into w_new) leave the moved particle's sphere
-        const int far_next = (a.nbr_on && !ends) ? window_outside(w_new, span, S.s_cb, sys, lane) : 0;
-        if (lane == 0) {
-          s_ctl[2] = toAccept ? 1 : 0;
-          s_ctl[3] = status;
-          int nv = 0;
-          if (!ends) {
-            s_rng = s_spec1;
-            S.s_far = far_next;
-          } else if (status == 0 && more && specwarp >= 0 && !(toAccept && s_next[2] == ptcl)) {
-            s_rng = s_spec2;
-            s_ctl[0] = s_next[1];
-            s_ctl[1] = s_next[2];
-            s_logsr[L - 1] = s_next_f[0];
-            s_logu[L - 1] = s_next_f[1];
-            S.s_cb = S.s_next_cb;
-            S.s_far = S.s_next_far;
-            nv = 1;
+          __syncwarp();
+        if (warp == 0) {
+          double v = 0.0;
+          if (lane < 4)
+            for (unsigned r = 0; r < ECL; r++) v += xchg[par][r][lane];
+          const double so = __shfl_sync(0xffffffffu, v, 0);
+          const double sn = __shfl_sync(0xffffffffu, v, 1);
+          const double so2 = __shfl_sync(0xffffffffu, v, 2);
+          const double sn2 = __shfl_sync(0xffffffffu, v, 3);
+          // ---- Metropolis test, identical in every CTA ----
+          const double currActionChange = sn - so;
+          const double logsr = s_logsr[level];
+          const double logAcceptProb = logsr - currActionChange + prevDS;
+          const double logu = s_logu[level];
+          bool toAccept = logAcceptProb >= logu;
+          if (toAccept && (fabs(sn) > 1e50 || fabs(so) > 1e50)) {  // StageClass.cc:74-85
+            toAccept = false;
+            status = PIMC_E_STAGING;
           }
-          s_next[0] = nv;
+          if (!isfinite(currActionChange)) status = PIMC_E_NAN;
+          if (SHADOW) {
+            const double dss = sn2 - so2;
+            const bool other = (logsr - dss + prevDS_s) >= logu;
+            if (other != toAccept && lead) c_flips++;
+            prevDS_s = dss;
+            if (lead && si < 8) rec.dS_shadow[si] = dss;
+          }
+          prevDS = currActionChange;
+          if (lead && si < 8) rec.dS[si] = currActionChange;
+          // commit the stream position the outcome selects
+          const bool ends = !toAccept || level == 0 || status != 0;
+          // neighbour lists: whether the next stage's NEW positions (the level
+          // sampled speculatively into w_new) leave the moved particle's sphere
+          const int far_next = (a.nbr_on && !ends) ? window_outside(w_new, span, S.s_cb, sys, lane) : 0;
+          if (lane == 0) {
+            s_ctl[2] = toAccept ? 1 : 0;
+            s_ctl[3] = status;
+            int nv = 0;
+            if (!ends) {
+              s_rng = s_spec1;
+              S.s_far = far_next;
+            } else if (status == 0 && more && specwarp >= 0 && !(toAccept && s_next[2] == ptcl)) {
+              s_rng = s_spec2;
+              s_ctl[0] = s_next[1];
+              s_ctl[1] = s_next[2];
+              s_logsr[L - 1] = s_next_f[0];
+              s_logu[L - 1] = s_next_f[1];
+              S.s_cb = S.s_next_cb;
+              S.s_far = S.s_next_far;
+              nv = 1;
+            }
+            s_next[0] = nv;
+          }
         }
+        G.sync();
+        if (tid == 0) c_stages++;
+        if (!s_ctl[2] || s_ctl[3]) {
+          acc_all = false;
+          break;
+        }
+        passed++;
       }
-      G.sync();
-      if (tid == 0) stages++;
-      if (!s_ctl[2] || s_ctl[3]) {
-        acc_all = false;
-        break;
+      have_next = s_next[0] != 0;
+      if (lead) {
+        rec.accepted = acc_all ? 1 : 0;
+        rec.stages_passed = passed;
       }
-      passed++;
-    }
-    have_next = s_next[0] != 0;
+    }  // active
     // ---- AcceptCopy (PathClass.cc:797-863); a rejected move left HBM untouched ----
-    if (acc_all && move_far) {
-      // this move left its sphere: the lists no longer bound this job's
-      // positions; all partners from here on, and a rebuild before the next launch
-      if (tid == 0) S.s_allpairs = 1;
-      if (lead) atomicExch(a.nbr_dirty, 1);
-    }
-    if (acc_all) {
+    // The moved particle's window (and, with long range, the window's rho_k)
+    // by this CTA's threads.
+    auto accept_copy = [&](bool write_path) {
       if (a.use_lr) {
         // AcceptCopy of rho_k (PathClass.cc:797-863): the NEW rho_k of the
         // window, recomputed with the arithmetic of the stage sums, from the
@@ -850,41 +911,114 @@ __device__ void run_job(const BisectionArgs &a, ChainState *cs, int window, unsi
         // their update is rounding only).
         const int lo = a.concurrent ? 1 : 0, hi = a.concurrent ? span - 1 : span;
         const int nk = a.nk, total = (hi - lo + 1) * nk;
-        for (int it = (int)rank * G.size + tid; it < total; it += (int)CL * G.size) {
+        for (int it = (int)erank * G.size + tid; it < total; it += (int)ECL * G.size) {
           const int rel = lo + it / nk, k = it - (it / nk) * nk;
           double2 *p2 = &a.rhok[(size_t)(slice1 + rel) * nk + k];
-          const double2 rn = rho_new_k<R>(__ldcg(p2), a.kvec + 3 * k, w_new[rel], w_old[rel]);
+          const double2 rn = rho_new_k<R>(__ldcg(p2), a.kvec + 3 * k, win_new[cur][rel], win_old[cur][rel]);
           __stcg(p2, rn);
         }
       }
-      if (rank == 0)
+      if (write_path)
         for (int rel = tid; rel <= span; rel += G.size) {
-          double v[3] = {w_new[rel][0], w_new[rel][1], w_new[rel][2]};
+          double v[3] = {win_new[cur][rel][0], win_new[cur][rel][1], win_new[cur][rel][2]};
           put_in_box_fast(v, sys);
-          double *q = path + ((size_t)(slice1 + rel) * N + ptcl) * 3;
+          double *q = path + ((size_t)(slice1 + rel) * N + mptcl) * 3;
           q[0] = v[0];
           q[1] = v[1];
           q[2] = v[2];
         }
-      if (CL > 1)
-        cluster.sync();
-      else
-        G.sync();
-    }
-    if (lead) {
+    };
+    auto count_move = [&](long long at) {  // by the lead thread
       moves++;
       if (acc_all) accepted++;
-      if (a.trace) {
-        rec.accepted = acc_all ? 1 : 0;
-        rec.stages_passed = passed;
-        const long long idx = a.concurrent ? a.trace_offset + (long long)window * a.steps_per_block + step
-                                           : a.trace_offset + (long long)blk * a.steps_per_block + step;
-        a.trace[idx] = rec;
+      if (PROP) {
+        stages += mv_stages;
+        pair_evals += mv_pairs;
+        flips += mv_flips;
       }
+      if (a.trace) a.trace[a.trace_offset + at] = rec;
+    };
+    if (!PROP) {
+      if (acc_all && move_far) {
+        // this move left its sphere: the lists no longer bound this job's
+        // positions; all partners from here on, and a rebuild before the next launch
+        if (tid == 0) S.s_allpairs = 1;
+        if (lead) atomicExch(a.nbr_dirty, 1);
+      }
+      if (acc_all) {
+        accept_copy(rank == 0);
+        if (CL > 1)
+          cluster.sync();
+        else
+          G.sync();
+      }
+      if (lead)
+        count_move(a.concurrent ? (long long)window * a.steps_per_block + step
+                                : (long long)blk * a.steps_per_block + step);
+      if (s_ctl[3] != 0) break;
+      if (have_next) cur ^= 1;
+      G.sync();  // every thread has read s_ctl / s_next before the next move rewrites them
+    } else {
+      // ---- in-order commit of the pass ----
+      // Every slot publishes its outcome to every CTA of the window: accepted,
+      // particle, which partners its sums read (bit 0: all, bit 1: its list),
+      // whether it left its sphere (bit 2), status.
+      if (tid == 0) {
+        const int4 pub = active ? make_int4(acc_all ? 1 : 0, mptcl, reads_all | (reads_list << 1) | (move_far << 2),
+                                            s_ctl[3])
+                                : make_int4(0, -1, 0, 0);
+        for (unsigned r = 0; r < CL; r++) cluster.map_shared_rank(&S.s_pub[rank], r)[0] = pub;
+      }
+      cluster.sync();
+      if (warp == 0) {
+        // Slot `lane` is redone if an earlier slot of the pass accepted a move
+        // of its own particle, or of a partner its sums read: any particle
+        // when they read all, a list member, or a particle that left its
+        // sphere (the lists no longer bound it).  Every CTA computes the same.
+        bool redo = false;
+        int4 me = make_int4(0, -1, 0, 0);
+        if (lane >= pfirst && lane < P) me = S.s_pub[lane];
+        for (int q = pfirst; q < lane && q < P && !redo; q++) {
+          const int4 o = S.s_pub[q];
+          if (!o.x) continue;  // a rejected move changed nothing
+          redo = o.y == me.y || (me.z & 1) || ((me.z & 2) && ((o.z & 4) || in_nbr_list(a, me.y, o.y)));
+        }
+        const unsigned bad = __ballot_sync(0xffffffffu, redo);
+        const int nf = bad ? __ffs(bad) - 1 : P;
+        const bool kept = lane >= pfirst && lane < nf;
+        const bool stop = __any_sync(0xffffffffu, me.w != 0);
+        const bool far_acc = __any_sync(0xffffffffu, kept && me.x && (me.z & 4));
+        if (lane == 0) {
+          S.s_commit[0] = nf;
+          S.s_commit[1] = stop ? 1 : 0;
+          S.s_commit[2] = far_acc ? 1 : 0;
+        }
+      }
+      G.sync();
+      const int nf = S.s_commit[0];
+      if (active && (int)rank < nf) {
+        if (acc_all) accept_copy(true);
+        if (lead) count_move(((long long)window * a.steps_per_block + step) * P + rank);
+      } else if (active) {
+        if (tid == 0) {
+          s_rng = S.s_rng0;  // the redo draws from the move's first number again
+          redone++;
+        }
+      }
+      if (S.s_commit[2]) {
+        // a kept move left its sphere: all partners for the rest of the round
+        if (tid == 0) S.s_allpairs = 1;
+        if (rank == 0 && tid == 0) atomicExch(a.nbr_dirty, 1);
+      }
+      cluster.sync();  // kept windows are in HBM; every CTA has read s_pub and s_commit
+      if (nf >= P) {
+        pstep++;
+        pfirst = 0;
+      } else {
+        pfirst = nf;
+      }
+      if (S.s_commit[1]) break;
     }
-    if (s_ctl[3] != 0) break;
-    if (have_next) cur ^= 1;
-    G.sync();  // every thread has read s_ctl / s_next before the next move rewrites them
     // Refill the stream table once less than half of it is ahead of the
     // committed position (the next move's draws, if any, are committed).
     if ((long long)(S.tab.tb + (uint64_t)S.tab.W) - (long long)s_rng.n < (long long)(tab_mem.W >> 1))
@@ -899,6 +1033,7 @@ __device__ void run_job(const BisectionArgs &a, ChainState *cs, int window, unsi
     cs->stages += stages;
     cs->pair_evals += pair_evals;
     cs->flips += flips;
+    cs->redone += redone;
     if (status) cs->status = status;
   }
   if (CL > 1) cluster.sync();
@@ -908,7 +1043,7 @@ __device__ void run_job(const BisectionArgs &a, ChainState *cs, int window, unsi
 // One chain on a thread-block cluster: the sequential schedule (one launch
 // runs n_blocks blocks), or one round of the concurrent-window schedule
 // (cluster w works window w).
-template <int KIND, typename R, bool SHADOW>
+template <int KIND, typename R, bool SHADOW, bool PROP>
 __global__ void __launch_bounds__(512, 1) bisection_kernel(BisectionArgs a) {
   __shared__ KernelShared S;
   __shared__ RngStore<2> store;
@@ -924,12 +1059,12 @@ __global__ void __launch_bounds__(512, 1) bisection_kernel(BisectionArgs a) {
   }
   __syncthreads();
   unsigned phase = 0;
-  ChainState *cs = a.chains + (a.concurrent ? window : 0);
+  ChainState *cs = a.chains + (a.concurrent ? (PROP ? (int)rank * kMaxWindows + window : window) : 0);
   const Group G = {(int)threadIdx.x, (int)blockDim.x, 0u};
   unsigned dyn_size;
   asm("mov.u32 %0, %%dynamic_smem_size;" : "=r"(dyn_size));
   const RngTab tab = store.part<2>(0, 2);
-  run_job<KIND, R, SHADOW, false>(a, cs, window, rank, CL, cluster, G, dyn, dyn_size, S, &s_bar, phase, tab);
+  run_job<KIND, R, SHADOW, false, PROP>(a, cs, window, rank, CL, cluster, G, dyn, dyn_size, S, &s_bar, phase, tab);
 }
 
 // Many independent chains in one persistent launch (the reference's clone
@@ -1010,9 +1145,9 @@ __global__ void __launch_bounds__(512, 1) batch_kernel(BatchArgs b) {
 }
 
 
-template <int KIND, typename R, bool SHADOW>
+template <int KIND, typename R, bool SHADOW, bool PROP = false>
 static cudaError_t launch_t(const BisectionArgs &a, int cl, int clusters, int threads, size_t dyn, cudaStream_t st) {
-  auto kfn = bisection_kernel<KIND, R, SHADOW>;
+  auto kfn = bisection_kernel<KIND, R, SHADOW, PROP>;
   cudaError_t e = cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn);
   if (e != cudaSuccess) return e;
   if (cl > 8) {
@@ -1034,9 +1169,9 @@ static cudaError_t launch_t(const BisectionArgs &a, int cl, int clusters, int th
   return cudaLaunchKernelEx(&cfg, kfn, a);
 }
 
-template <int KIND, typename R, bool SHADOW>
+template <int KIND, typename R, bool SHADOW, bool PROP = false>
 static cudaError_t occupancy_t(int cl, int threads, size_t dyn, int *max_clusters) {
-  auto kfn = bisection_kernel<KIND, R, SHADOW>;
+  auto kfn = bisection_kernel<KIND, R, SHADOW, PROP>;
   cudaError_t e = cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn);
   if (e != cudaSuccess) return e;
   if (cl > 8) {
@@ -1061,6 +1196,13 @@ cudaError_t bisection_occupancy(const BisectionArgs &a, int precision, int shado
                                 int *max_clusters) {
   const size_t dyn = bisection_dyn_smem(a, precision, shadow);
   const bool mixed = precision == PIMC_MIXED;
+  if (a.proposals > 1) {
+    if (a.pa.kind != PA_DAVID) return cudaErrorInvalidValue;
+    if (mixed) return shadow ? occupancy_t<PA_DAVID, float, true, true>(cl, threads, dyn, max_clusters)
+                             : occupancy_t<PA_DAVID, float, false, true>(cl, threads, dyn, max_clusters);
+    return shadow ? occupancy_t<PA_DAVID, double, true, true>(cl, threads, dyn, max_clusters)
+                  : occupancy_t<PA_DAVID, double, false, true>(cl, threads, dyn, max_clusters);
+  }
   if (a.pa.kind == PA_DAVID) {
     if (mixed) return shadow ? occupancy_t<PA_DAVID, float, true>(cl, threads, dyn, max_clusters)
                              : occupancy_t<PA_DAVID, float, false>(cl, threads, dyn, max_clusters);
@@ -1137,6 +1279,13 @@ cudaError_t launch_bisection(const BisectionArgs &a, int precision, int shadow, 
       clusters > kMaxWindows)
     return cudaErrorInvalidValue;
   const bool mixed = precision == PIMC_MIXED;
+  if (a.proposals > 1) {  // concurrent proposals: DavidPA tables (the neighbour lists' action)
+    if (a.pa.kind != PA_DAVID || !a.concurrent || a.use_lr) return cudaErrorInvalidValue;
+    if (mixed) return shadow ? launch_t<PA_DAVID, float, true, true>(a, cl, clusters, threads, dyn, st)
+                             : launch_t<PA_DAVID, float, false, true>(a, cl, clusters, threads, dyn, st);
+    return shadow ? launch_t<PA_DAVID, double, true, true>(a, cl, clusters, threads, dyn, st)
+                  : launch_t<PA_DAVID, double, false, true>(a, cl, clusters, threads, dyn, st);
+  }
   if (a.pa.kind == PA_DAVID) {
     if (mixed) return shadow ? launch_t<PA_DAVID, float, true>(a, cl, clusters, threads, dyn, st)
                              : launch_t<PA_DAVID, float, false>(a, cl, clusters, threads, dyn, st);

@@ -16,6 +16,10 @@ struct BisectionArgs {
   long long trace_offset;
   int num_levels, steps_per_block, n_blocks, sr_higher;
   int concurrent;             // 0: sequential schedule; 1: concurrent windows, one round per launch
+  // Concurrent windows with P > 1 proposal slots per window (DavidPA): the
+  // cluster of a window has P CTAs, CTA p runs slot p from ChainState
+  // p * kMaxWindows + w.  0 or 1: one proposal per window.
+  int proposals;
   unsigned long long round;   // Common-stream index of this round (concurrent)
   // LongRangeClass::SingleAction in the lowest stage (BisectionBlock.cc:92-103):
   // rho_k of the OLD path [slice][k], the k-vectors [k][3] and Ulong_k of level 0

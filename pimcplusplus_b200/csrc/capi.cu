@@ -240,8 +240,8 @@ int pimc_create(const pimc_system_desc *d, pimc_context **out) {
   if (e == cudaSuccess) e = cudaMemset(ctx->d_counter, 0, sizeof(unsigned int));
   if (e == cudaSuccess) e = cudaMalloc(&ctx->d_out, 4 * sizeof(double));
   if (e == cudaSuccess) e = cudaMallocHost(&ctx->h_out, 4 * sizeof(double));
-  if (e == cudaSuccess) e = cudaMalloc(&ctx->d_chain, kMaxWindows * sizeof(ChainState));
-  if (e == cudaSuccess) e = cudaMemset(ctx->d_chain, 0, kMaxWindows * sizeof(ChainState));
+  if (e == cudaSuccess) e = cudaMalloc(&ctx->d_chain, kMaxChainStates * sizeof(ChainState));
+  if (e == cudaSuccess) e = cudaMemset(ctx->d_chain, 0, kMaxChainStates * sizeof(ChainState));
   if (e == cudaSuccess) e = cudaDeviceGetAttribute(&ctx->sm_count, cudaDevAttrMultiProcessorCount, d->device);
   if (e == cudaSuccess) e = cudaMemset(ctx->d_path[0], 0, ctx->path_elems * sizeof(double));
   if (e == cudaSuccess) e = cudaMemset(ctx->d_path[1], 0, ctx->path_elems * sizeof(double));
@@ -613,10 +613,15 @@ int pimc_bisection_setup(pimc_context *ctx, const pimc_bisection_desc *d) {
   if (d->cluster_ctas < 0 || d->cluster_ctas > kMaxCluster) return fail(ctx, PIMC_E_ARG, "cluster_ctas 0..16");
   if (d->threads_per_cta != 0 && (d->threads_per_cta < 64 || d->threads_per_cta > 512 || d->threads_per_cta % 32))
     return fail(ctx, PIMC_E_ARG, "threads_per_cta must be a multiple of 32 in 64..512");
-  if (d->schedule != PIMC_SCHEDULE_SEQUENTIAL && d->schedule != PIMC_SCHEDULE_WINDOWS)
+  if (d->schedule != PIMC_SCHEDULE_SEQUENTIAL && d->schedule != PIMC_SCHEDULE_WINDOWS &&
+      d->schedule != PIMC_SCHEDULE_PROPOSALS)
     return fail(ctx, PIMC_E_ARG, "bad schedule");
-  if (d->schedule == PIMC_SCHEDULE_WINDOWS && window_slots(ctx, d->num_levels) < 1)
+  if (d->schedule != PIMC_SCHEDULE_SEQUENTIAL && window_slots(ctx, d->num_levels) < 1)
     return fail(ctx, PIMC_E_ARG, "no window fits");
+  if (d->schedule == PIMC_SCHEDULE_PROPOSALS && d->use_longrange)
+    return fail(ctx, PIMC_E_ARG, "concurrent proposals are short-range only (every move changes the window's rho_k)");
+  if (d->schedule == PIMC_SCHEDULE_PROPOSALS && ctx->pa.kind != PA_DAVID)
+    return fail(ctx, PIMC_E_ARG, "concurrent proposals need a DavidPA table");
   if (d->use_longrange) {
     // LongRange joins the lowest stage (BisectionBlock.cc:92-103); its short-range
     // counterpart must subtract the same Ulong
@@ -647,12 +652,13 @@ int pimc_bisection_setup(pimc_context *ctx, const pimc_bisection_desc *d) {
   }
   CK(cudaSetDevice(ctx->device));
   ctx->bis = *d;
-  if (ctx->bis.cluster_ctas == 0) ctx->bis.cluster_ctas = ctx->sys.N >= 256 ? 8 : 1;
+  if (ctx->bis.cluster_ctas == 0)
+    ctx->bis.cluster_ctas = (ctx->sys.N >= 256 || d->schedule == PIMC_SCHEDULE_PROPOSALS) ? 8 : 1;
   if (ctx->bis.threads_per_cta == 0) ctx->bis.threads_per_cta = 256;
-  std::vector<ChainState> cs(kMaxWindows);
+  std::vector<ChainState> cs(kMaxChainStates);
   CK(cudaMemcpy(cs.data(), ctx->d_chain, cs.size() * sizeof(ChainState), cudaMemcpyDeviceToHost));
   for (auto &c : cs) {
-    c.moves = c.accepted = c.stages = c.pair_evals = c.flips = 0;
+    c.moves = c.accepted = c.stages = c.pair_evals = c.flips = c.redone = 0;
     c.status = 0;
   }
   CK(cudaMemcpy(ctx->d_chain, cs.data(), cs.size() * sizeof(ChainState), cudaMemcpyHostToDevice));
@@ -663,9 +669,9 @@ int pimc_bisection_setup(pimc_context *ctx, const pimc_bisection_desc *d) {
 int pimc_rng_seed(pimc_context *ctx, uint64_t seed) {
   if (!ctx) return PIMC_E_ARG;
   CK(cudaSetDevice(ctx->device));
-  std::vector<ChainState> cs(kMaxWindows);
+  std::vector<ChainState> cs(kMaxChainStates);
   CK(cudaMemcpy(cs.data(), ctx->d_chain, cs.size() * sizeof(ChainState), cudaMemcpyDeviceToHost));
-  for (int w = 0; w < kMaxWindows; w++) {
+  for (int w = 0; w < kMaxChainStates; w++) {
     cs[w].seed = seed;
     cs[w].nlocal = 0;
     cs[w].stream = w == 0 && ctx->bis.schedule == PIMC_SCHEDULE_SEQUENTIAL ? kStreamLocal : kStreamWindow0 + w;
@@ -674,7 +680,7 @@ int pimc_rng_seed(pimc_context *ctx, uint64_t seed) {
   }
   // stream ids are fixed by the schedule at seeding time; window 0 of the
   // concurrent schedule uses kStreamWindow0, the sequential chain kStreamLocal
-  cs[0].stream = ctx->bis.schedule == PIMC_SCHEDULE_WINDOWS ? kStreamWindow0 : kStreamLocal;
+  cs[0].stream = ctx->bis.schedule == PIMC_SCHEDULE_SEQUENTIAL ? kStreamLocal : kStreamWindow0;
   ctx->rounds = 0;
   CK(cudaMemcpy(ctx->d_chain, cs.data(), cs.size() * sizeof(ChainState), cudaMemcpyHostToDevice));
   return PIMC_OK;
@@ -683,12 +689,13 @@ int pimc_rng_seed(pimc_context *ctx, uint64_t seed) {
 int pimc_bisection_windows(pimc_context *ctx, int *windows) {
   if (!ctx || !windows) return PIMC_E_ARG;
   if (!ctx->bis_ready) return fail(ctx, PIMC_E_STATE, "pimc_bisection_setup not called");
-  *windows = ctx->bis.schedule == PIMC_SCHEDULE_WINDOWS ? window_slots(ctx, ctx->bis.num_levels) : 1;
+  *windows = ctx->bis.schedule != PIMC_SCHEDULE_SEQUENTIAL ? window_slots(ctx, ctx->bis.num_levels) : 1;
   return PIMC_OK;
 }
 
 static size_t records_for(const pimc_context *ctx, int n_blocks) {
-  size_t per = ctx->bis.schedule == PIMC_SCHEDULE_WINDOWS ? (size_t)window_slots(ctx, ctx->bis.num_levels) : 1;
+  size_t per = ctx->bis.schedule != PIMC_SCHEDULE_SEQUENTIAL ? (size_t)window_slots(ctx, ctx->bis.num_levels) : 1;
+  if (ctx->bis.schedule == PIMC_SCHEDULE_PROPOSALS) per *= (size_t)ctx->bis.cluster_ctas;
   return (size_t)n_blocks * per * ctx->bis.steps_per_block;
 }
 
@@ -704,7 +711,8 @@ static int run_bisection(pimc_context *ctx, int n_blocks, pimc_move_record *devi
   a.steps_per_block = ctx->bis.steps_per_block;
   a.n_blocks = n_blocks;
   a.sr_higher = ctx->bis.shortrange_at_higher_levels;
-  a.concurrent = ctx->bis.schedule == PIMC_SCHEDULE_WINDOWS;
+  a.concurrent = ctx->bis.schedule != PIMC_SCHEDULE_SEQUENTIAL;
+  a.proposals = ctx->bis.schedule == PIMC_SCHEDULE_PROPOSALS ? ctx->bis.cluster_ctas : 1;
   a.round = ctx->rounds;
   a.use_lr = ctx->bis.use_longrange ? 1 : 0;
   a.rhok = ctx->d_rhok[0];
@@ -736,7 +744,7 @@ static int run_bisection(pimc_context *ctx, int n_blocks, pimc_move_record *devi
   const int W = window_slots(ctx, ctx->bis.num_levels);
   for (int r = 0; r < n_blocks; r++) {
     a.round = ctx->rounds + r;
-    a.trace_offset = (long long)r * W * ctx->bis.steps_per_block;
+    a.trace_offset = (long long)r * W * ctx->bis.steps_per_block * a.proposals;
     CK(rebuild());
     CK(launch_bisection(a, ctx->bis.precision, ctx->bis.shadow, cl, W, thr, ctx->stream));
   }
@@ -785,7 +793,7 @@ int pimc_run_bisection(pimc_context *ctx, int n_blocks, pimc_move_record *trace,
 int pimc_bisection_get_stats(pimc_context *ctx, pimc_bisection_stats *stats) {
   if (!ctx || !stats) return PIMC_E_ARG;
   CK(cudaSetDevice(ctx->device));
-  std::vector<ChainState> cs(kMaxWindows);
+  std::vector<ChainState> cs(kMaxChainStates);
   CK(cudaMemcpyAsync(cs.data(), ctx->d_chain, cs.size() * sizeof(ChainState), cudaMemcpyDeviceToHost, ctx->stream));
   CK(cudaStreamSynchronize(ctx->stream));
   std::memset(stats, 0, sizeof(*stats));
@@ -795,6 +803,7 @@ int pimc_bisection_get_stats(pimc_context *ctx, pimc_bisection_stats *stats) {
     stats->stages_attempted += (int64_t)c.stages;
     stats->pair_evals += (int64_t)c.pair_evals;
     stats->flips += (int64_t)c.flips;
+    stats->redone += (int64_t)c.redone;
     if (c.status && !stats->status) stats->status = c.status;
   }
   return PIMC_OK;
@@ -807,6 +816,7 @@ int pimc_bisection_occupancy(pimc_context *ctx, int *max_active_clusters) {
   BisectionArgs a{};
   a.pa = ctx->pa;
   a.num_levels = ctx->bis.num_levels;
+  a.proposals = ctx->bis.schedule == PIMC_SCHEDULE_PROPOSALS ? ctx->bis.cluster_ctas : 1;
   CK(bisection_occupancy(a, ctx->bis.precision, ctx->bis.shadow, ctx->bis.cluster_ctas, ctx->bis.threads_per_cta,
                          max_active_clusters));
   return PIMC_OK;

@@ -133,7 +133,10 @@ struct DevSystem {
 
 constexpr int kMaxWindows = 64;      // concurrent slice windows of one chain
 constexpr uint32_t kStreamLocal = 0, kStreamCommon = 1, kStreamWorld = 2;
-constexpr uint32_t kStreamWindow0 = 0x100;  // Local stream of window w is kStreamWindow0 + w
+// Local stream of window w, proposal slot p (slot 0 without proposals) is
+// kStreamWindow0 + p * kMaxWindows + w, in ChainState p * kMaxWindows + w
+constexpr uint32_t kStreamWindow0 = 0x100;
+constexpr int kMaxChainStates = kMaxWindows * kMaxCluster;
 
 // Device state of one Local RNG stream and its move counters: the chain in
 // the sequential schedule, or one slice window in the concurrent schedule.
@@ -146,6 +149,7 @@ struct ChainState {
   int32_t status;
   int32_t pad;
   unsigned long long moves, accepted, stages, pair_evals, flips;
+  unsigned long long redone;  // concurrent proposals: moves discarded and made again
 };
 
 struct DeviceBuffer {
