@@ -692,7 +692,9 @@ def run_c5(args, P, torch, flush, local, rank, world, agg):
     """C5: one large chain, 4096 LJ He-4 at 0.02186 A^-3, T = 1 K, M = 256,
     LJ truncated and shifted to zero at 2.5 sigma (table to the cutoff),
     bisection level 5, concurrent windows, neighbour lists (skin 2.5 A)
-    against the all-partner sum, mixed and FP64."""
+    against the all-partner sum, mixed and FP64; and concurrent
+    moved-particle proposals (P slots per window, one CTA each: 8 windows x
+    8 slots = 64 proposals by default)."""
     import tempfile
 
     from pimcplusplus_b200 import workloads as W
@@ -704,12 +706,16 @@ def run_c5(args, P, torch, flush, local, rank, world, agg):
     spb = 16
     start = W.lattice_path(n, m + 1, box, np.random.default_rng(5 + rank))
 
-    def make(precision, skin, path):
+    def make(precision, skin, path, proposals=0):
         d = P.PathData(n, m + 1, box, tau, W.HE4_LAMBDA, 0, device=local)
         d.pa_david_from_dm(dm, 0)
         d.set_path(path)
-        bb = P.BisectionBlock(d, L, spb, precision=precision, cluster_ctas=args.c5_cluster, threads_per_cta=512,
-                              schedule=P.WINDOWS, neighbor_skin=skin)
+        if proposals:
+            bb = P.BisectionBlock(d, L, spb, precision=precision, cluster_ctas=proposals,
+                                  threads_per_cta=args.c5_prop_threads, schedule=P.PROPOSALS, neighbor_skin=skin)
+        else:
+            bb = P.BisectionBlock(d, L, spb, precision=precision, cluster_ctas=args.c5_cluster, threads_per_cta=512,
+                                  schedule=P.WINDOWS, neighbor_skin=skin)
         bb.seed(900 + rank)
         return d, bb
 
@@ -720,8 +726,8 @@ def run_c5(args, P, torch, flush, local, rank, world, agg):
     d.close()
     rounds = args.c5_rounds
 
-    def timed(precision, skin):
-        d, bb = make(precision, skin, eq)
+    def timed(precision, skin, proposals=0):
+        d, bb = make(precision, skin, eq, proposals)
         stream = torch.cuda.ExternalStream(P.lib().pimc_stream(d.h), device=f"cuda:{local}")
         for _ in range(args.warmup):
             bb.launch_async(rounds)
@@ -742,25 +748,39 @@ def run_c5(args, P, torch, flush, local, rank, world, agg):
         if s1["status"]:
             raise RuntimeError(f"C5 device status {s1['status']}")
         d.close()
-        st = {k: s1[k] - s0[k] for k in ("moves", "accepted", "pair_evals", "stages_attempted")}
+        st = {k: s1[k] - s0[k] for k in ("moves", "accepted", "pair_evals", "stages_attempted", "redone")}
         ms, st = agg(float(np.sum(times)), st)
         s = ms / 1000.0
-        return {"pair_evals_per_s": st["pair_evals"] / s, "moves_per_s": st["moves"] / s,
-                "accepted_moves_per_s": st["accepted"] / s, "pair_evals_per_move": st["pair_evals"] / st["moves"],
-                "ms_per_step": ms / args.steps}
+        out = {"pair_evals_per_s": st["pair_evals"] / s, "moves_per_s": st["moves"] / s,
+               "accepted_moves_per_s": st["accepted"] / s, "pair_evals_per_move": st["pair_evals"] / st["moves"],
+               "ms_per_step": ms / args.steps}
+        if proposals:
+            out["redone_per_move"] = st["redone"] / st["moves"]
+        return out
 
     lists32 = timed(P.MIXED, args.c5_skin)
     lists64 = timed(P.FP64, args.c5_skin)
     plain32 = timed(P.MIXED, 0.0)
+    pp = args.c5_proposals
+    prop32 = timed(P.MIXED, args.c5_skin, pp)
+    prop64 = timed(P.FP64, args.c5_skin, pp)
+    wide32 = timed(P.MIXED, args.c5_skin, args.c5_proposals_wide) if args.c5_proposals_wide else None
     return {
         "workload": f"{n} LJ He-4, rho 0.02186/A^3, T=1 K, M={m}, LJ truncated/shifted at 2.5 sigma, level {L}, "
                     f"{m >> L} concurrent windows x {args.c5_cluster}-CTA clusters, {spb * rounds} moves per "
-                    f"window per step",
+                    f"window per step; proposals: {m >> L} windows x {pp} slots = {(m >> L) * pp} concurrent "
+                    f"moved-particle proposals, {spb * rounds * pp} moves per window per step",
         "neighbor_lists_mixed": lists32, "neighbor_lists_fp64": lists64, "all_partners_mixed": plain32,
+        "proposals_mixed": prop32, "proposals_fp64": prop64,
+        f"proposals_{(m >> L) * args.c5_proposals_wide}_mixed": wide32,
         "lists_over_all_partners": lists32["accepted_moves_per_s"] / plain32["accepted_moves_per_s"],
         "mixed_over_fp64": lists32["accepted_moves_per_s"] / lists64["accepted_moves_per_s"],
-        "skin": args.c5_skin,
-        "_launches": 3 * args.steps * rounds,
+        "proposals_over_one_per_window": prop32["accepted_moves_per_s"] / lists32["accepted_moves_per_s"],
+        "proposals_mixed_over_fp64": prop32["accepted_moves_per_s"] / prop64["accepted_moves_per_s"],
+        "skin": args.c5_skin, "proposals": pp,
+        # per round: one bisection launch per variant, plus the three neighbour
+        # list kernels (bounds, fill, clear) of each variant with lists
+        "_launches": (6 + 5 * 3 if args.c5_proposals_wide else 5 + 4 * 3) * args.steps * rounds,
     }
 
 
@@ -790,6 +810,9 @@ def main():
     ap.add_argument("--c5-skin", type=float, default=2.5)
     ap.add_argument("--c5-rounds", type=int, default=4)
     ap.add_argument("--c5-equil", type=int, default=60)
+    ap.add_argument("--c5-proposals", type=int, default=8)
+    ap.add_argument("--c5-proposals-wide", type=int, default=16, help="a second proposals shape (0: none)")
+    ap.add_argument("--c5-prop-threads", type=int, default=512)
     ap.add_argument("--c4-cluster", type=int, default=8)
     ap.add_argument("--c3-chains", type=int, default=1024)
     ap.add_argument("--c3-blocks", type=int, default=4)

@@ -424,6 +424,7 @@ struct KernelShared {
   // window published for the in-order commit, and the commit's verdict
   RngSnap s_rng0;
   int4 s_pub[kMaxCluster];
+  int s_redo[kMaxCluster], s_redo_local;
   int s_commit[4];  // first slot to redo, stop, any committed move left its sphere
 };
 
@@ -445,21 +446,30 @@ __device__ __forceinline__ int window_outside(const double (*w)[3], int span, do
   return __any_sync(0xffffffffu, out);
 }
 
-// Whether particle j is in particle i's neighbour list (ascending, cnt >= 0).
-__device__ __forceinline__ bool in_nbr_list(const BisectionArgs &a, int i, int j) {
-  const int cnt = __ldcg(&a.nbr_cnt[i]);
-  const int *l = a.nbr_idx + (size_t)i * a.nbr_kmax;
-  int lo = 0, hi = cnt;  // search [lo, hi)
-  while (lo < hi) {
-    const int mid = (lo + hi) >> 1;
-    const int v = __ldg(&l[mid]);
-    if (v == j) return true;
-    if (v < j)
-      lo = mid + 1;
-    else
-      hi = mid;
+// Whether a DavidPA pair term of the windows a and b can be nonzero: some
+// slice of the window where one of a's OLD/NEW positions and one of b's
+// OLD/NEW positions are closer than `range` (minimum image), by one warp.  A
+// DavidPA table is zero from its grid end on, and DistDisp's second distance
+// is never below the minimum image, so beyond it every link term is zero.
+__device__ __forceinline__ bool windows_near(const double (*ao)[3], const double (*an)[3], const double (*bo)[3],
+                                             const double (*bn)[3], int span, double range, const DevSystem &sys,
+                                             int lane) {
+  bool hit = false;
+  const double r2 = range * range;
+  for (int rel = lane; rel <= span; rel += 32) {
+    const double *A[2] = {ao[rel], an[rel]}, *B[2] = {bo[rel], bn[rel]};
+    for (int x = 0; x < 2; x++)
+      for (int y = 0; y < 2; y++) {
+        double d2 = 0.0;
+        for (int i = 0; i < 3; i++) {
+          double d = A[x][i] - B[y][i];
+          d -= rint(d * sys.boxinv[i]) * sys.box[i];
+          d2 += d * d;
+        }
+        hit |= d2 < r2;
+      }
   }
-  return false;
+  return __any_sync(0xffffffffu, hit);
 }
 
 // Storage of the precomputed stream tables of a CTA: NF parts of kTabFine
@@ -661,7 +671,6 @@ __device__ void run_job(const BisectionArgs &a, ChainState *cs, int window, unsi
     unsigned long long mv_stages = 0, mv_pairs = 0, mv_flips = 0;
     unsigned long long &c_stages = PROP ? mv_stages : stages, &c_pairs = PROP ? mv_pairs : pair_evals,
                        &c_flips = PROP ? mv_flips : flips;
-    int reads_all = 0, reads_list = 0;  // the partner sums read all particles / the neighbour list
     bool acc_all = true;
     int move_far = 0;  // some stage of this move sampled outside the moved particle's sphere
     int mptcl = 0;     // the moved particle
@@ -806,15 +815,7 @@ __device__ void run_job(const BisectionArgs &a, ChainState *cs, int window, unsi
           if (lane < 4) sh_red[warp][lane] = 0.0;
         }
         // Counted as the reference performs them: OLD + NEW of the stage's links.
-        if (level == 0 || a.sr_higher) {
-          if (lead) c_pairs += 2ull * (unsigned long long)np * (span >> level);
-          if (PROP) {
-            if (plist)
-              reads_list = 1;
-            else
-              reads_all = 1;
-          }
-        }
+        if (lead && (level == 0 || a.sr_higher)) c_pairs += 2ull * (unsigned long long)np * (span >> level);
         G.sync();
         // ---- reduce: warps -> CTA (warp 0) -> cluster (DSMEM, rank order) ----
         const int par = xc & 1;
@@ -961,33 +962,43 @@ __device__ void run_job(const BisectionArgs &a, ChainState *cs, int window, unsi
     } else {
       // ---- in-order commit of the pass ----
       // Every slot publishes its outcome to every CTA of the window: accepted,
-      // particle, which partners its sums read (bit 0: all, bit 1: its list),
-      // whether it left its sphere (bit 2), status.
+      // particle, whether it left its sphere, status.
       if (tid == 0) {
-        const int4 pub = active ? make_int4(acc_all ? 1 : 0, mptcl, reads_all | (reads_list << 1) | (move_far << 2),
-                                            s_ctl[3])
-                                : make_int4(0, -1, 0, 0);
+        const int4 pub = active ? make_int4(acc_all ? 1 : 0, mptcl, move_far, s_ctl[3]) : make_int4(0, -1, 0, 0);
         for (unsigned r = 0; r < CL; r++) cluster.map_shared_rank(&S.s_pub[rank], r)[0] = pub;
+        S.s_redo_local = 0;
       }
       cluster.sync();
-      if (warp == 0) {
-        // Slot `lane` is redone if an earlier slot of the pass accepted a move
-        // of its own particle, or of a partner its sums read: any particle
-        // when they read all, a list member, or a particle that left its
-        // sphere (the lists no longer bound it).  Every CTA computes the same.
-        bool redo = false;
-        int4 me = make_int4(0, -1, 0, 0);
-        if (lane >= pfirst && lane < P) me = S.s_pub[lane];
-        for (int q = pfirst; q < lane && q < P && !redo; q++) {
+      // This slot is made again if an earlier slot q of the pass accepted a
+      // move of its particle, or of a particle whose OLD or NEW positions come
+      // within the pair range of this slot's OLD or NEW positions at some
+      // slice (q's window is read from q's shared memory).  Otherwise every
+      // pair term between the two particles is zero before and after q's
+      // move, and this slot's sums are those of the in-order move.
+      if (active && (int)rank > pfirst)
+        for (int q = pfirst + warp; q < (int)rank; q += nwarps) {
           const int4 o = S.s_pub[q];
           if (!o.x) continue;  // a rejected move changed nothing
-          redo = o.y == me.y || (me.z & 1) || ((me.z & 2) && ((o.z & 4) || in_nbr_list(a, me.y, o.y)));
+          bool hit = o.y == mptcl;
+          if (!hit) {
+            const double(*qo)[3] = cluster.map_shared_rank(&S.win_old[0][0], (unsigned)q);
+            const double(*qn)[3] = cluster.map_shared_rank(&S.win_new[0][0], (unsigned)q);
+            hit = windows_near(win_old[0], win_new[0], qo, qn, span, a.pair_range, sys, lane);
+          }
+          if (hit && lane == 0) S.s_redo_local = 1;
         }
+      G.sync();
+      if (tid == 0)
+        for (unsigned r = 0; r < CL; r++) cluster.map_shared_rank(&S.s_redo[rank], r)[0] = S.s_redo_local;
+      cluster.sync();
+      if (warp == 0) {
+        const bool redo = lane > pfirst && lane < P && S.s_redo[lane] != 0;
         const unsigned bad = __ballot_sync(0xffffffffu, redo);
         const int nf = bad ? __ffs(bad) - 1 : P;
+        const int4 me = (lane >= pfirst && lane < P) ? S.s_pub[lane] : make_int4(0, -1, 0, 0);
         const bool kept = lane >= pfirst && lane < nf;
         const bool stop = __any_sync(0xffffffffu, me.w != 0);
-        const bool far_acc = __any_sync(0xffffffffu, kept && me.x && (me.z & 4));
+        const bool far_acc = __any_sync(0xffffffffu, kept && me.x && me.z);
         if (lane == 0) {
           S.s_commit[0] = nf;
           S.s_commit[1] = stop ? 1 : 0;

@@ -20,6 +20,7 @@ struct BisectionArgs {
   // cluster of a window has P CTAs, CTA p runs slot p from ChainState
   // p * kMaxWindows + w.  0 or 1: one proposal per window.
   int proposals;
+  double pair_range;          // DavidPA: pair terms are zero from this distance on (the grid end)
   unsigned long long round;   // Common-stream index of this round (concurrent)
   // LongRangeClass::SingleAction in the lowest stage (BisectionBlock.cc:92-103):
   // rho_k of the OLD path [slice][k], the k-vectors [k][3] and Ulong_k of level 0

@@ -713,6 +713,7 @@ static int run_bisection(pimc_context *ctx, int n_blocks, pimc_move_record *devi
   a.sr_higher = ctx->bis.shortrange_at_higher_levels;
   a.concurrent = ctx->bis.schedule != PIMC_SCHEDULE_SEQUENTIAL;
   a.proposals = ctx->bis.schedule == PIMC_SCHEDULE_PROPOSALS ? ctx->bis.cluster_ctas : 1;
+  a.pair_range = ctx->pa.kind == PA_DAVID ? ctx->pa.d64.grid.end : 0.0;
   a.round = ctx->rounds;
   a.use_lr = ctx->bis.use_longrange ? 1 : 0;
   a.rhok = ctx->d_rhok[0];

@@ -4,16 +4,15 @@ FP64 oracle's in-order replay.
 Each window of a round runs P proposal slots at once, one CTA each; a step
 of the window is slots 0..P-1 making one move each, and the device must give
 the result of making them one after another in slot order (oracle
-`run_proposals`).  The commit re-makes a slot whose move read a particle that
-an earlier slot's accepted move changed, so the traces must be identical
-whether or not the slots interact:
+`run_proposals`).  The commit makes a slot again when an earlier slot of the
+same pass accepted a move of its particle, or of a particle that comes
+within the table's range of it at some slice of the window, so the traces
+must be identical however the slots interact:
 
-  * neighbour lists with a skin above the moves' excursions: most slots are
-    independent and are kept in the first pass;
+  * neighbour lists with a skin above the moves' excursions;
   * a tiny skin: moves leave their spheres, which falls back to all partners
-    and forces re-makes;
-  * no lists: every slot reads every particle, so any accepted earlier slot
-    forces a re-make.
+    for the rest of the round;
+  * no lists: every slot sums over all partners.
 
 Tolerances as in test_gpu_parity: identical accept trace, per-stage dS within
 1e-9, final path within 1e-9.
@@ -75,9 +74,8 @@ def test_proposals_match_in_order_oracle(tmp_path, proposals, skin):
     assert stats["moves"] == len(live)
     assert 0 < acc < len(live)
     assert np.max(np.abs(d.get_path(P.OLDMODE) - o.get_path(0))) < 1e-9
-    if skin == 0.0:
-        # without lists every slot reads every particle: an accepted earlier
-        # slot forces the later ones to be made again
+    if proposals == 8:
+        # 8 slots in a 22.7 A box: some accepted moves come within range of a later slot's particle
         assert stats["redone"] > 0
 
 
