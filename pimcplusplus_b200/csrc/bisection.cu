@@ -21,7 +21,7 @@
 //    so each item reads its partner once and evaluates the pair action for
 //    the OLD and the NEW position of the moved particle, while the sampler
 //    warp draws the next level speculatively.
-//  * Two schedules.  Sequential: one window at a time, slice1 drawn from the
+//  * Three schedules.  Sequential: one window at a time, slice1 drawn from the
 //    Local stream exactly as ChooseTimeSlices does (BisectionBlock.cc:362-374).
 //    Concurrent windows: one launch is one round; the round draws an offset o
 //    from the Common stream and cluster w works the window starting at
@@ -30,6 +30,11 @@
 //    the windows commute: this is PIMC++'s time-slice parallelism (slice
 //    blocks moved concurrently, PathClass.h:33-36; the offset plays the role
 //    of ShiftMove, MetaMoves.cc:39-65) on the clusters of one GPU.
+//    Concurrent proposals: the windows schedule with P CTAs per window, each
+//    one proposal slot with its own Local stream evaluating alone; a step of
+//    the window has the result of slots 0..P-1 moving one after another, and
+//    a slot whose particle an earlier slot's accepted move came near is made
+//    again (the in-order commit in run_job).
 //  * The 1-D DavidPA diagonal column of every level is staged into shared
 //    memory once per launch by a bulk TMA copy (cp.async.bulk) completing on
 //    an mbarrier; tricubic tables stay in L2/HBM.
