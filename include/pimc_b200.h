@@ -57,6 +57,7 @@ extern "C" {
 #define PIMC_ACTION_SHORTRANGE 0
 #define PIMC_ACTION_KINETIC 1
 #define PIMC_ACTION_LONGRANGE 2
+#define PIMC_ACTION_DAVIDLONGRANGE 3 /* DavidLongRangeClassYk (pimc_davidlongrange_yk) */
 
 #define PIMC_GRID_LINEAR 0
 #define PIMC_GRID_LOG 1
@@ -160,6 +161,18 @@ int pimc_calc_rhok(pimc_context *ctx);
 int pimc_update_rhok(pimc_context *ctx, int slice1, int slice2, const int *active, int n_active,
                      int level);
 int pimc_get_rhok(pimc_context *ctx, int copy, double *out /* [slices][num_k][2] */);
+/* DavidLongRangeClassYk (Actions/DavidLongRangeClassYk.cc:38-126), one
+ * species: uk, duk and Vlong_k of the k-vectors from the squarer's k-space
+ * action uk_long at the magnitudes kvals (the .dm LongRange section read by
+ * DavidPAClass::ReadLongRangeHDF5, DavidPAClass.cc:914-950).  rpa = 1: the
+ * single-type RPA construction (BuildRPA_SingleType), 0: Build_MultipleSpecies
+ * (uk = tau uk_long/Omega, duk = Vlong_k = uk_long/Omega).  Every k-vector's
+ * |k| must be in kvals (within 1e-10).  Then PIMC_ACTION_DAVIDLONGRANGE in
+ * pimc_single_action / pimc_d_dbeta (d_dBeta ignores the level, as the
+ * reference), and DavidLongRangeClassYk::V (:367-389): */
+int pimc_davidlongrange_yk(pimc_context *ctx, int num_kvals, const double *kvals, const double *uk_long,
+                           int rpa);
+int pimc_davidlongrange_v(pimc_context *ctx, int slice1, int slice2, double *out);
 
 /* ---- device-resident bisection moves (BisectionBlockClass::MakeMove) ---- */
 

@@ -83,6 +83,11 @@ def lib():
         "oracle_get_rhok": (None, [p, i, dp]),
         "oracle_set_longrange": (None, [p, i, dp, dp, dp, dp, dp, dp, dp, dp, i]),
         "oracle_longrange_single": (d, [p, i, i, ip, i, i]),
+        "oracle_set_yk": (i, [p, i, dp, dp, i]),
+        "oracle_get_yk": (None, [p, dp, dp, dp]),
+        "oracle_yk_single": (d, [p, i, i, ip, i, i]),
+        "oracle_yk_dbeta": (d, [p, i, i]),
+        "oracle_yk_v": (d, [p, i, i]),
         "oracle_longrange_dbeta": (d, [p, i, i, i]),
         "oracle_bisection_config": (None, [p, i, i, i, i]),
         "oracle_rng_seed": (None, [p, u64]),
@@ -307,6 +312,33 @@ class System:
     def longrange_dbeta(self, s1, s2, level=0):
         self.set_mode(0)
         return lib().oracle_longrange_dbeta(self.h, s1, s2, level)
+
+    # ---- DavidLongRangeClassYk ----
+    def set_yk(self, kvals, uk_long, rpa=True):
+        """Tables from the squarer's k-space action uk_long(kvals); False if a
+        k-vector's |k| is not among kvals."""
+        kv = np.ascontiguousarray(kvals, dtype=np.float64)
+        uk = np.ascontiguousarray(uk_long, dtype=np.float64)
+        return lib().oracle_set_yk(self.h, len(kv), _dp(kv), _dp(uk), int(rpa)) == 0
+
+    def yk_tables(self):
+        n = lib().oracle_num_kvecs(self.h)
+        u, du, v = np.zeros(n), np.zeros(n), np.zeros(n)
+        lib().oracle_get_yk(self.h, _dp(u), _dp(du), _dp(v))
+        return u, du, v
+
+    def yk_single(self, s1, s2, active, level, copy=0):
+        a = np.ascontiguousarray(active, dtype=np.int32)
+        self.set_mode(copy)
+        return lib().oracle_yk_single(self.h, s1, s2, _ip(a), len(a), level)
+
+    def yk_dbeta(self, s1, s2):
+        self.set_mode(0)
+        return lib().oracle_yk_dbeta(self.h, s1, s2)
+
+    def yk_v(self, s1, s2):
+        self.set_mode(0)
+        return lib().oracle_yk_v(self.h, s1, s2)
 
     def bisection_config(self, num_levels, steps_per_block=1, shortrange_at_higher_levels=True,
                          use_longrange=False):

@@ -1114,6 +1114,97 @@ struct OracleSystem {
       U += k0Homo;
     return U;
   }
+  // ---- DavidLongRangeClassYk (PIMC++/src/Actions/DavidLongRangeClassYk.cc) ----
+  // uk, duk and Vlong_k per k-vector from the squarer's k-space table
+  // uk_long(k): BuildRPA_SingleType (:76-126) for one pair type (rpa), else
+  // Build_MultipleSpecies (:38-74).  A k-vector takes the table entry whose
+  // k equals its |k| within 1e-10; one without such an entry is an error
+  // here (the reference leaves it at -1 / unset).
+  std::vector<double> YkU, YkDU, YkV;
+  int SetYk(int nkv, const double *kvals, const double *uk_long, int rpa) {
+    const int K = nk();
+    double vol = 1.0;
+    for (int dim = 0; dim < 3; dim++) vol *= Box[dim];
+    YkU.assign(K, -1.0);
+    YkDU.assign(K, 0.0);
+    YkV.assign(K, 0.0);
+    std::vector<char> set(K, 0);
+    const double ncomps = N;
+    for (int i = 0; i < nkv; i++) {
+      const double k = kvals[i];
+      double u = 0.0, du = 0.0, v = uk_long[i] / vol;
+      if (rpa) {
+        if (std::fabs(k) < 1e-10) continue;  // yk_zero: not used by the action
+        const double arg = 1.0 + ncomps * 2.0 * uk_long[i] / (lambda * k * k * vol);
+        const double theta = 0.5 * k * k * lambda * tau;
+        double q, sv, tn;
+        if (arg < 0) {
+          q = sqrt(-arg);
+          tn = tan(q * theta);
+          sv = q * (1 - q * tn) / (q + tn);
+        } else if (arg == 0) {
+          sv = 1.0 / (1.0 + theta);
+        } else {
+          q = sqrt(arg);
+          tn = tanh(theta * q);
+          sv = q * (1.0 + q * tn) / (q + tn);
+        }
+        u = (-1.0 + sv) / ncomps;
+        du = uk_long[i] / vol - lambda * k * k * u * (1.0 + 0.5 * ncomps * u);
+      } else {
+        u = v * tau;
+        du = v;
+      }
+      for (int j = 0; j < K; j++) {
+        const double *kv = &kVecs[(size_t)j * 3];
+        if (std::fabs(sqrt(kv[0] * kv[0] + kv[1] * kv[1] + kv[2] * kv[2]) - k) < 1e-10) {
+          YkU[j] = u;
+          YkDU[j] = du;
+          YkV[j] = v;
+          set[j] = 1;
+        }
+      }
+    }
+    for (int j = 0; j < K; j++)
+      if (!set[j]) return -1;
+    return 0;
+  }
+  // SingleAction (:230-323): on NEW, rho_k updated over the window's
+  // interior (the whole path: [slice1, slice2 - skip]); then
+  // sum_k sum_slices |rho_k|^2 uk with weight 1, over [slice1 + skip,
+  // slice2 - skip] (the whole path: [slice1, slice2 - skip]).  No active
+  // particle: no species, 0.
+  double YkSingle(int slice1, int slice2, const int *changed, int n, int level) {
+    const int skip = 1 << level, K = nk();
+    const bool inclusive = !(slice1 == 0 && slice2 == NumSlices - 1);
+    const int startSlice = inclusive ? slice1 + skip : slice1, endSlice = slice2 - skip;
+    if (mode == 1 && startSlice <= endSlice) UpdateRho_ks(startSlice, endSlice, changed, n, level);
+    if (n == 0) return 0.0;
+    double total = 0.0;
+    for (int ki = 0; ki < K; ki++)
+      for (int slice = startSlice; slice <= endSlice; slice += skip) {
+        const std::complex<double> z = Rho_k[mode][(size_t)slice * K + ki];
+        total += 1.0 * (z.real() * z.real() + z.imag() * z.imag()) * YkU[ki];
+      }
+    return total;
+  }
+  // d_dBeta (:327-363) and V (:367-389): every slice of [slice1, slice2]
+  // recomputed, weight 1/2 at both ends, with duk or Vlong_k.
+  double YkSum(int slice1, int slice2, const std::vector<double> &w) {
+    const int K = nk();
+    double total = 0.0;
+    for (int slice = slice1; slice <= slice2; slice++) {
+      double sliceTotal = 0.0;
+      const double factor = ((slice == slice1) || (slice == slice2)) ? 0.5 : 1.0;
+      CalcRho_ks_Fast(slice);
+      for (int ki = 0; ki < K; ki++) {
+        const std::complex<double> z = Rho_k[mode][(size_t)slice * K + ki];
+        sliceTotal += factor * (z.real() * z.real() + z.imag() * z.imag()) * w[ki];
+      }
+      total += sliceTotal;
+    }
+    return total;
+  }
   // LongRangeClass::d_dBeta (LongRangeClass.cc:374-442), one species
   double LongRangeDBeta(int slice1, int slice2, int level) {
     int skip = 1 << level, K = nk();
@@ -1404,6 +1495,19 @@ double oracle_longrange_dbeta(OracleSystem *s, int slice1, int slice2, int level
   return s->LongRangeDBeta(slice1, slice2, level);
 }
 
+int oracle_set_yk(OracleSystem *s, int num_kvals, const double *kvals, const double *uk_long, int rpa) {
+  return s->SetYk(num_kvals, kvals, uk_long, rpa);
+}
+void oracle_get_yk(OracleSystem *s, double *uk, double *duk, double *vlong) {
+  memcpy(uk, s->YkU.data(), s->YkU.size() * sizeof(double));
+  memcpy(duk, s->YkDU.data(), s->YkDU.size() * sizeof(double));
+  memcpy(vlong, s->YkV.data(), s->YkV.size() * sizeof(double));
+}
+double oracle_yk_single(OracleSystem *s, int slice1, int slice2, const int *active, int n, int level) {
+  return s->YkSingle(slice1, slice2, active, n, level);
+}
+double oracle_yk_dbeta(OracleSystem *s, int slice1, int slice2) { return s->YkSum(slice1, slice2, s->YkDU); }
+double oracle_yk_v(OracleSystem *s, int slice1, int slice2) { return s->YkSum(slice1, slice2, s->YkV); }
 void oracle_bisection_config(OracleSystem *s, int num_levels, int steps_per_block, int sr_higher, int use_longrange) {
   s->NumLevels = num_levels;
   s->StepsPerBlock = steps_per_block;

@@ -123,6 +123,15 @@ int oracle_run_bisection(OracleSystem *s, int n_blocks, OracleMoveRecord *record
 /* Concurrent-window schedule replayed sequentially: n_rounds rounds, each
  * windows*steps_per_block records (slice1 = -1 for a window that does not
  * fit); returns windows = floor((slices-1)/2^L). */
+/* DavidLongRangeClassYk on the k-vectors of oracle_setup_kvecs: tables from
+ * the squarer's k-space action uk_long(kvals) (rpa: the single-type RPA
+ * construction), -1 if a k-vector's |k| is not among kvals; the actions on
+ * the active copy (oracle_system_set_mode). */
+int oracle_set_yk(OracleSystem *s, int num_kvals, const double *kvals, const double *uk_long, int rpa);
+void oracle_get_yk(OracleSystem *s, double *uk, double *duk, double *vlong);
+double oracle_yk_single(OracleSystem *s, int slice1, int slice2, const int *active, int n, int level);
+double oracle_yk_dbeta(OracleSystem *s, int slice1, int slice2);
+double oracle_yk_v(OracleSystem *s, int slice1, int slice2);
 int oracle_run_windows(OracleSystem *s, int n_rounds, OracleMoveRecord *records);
 /* The same with `proposals` (1..16) slots per window: every step of a window
  * is slots 0..proposals-1 making one move each, in slot order, slot p from

@@ -32,7 +32,7 @@ PIMC_OK = 0
 PIMC_E_ARG = 1
 OLDMODE, NEWMODE, BOTH = 0, 1, 2
 FP64, MIXED = 0, 1
-ACTION_SHORTRANGE, ACTION_KINETIC, ACTION_LONGRANGE = 0, 1, 2
+ACTION_SHORTRANGE, ACTION_KINETIC, ACTION_LONGRANGE, ACTION_DAVIDLONGRANGE = 0, 1, 2, 3
 GRID_LINEAR, GRID_LOG = 0, 1
 SEQUENTIAL, WINDOWS, PROPOSALS = 0, 1, 2
 
@@ -155,6 +155,8 @@ _SIGS = {
     "pimc_get_rhok": (_i, [_p, _i, _dp]),
     "pimc_pa_coulomb": (_i, [_p, _i, _i, _d, _i]),
     "pimc_longrange_coulomb": (_i, [_p, _i, _i]),
+    "pimc_davidlongrange_yk": (_i, [_p, _i, _dp, _dp, _i]),
+    "pimc_davidlongrange_v": (_i, [_p, _i, _i, _dp]),
     "pimc_coulomb_breakup": (_i, [_dp, _d, _d, _i, _i, _d, _i, _dp] + [_dp] * 11),
     "pimc_quintic_spline": (_i, [_i, _d, _dp, _dp]),
     "pimc_energy": (_i, [_p, C.POINTER(EnergyTerms)]),
@@ -352,6 +354,16 @@ class PathData:
         self._check(_lib.pimc_set_longrange(self.h, arrs[1].shape[0], *[_dptr(a) for a in arrs],
                                             int(use_background)), "set_longrange")
 
+    def davidlongrange_yk(self, kvals, uk_long, rpa=True):
+        """DavidLongRangeClassYk tables (after setup_kvecs) from the squarer's
+        k-space action uk_long at the magnitudes kvals."""
+        kv = np.ascontiguousarray(kvals, dtype=np.float64)
+        uk = np.ascontiguousarray(uk_long, dtype=np.float64)
+        if kv.shape != uk.shape or kv.ndim != 1:
+            raise ValueError("kvals and uk_long must be 1-D arrays of one length")
+        self._check(_lib.pimc_davidlongrange_yk(self.h, len(kv), _dptr(kv), _dptr(uk), int(rpa)),
+                    "davidlongrange_yk")
+
     def calc_rhok(self):
         self._check(_lib.pimc_calc_rhok(self.h), "calc_rhok")
 
@@ -441,6 +453,21 @@ class LongRangeClass(ActionBaseClass):
 
     def GetName(self):
         return "LongRange"
+
+
+class DavidLongRangeClassYk(ActionBaseClass):
+    """DavidLongRangeClassYk (PIMC++/src/Actions/DavidLongRangeClassYk.cc:230-389),
+    after PathData.davidlongrange_yk."""
+    kind = ACTION_DAVIDLONGRANGE
+
+    def GetName(self):
+        return "DavidsLongRange"
+
+    def V(self, slice1, slice2, level=0):
+        out = C.c_double()
+        self.PathData._check(_lib.pimc_davidlongrange_v(self.PathData.h, slice1, slice2, C.byref(out)),
+                             "davidlongrange_v")
+        return out.value
 
 
 class BisectionBlock:

@@ -270,6 +270,7 @@ int pimc_destroy(pimc_context *ctx) {
   cudaFree(ctx->d_rhok[1]);
   cudaFree(ctx->d_ulong_k);
   cudaFree(ctx->d_dulong_k);
+  cudaFree(ctx->d_yk);
   cudaFree(ctx->d_gofr);
   cudaFree(ctx->d_kvec);
   cudaFree(ctx->d_nbr_cb);
@@ -448,6 +449,9 @@ int pimc_get_path(pimc_context *ctx, int copy, double *path) {
 
 static int longrange_single(pimc_context *ctx, int copy, int slice1, int slice2, const ActiveList &act, int level,
                             double *out);
+static int yk_single(pimc_context *ctx, int copy, int slice1, int slice2, const ActiveList &act, int level,
+                     double *out);
+static int yk_sum(pimc_context *ctx, int slice1, int slice2, int table, double *out);
 
 static int check_slices(pimc_context *ctx, int slice1, int slice2, int level, bool inclusive) {
   if (level < 0 || level >= kMaxLevels) return fail(ctx, PIMC_E_ARG, "level out of range");
@@ -467,6 +471,7 @@ int pimc_single_action(pimc_context *ctx, int action, int copy, int slice1, int 
   if ((rc = check_active(ctx, active, n_active, act))) return rc;
   CK(cudaSetDevice(ctx->device));
   if (action == PIMC_ACTION_LONGRANGE) return longrange_single(ctx, copy, slice1, slice2, act, level, out);
+  if (action == PIMC_ACTION_DAVIDLONGRANGE) return yk_single(ctx, copy, slice1, slice2, act, level, out);
   const int skip = 1 << level;
   const int nlinks = (slice2 - slice1 + skip - 1) / skip;
   ReduceTarget t{ctx->stream, ctx->d_partials, ctx->d_counter, ctx->d_out};
@@ -525,6 +530,7 @@ int pimc_d_dbeta(pimc_context *ctx, int action, int slice1, int slice2, int leve
   if (rc) return rc;
   CK(cudaSetDevice(ctx->device));
   const int skip = 1 << level;
+  if (action == PIMC_ACTION_DAVIDLONGRANGE) return yk_sum(ctx, slice1, slice2, 1, out);
   if (action == PIMC_ACTION_LONGRANGE) {
     // LongRangeClass::d_dBeta (LongRangeClass.cc:374-442): rho_k of the OLD
     // copy recomputed (CalcRho_ks_Fast), then the dU tables.
@@ -863,6 +869,7 @@ int pimc_setup_kvecs(pimc_context *ctx, double kcutoff, int *num_k) {
   ctx->num_k = (int)kidx.size();
   ctx->kcutoff = kcutoff;
   ctx->rhok_valid = false;
+  ctx->yk_ready = false;  // tables are per k-vector
   cudaFree(ctx->d_kvec);
   ctx->d_kvec = nullptr;
   CK(cudaMalloc(&ctx->d_kvec, ctx->kvecs.size() * sizeof(double) + 16));
@@ -918,6 +925,111 @@ int pimc_set_longrange(pimc_context *ctx, int num_levels, const double *ulong_k,
   ctx->use_background = use_background;
   ctx->lr_ready = true;
   return PIMC_OK;
+}
+
+// ---- DavidLongRangeClassYk (PIMC++/src/Actions/DavidLongRangeClassYk.cc) ----
+// BuildRPA_SingleType (:76-126) for one pair type (rpa), else
+// Build_MultipleSpecies (:38-74): per k-vector the entry of the squarer's
+// k-space table whose k equals its |k| within 1e-10 (:57, :111).
+int pimc_davidlongrange_yk(pimc_context *ctx, int num_kvals, const double *kvals, const double *uk_long, int rpa) {
+  if (!ctx) return PIMC_E_ARG;
+  if (num_kvals < 1 || !kvals || !uk_long) return fail(ctx, PIMC_E_ARG, "bad k-space table");
+  if (ctx->num_k <= 0) return fail(ctx, PIMC_E_STATE, "pimc_setup_kvecs not called");
+  const int K = ctx->num_k;
+  const double vol = ctx->sys.box[0] * ctx->sys.box[1] * ctx->sys.box[2];
+  const double ncomps = ctx->sys.N, lambda = ctx->sys.lambda, tau = ctx->sys.tau;
+  if (rpa && !(lambda > 0.0)) return fail(ctx, PIMC_E_ARG, "the RPA construction needs lambda > 0");
+  std::vector<double> t(3 * (size_t)K, 0.0);
+  std::vector<char> set(K, 0);
+  for (int i = 0; i < num_kvals; i++) {
+    const double k = kvals[i];
+    const double v = uk_long[i] / vol;
+    double u, du;
+    if (rpa) {
+      if (std::fabs(k) < 1e-10) continue;  // yk_zero: not used by the action
+      const double arg = 1.0 + ncomps * 2.0 * uk_long[i] / (lambda * k * k * vol);
+      const double theta = 0.5 * k * k * lambda * tau;
+      double sv;
+      if (arg < 0) {
+        const double q = std::sqrt(-arg), tn = std::tan(q * theta);
+        sv = q * (1 - q * tn) / (q + tn);
+      } else if (arg == 0) {
+        sv = 1.0 / (1.0 + theta);
+      } else {
+        const double q = std::sqrt(arg), tn = std::tanh(theta * q);
+        sv = q * (1.0 + q * tn) / (q + tn);
+      }
+      u = (-1.0 + sv) / ncomps;
+      du = uk_long[i] / vol - lambda * k * k * u * (1.0 + 0.5 * ncomps * u);
+    } else {
+      u = v * tau;
+      du = v;
+    }
+    for (int j = 0; j < K; j++) {
+      const double *kv = &ctx->kvecs[(size_t)j * 3];
+      if (std::fabs(std::sqrt(kv[0] * kv[0] + kv[1] * kv[1] + kv[2] * kv[2]) - k) < 1e-10) {
+        t[j] = u;
+        t[K + j] = du;
+        t[2 * (size_t)K + j] = v;
+        set[j] = 1;
+      }
+    }
+  }
+  for (int j = 0; j < K; j++)
+    if (!set[j]) return fail(ctx, PIMC_E_ARG, "a k-vector's |k| is not in the k-space table");
+  CK(cudaSetDevice(ctx->device));
+  cudaFree(ctx->d_yk);
+  ctx->d_yk = nullptr;
+  ctx->yk_ready = false;
+  CK(cudaMalloc(&ctx->d_yk, t.size() * sizeof(double)));
+  CK(cudaMemcpy(ctx->d_yk, t.data(), t.size() * sizeof(double), cudaMemcpyHostToDevice));
+  ctx->yk_ready = true;
+  return PIMC_OK;
+}
+
+// DavidLongRangeClassYk::SingleAction (:230-323).  Away from the whole path
+// only the window's interior counts: on NEW, rho_k is updated over
+// [slice1 + skip, slice2 - skip] ([slice1, slice2 - skip] for the whole
+// path), and sum_k sum_slices |rho_k|^2 uk runs over the same slices with
+// weight 1.  No active particle: no species in the sum, 0.
+static int yk_single(pimc_context *ctx, int copy, int slice1, int slice2, const ActiveList &act, int level,
+                     double *out) {
+  if (!ctx->yk_ready) return fail(ctx, PIMC_E_STATE, "pimc_davidlongrange_yk not called");
+  const int skip = 1 << level;
+  const bool inclusive = !(slice1 == 0 && slice2 == ctx->sys.S - 1);
+  const int first = inclusive ? slice1 + skip : slice1, last = slice2 - skip;
+  const LRDesc lr = lr_desc(ctx);
+  if (copy == PIMC_NEW && first <= last)
+    CK(launch_rhok_update(ctx->stream, ctx->d_path[0], ctx->d_path[1], ctx->sys.N, lr, act, first, last, skip,
+                          ctx->d_rhok[0], ctx->d_rhok[1]));
+  if (act.n == 0 || first > last) {
+    CK(cudaStreamSynchronize(ctx->stream));
+    *out = 0.0;
+    return PIMC_OK;
+  }
+  ReduceTarget t{ctx->stream, ctx->d_partials, ctx->d_counter, ctx->d_out};
+  CK(launch_lr_sum(t, ctx->d_rhok[copy], lr, ctx->d_yk, first, last, skip, ctx->sm_count, 1.0));
+  return finish_scalar(ctx, out);
+}
+
+// DavidLongRangeClassYk::d_dBeta (:327-363, table 1: duk) and V (:367-389,
+// table 2: Vlong_k): rho_k of the OLD copy recomputed, every slice of
+// [slice1, slice2] (the level is not used), weight 1/2 at both ends.
+static int yk_sum(pimc_context *ctx, int slice1, int slice2, int table, double *out) {
+  if (!ctx->yk_ready) return fail(ctx, PIMC_E_STATE, "pimc_davidlongrange_yk not called");
+  const LRDesc lr = lr_desc(ctx);
+  CK(launch_rhok_full(ctx->stream, ctx->d_path[0], ctx->sys.N, ctx->sys.S, lr, ctx->d_rhok[0]));
+  ReduceTarget t{ctx->stream, ctx->d_partials, ctx->d_counter, ctx->d_out};
+  CK(launch_lr_sum(t, ctx->d_rhok[0], lr, ctx->d_yk + (size_t)table * ctx->num_k, slice1, slice2, 1, ctx->sm_count,
+                   0.5));
+  return finish_scalar(ctx, out);
+}
+
+int pimc_davidlongrange_v(pimc_context *ctx, int slice1, int slice2, double *out) {
+  if (!ctx || !out) return PIMC_E_ARG;
+  if (int rc = check_slices(ctx, slice1, slice2, 0, true)) return rc;
+  CK(cudaSetDevice(ctx->device));
+  return yk_sum(ctx, slice1, slice2, 2, out);
 }
 
 // PathClass::UpdateRho_ks() full recompute (PathClass.cc:710-718): OLD, then NEW = OLD.

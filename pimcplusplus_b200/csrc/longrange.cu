@@ -4,6 +4,8 @@
 //   PathClass::UpdateRho_ks       (PathClass.cc:649-707)  — rhok_update_kernel
 //   LongRangeClass::SingleAction  (LongRangeClass.cc:273-371) and
 //   LongRangeClass::d_dBeta       (LongRangeClass.cc:374-442) — lr_sum_kernel
+//   DavidLongRangeClassYk::SingleAction / d_dBeta / V
+//                                 (DavidLongRangeClassYk.cc:230-389) — lr_sum_kernel
 //
 // rho_k is stored [slice][k] as double2 (re, im), one species.  The phase
 // factors follow the reference exactly: per particle and dimension,
@@ -142,7 +144,8 @@ __device__ __forceinline__ double lr_block_sum(double v, double *sh) {
 // (the homologous k-space term); factor 1/2 at the two ends.
 __global__ void __launch_bounds__(256) lr_sum_kernel(const double2 *__restrict__ rhok, LRDesc lr,
                                                      const double *__restrict__ uk, int slice1, int slice2, int skip,
-                                                     double *partials, unsigned int *counter, double *out) {
+                                                     double end_weight, double *partials, unsigned int *counter,
+                                                     double *out) {
   __shared__ double sh[32];
   __shared__ int s_last;
   const int nsl = (slice2 - slice1) / skip + 1;
@@ -152,7 +155,7 @@ __global__ void __launch_bounds__(256) lr_sum_kernel(const double2 *__restrict__
        i += (long long)gridDim.x * blockDim.x) {
     const int b = (int)(i / lr.nk), k = (int)(i - (long long)b * lr.nk);
     const int slice = slice1 + b * skip;
-    const double factor = (slice == slice1 || slice == slice2) ? 0.5 : 1.0;
+    const double factor = (slice == slice1 || slice == slice2) ? end_weight : 1.0;
     const double2 r = rhok[(size_t)slice * lr.nk + k];
     const double rhok2 = r.x * r.x + r.y * r.y;
     acc += factor * 0.5 * 2.0 * rhok2 * uk[k];
@@ -200,14 +203,15 @@ cudaError_t launch_rhok_update(cudaStream_t st, const double *path_old, const do
 }
 
 cudaError_t launch_lr_sum(const ReduceTarget &t, const double2 *rhok, const LRDesc &lr, const double *uk, int slice1,
-                          int slice2, int skip, int sm_count) {
+                          int slice2, int skip, int sm_count, double end_weight) {
   const int nsl = (slice2 - slice1) / skip + 1;
   long long items = (long long)nsl * lr.nk;
   long long blocks = (items + 255) / 256;
   if (blocks > sm_count * 4) blocks = sm_count * 4;
   if (blocks > kPartialSlots) blocks = kPartialSlots;
   if (blocks < 1) blocks = 1;
-  lr_sum_kernel<<<(int)blocks, 256, 0, t.stream>>>(rhok, lr, uk, slice1, slice2, skip, t.partials, t.counter, t.out);
+  lr_sum_kernel<<<(int)blocks, 256, 0, t.stream>>>(rhok, lr, uk, slice1, slice2, skip, end_weight, t.partials,
+                                                   t.counter, t.out);
   return cudaGetLastError();
 }
 

@@ -204,6 +204,9 @@ struct pimc_context {
   int lr_levels = 0, use_background = 0;
   double *d_ulong_k = nullptr, *d_dulong_k = nullptr;  // [levels][k]
   std::vector<double> ulong_r0, ushort_k0, ulong_k0, dulong_r0, dushort_k0, dulong_k0;
+  // DavidLongRangeClassYk: uk, duk, Vlong_k of the k-vectors ([3][k])
+  double *d_yk = nullptr;
+  bool yk_ready = false;
   // pair correlation accumulator (PairCorrelationClass)
   unsigned long long *d_gofr = nullptr;
   int gofr_points = 0;
