@@ -33,6 +33,14 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
+_T0 = time.perf_counter()
+
+
+def progress(msg):
+    """One timestamped line per leg on stderr (the JSON line stays alone on stdout)."""
+    print(f"[bench +{time.perf_counter() - _T0:7.1f}s] {msg}", file=sys.stderr, flush=True)
+
+
 METRIC = "pair-action evals/s & bisection moves/s, mixed vs FP64 GPU at ΔS relerr≤1e-6"
 UNIT = "pair-action evals/s"
 # Algorithmic bytes per tricubic pair evaluation: partner at two slices (48 B
@@ -361,8 +369,10 @@ def run_ours(args):
     sampler = ClockSampler(local) if rank == 0 else None
     if sampler:
         sampler.start()
+    progress("C2 timed legs")
     ms64, st64 = timed(P.FP64)
     ms32, st32 = timed(P.MIXED)
+    progress("C2 FP64 and mixed done")
     ms64, st64 = agg(ms64, st64)
     ms32, st32 = agg(ms32, st32)
     other = "sequential" if args.schedule == "windows" else "windows"
@@ -370,6 +380,7 @@ def run_ours(args):
     ms_o, st_o = agg(ms_o, st_o)
 
     # dS accuracy of the mixed path: mixed decisions with the FP64 terms alongside
+    progress("C2 dS accuracy")
     d, bb = make(P.MIXED, shadow=True, schedule="sequential")
     bb.MakeMoves(200 // args.steps_per_block, trace=False)
     rec, sh = bb.MakeMoves(max(1, args.accuracy_moves // args.steps_per_block), trace=True)
@@ -379,6 +390,7 @@ def run_ours(args):
     flip_rate = sh["flips"] / max(1, sh["stages_attempted"])
 
     # end to end through the public API: host path in, moves, path + counters out
+    progress("C2 end to end")
     d, bb = make(P.MIXED)
     host = start.copy()
     for _ in range(2):
@@ -404,9 +416,13 @@ def run_ours(args):
         dist.all_reduce(v)
         e2e_evals_timed = float(v.item())
 
+    progress("C3")
     c3 = None if args.no_c3 else run_c3(args, P, torch, flush, local, rank, world, agg)
+    progress("C4")
     c4 = None if args.no_c4 else run_c4(args, P, torch, flush, local, rank, world, agg)
+    progress("C5")
     c5 = None if args.no_c5 else run_c5(args, P, torch, flush, local, rank, world, agg)
+    progress("GPU legs done")
     clocks = sampler.stop() if sampler else None
     if clocks:
         clocks["window"] = "all timed legs (C2 FP64, mixed, other schedule, accuracy, e2e, C3)"
@@ -425,6 +441,7 @@ def run_ours(args):
             with open(prof) as f:
                 pj = json.load(f)
             traffic = pj.get("dram_bytes_per_pair_eval_mixed", 0) * evals_per_launch
+        progress("CPU baseline")
         cpu = cpu_baseline(1, args.cpu_seconds) if world == 1 and not args.no_cpu else None
         path_bytes = n * slices * 3 * 8
         line = {
@@ -494,6 +511,7 @@ def run_c3(args, P, torch, flush, local, rank, world, agg):
             tune = dict(threads_per_cta=int(t), max_split=int(sp), split_ratio=float(r), fixed=True)
         else:
             tune = b.autotune(nb)
+        progress(f"C3 batched {'mixed' if precision == P.MIXED else 'FP64'}: {tune}")
         stream = torch.cuda.ExternalStream(b.stream, device=f"cuda:{local}")
         for _ in range(args.warmup):
             b.run_async(nb)
@@ -554,6 +572,7 @@ def run_c3(args, P, torch, flush, local, rank, world, agg):
         return tot_ms, dict(accepted=acc, moves=mv, pair_evals=ev)
 
     sample = chains[: args.c3_plain_sample]
+    progress("C3 plain path")
     pms64, pst64 = agg(*plain(P.FP64, sample))
     pms32, pst32 = agg(*plain(P.MIXED, sample))
 
@@ -650,7 +669,9 @@ def run_c4(args, P, torch, flush, local, rank, world, agg):
         return ms, st, frac0, nk
 
     ms32, st32, f32, nk = timed(P.MIXED)
+    progress("C4 mixed done")
     ms64, st64, f64, _ = timed(P.FP64)
+    progress("C4 FP64 done")
     d, bb, _ = make(P.MIXED, shadow=True, schedule=P.SEQUENTIAL)
     bb.MakeMoves(20, trace=False)
     rec, sh = bb.MakeMoves(max(1, args.accuracy_moves // spb), trace=True)
@@ -722,6 +743,7 @@ def run_c5(args, P, torch, flush, local, rank, world, agg):
     # a short all-partner run gives the path its quantum spread first (untimed)
     d, bb = make(P.MIXED, 0.0, start)
     bb.MakeMoves(args.c5_equil, trace=False)
+    progress("C5 equilibrated")
     eq = d.get_path(P.OLDMODE)
     d.close()
     rounds = args.c5_rounds
@@ -761,9 +783,11 @@ def run_c5(args, P, torch, flush, local, rank, world, agg):
     lists32 = timed(P.MIXED, args.c5_skin)
     lists64 = timed(P.FP64, args.c5_skin)
     plain32 = timed(P.MIXED, 0.0)
+    progress("C5 windows legs done")
     pp = args.c5_proposals
     prop32 = timed(P.MIXED, args.c5_skin, pp)
     prop64 = timed(P.FP64, args.c5_skin, pp)
+    progress("C5 proposals done")
     wide32 = timed(P.MIXED, args.c5_skin, args.c5_proposals_wide) if args.c5_proposals_wide else None
     return {
         "workload": f"{n} LJ He-4, rho 0.02186/A^3, T=1 K, M={m}, LJ truncated/shifted at 2.5 sigma, level {L}, "
