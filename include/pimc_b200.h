@@ -126,6 +126,46 @@ int pimc_pa_tricubic(pimc_context *ctx, int sp1, int sp2, const double qgrid[3],
 int pimc_set_path(pimc_context *ctx, int copy, const double *path);
 int pimc_get_path(pimc_context *ctx, int copy, double *path);
 
+/* Host-only (no GPU needed): PathClass::InitRandomFixed
+ * (PIMC++/src/InitPaths.cc:966-999).  Places num_particles points uniformly
+ * in the box from the World stream of `seed` (Philox-4x32-10, stream 2,
+ * drawn in the reference's order), each at least 2*radius (minimum image)
+ * from the earlier ones; writes positions[num_particles][3].  Returns
+ * PIMC_E_CAP where the reference aborts: a particle that took 1000 tries. */
+int pimc_init_random_fixed(const double box[3], int num_particles, double radius, uint64_t seed,
+                           double *positions);
+
+/* Host-only: element `index` of the library's Philox-4x32-10 stream `stream`
+ * under `seed`, a double in [0, 1) (the draw RandomClass::Local/Common/World
+ * make, Common/Random/Random.h:33-49).  Streams 0, 1, 2 are Local, Common,
+ * World; 3 serves host-side ShiftMove draws; 0x100 + 64p + w are the windows'
+ * and proposal slots' Local streams. */
+int pimc_stream_uniform(uint64_t seed, uint32_t stream, uint64_t index, double *out);
+
+/* PathClass::ShiftPathData on one process (PIMC++/src/PathClass.cc:1026-1110),
+ * the data step of ShiftMoveClass::MakeMove (PIMC++/src/Moves/MetaMoves.cc:39-65):
+ * row j of both copies becomes row (j - slices_to_shift) mod M of OLD,
+ * M = num_time_slices - 1.  Call between moves (OLD == NEW); rho_k and the
+ * neighbour lists are rebuilt by the next device moves. */
+int pimc_shift_data(pimc_context *ctx, int slices_to_shift);
+
+/* ShiftMoveClass::MakeMove (PIMC++/src/Moves/MetaMoves.cc:39-65): draws
+ * CommonInt(M) = floor(u * M) slices, u from stream 3 of the pimc_rng_seed key
+ * at the context's own draw counter, and calls pimc_shift_data.  Writes the
+ * shift to *slices_shifted (may be NULL). */
+int pimc_shift_move(pimc_context *ctx, int *slices_shifted);
+
+/* Flat-binary checkpoint of a chain: both path copies, every Local/window
+ * RNG stream position with its Gaussian cache, the move counters and the
+ * concurrent-window round counter, the seed and the ShiftMove draw counter.  Replaces the reference's HDF5 path dump
+ * and InitPaths = "RESTART" (PIMC++/src/InitPaths.cc:826-845).  Reading
+ * checks that N, slices, box, tau and lambda equal the context's
+ * (PIMC_E_ARG otherwise, PIMC_E_FILE for a missing or malformed file); a
+ * chain continued from its checkpoint makes the same moves as the chain
+ * that wrote it. */
+int pimc_checkpoint_write(pimc_context *ctx, const char *filename);
+int pimc_checkpoint_read(pimc_context *ctx, const char *filename);
+
 /* ---- ActionBaseClass drop-in ---- */
 
 /* ActionBaseClass::SingleAction(slice1, slice2, activeParticles, level) of the

@@ -70,6 +70,7 @@ def lib():
         "oracle_system_get_path": (None, [p, i, dp]),
         "oracle_system_set_mode": (None, [p, i]),
         "oracle_init_random_fixed": (i, [p, u64, d]),
+        "oracle_shift_data": (i, [p, i]),
         "oracle_shortrange_single": (d, [p, i, i, ip, i, i]),
         "oracle_shortrange_single_abs": (d, [p, i, i, ip, i, i]),
         "oracle_shortrange_dbeta": (d, [p, i, i, i]),
@@ -250,6 +251,10 @@ class System:
     def init_random_fixed(self, seed, radius):
         if lib().oracle_init_random_fixed(self.h, seed, radius):
             raise RuntimeError("InitRandomFixed: exceeded 1000 tries")
+
+    def shift_data(self, slices_to_shift):
+        if lib().oracle_shift_data(self.h, slices_to_shift):
+            raise ValueError("|slices_to_shift| must be below num_time_slices")
 
     def shortrange_single(self, s1, s2, active, level, copy=0):
         a = np.ascontiguousarray(active, dtype=np.int32)

@@ -1439,6 +1439,38 @@ int oracle_init_random_fixed(OracleSystem *s, uint64_t seed, double radius) {
   return 0;
 }
 
+// PathClass::ShiftPathData (PIMC++/src/PathClass.cc:1026-1110) on one
+// process: sendProc == recvProc == 0, so the ring send/receive hands the
+// send buffer straight back.  Permutations are the identity (MoveJoin no-op).
+int oracle_shift_data(OracleSystem *s, int slicesToShift) {
+  const int numPtcls = s->N, numSlices = s->NumSlices;
+  if (!(abs(slicesToShift) < numSlices)) return 1;
+  auto NEWp = [&](int slice, int ptcl) { return s->P(1, slice, ptcl); };
+  auto OLDp = [&](int slice, int ptcl) { return s->P(0, slice, ptcl); };
+  if (slicesToShift > 0) {
+    for (int slice = numSlices - 1; slice >= slicesToShift; slice--)
+      for (int ptcl = 0; ptcl < numPtcls; ptcl++) memcpy(NEWp(slice, ptcl), NEWp(slice - slicesToShift, ptcl), 24);
+  } else {
+    for (int slice = 0; slice < numSlices + slicesToShift; slice++)
+      for (int ptcl = 0; ptcl < numPtcls; ptcl++) memcpy(NEWp(slice, ptcl), NEWp(slice - slicesToShift, ptcl), 24);
+  }
+  const int count = abs(slicesToShift) * numPtcls;
+  std::vector<double> buffer((size_t)count * 3);
+  int buffIndex = 0;
+  int startSlice = slicesToShift > 0 ? numSlices - slicesToShift : 0;
+  for (int slice = startSlice; slice < startSlice + abs(slicesToShift); slice++)
+    for (int ptcl = 0; ptcl < numPtcls; ptcl++, buffIndex++)
+      memcpy(&buffer[(size_t)buffIndex * 3], OLDp(slicesToShift > 0 ? slice - 1 : slice + 1, ptcl), 24);
+  startSlice = slicesToShift > 0 ? 0 : numSlices + slicesToShift;
+  buffIndex = 0;
+  for (int slice = startSlice; slice < startSlice + abs(slicesToShift); slice++)
+    for (int ptcl = 0; ptcl < numPtcls; ptcl++, buffIndex++)
+      memcpy(NEWp(slice, ptcl), &buffer[(size_t)buffIndex * 3], 24);
+  for (int slice = 0; slice < numSlices; slice++)
+    for (int ptcl = 0; ptcl < numPtcls; ptcl++) memcpy(OLDp(slice, ptcl), NEWp(slice, ptcl), 24);
+  return 0;
+}
+
 double oracle_shortrange_single(OracleSystem *s, int slice1, int slice2, const int *active, int n, int level) {
   return s->ShortRangeSingle(slice1, slice2, active, n, level);
 }

@@ -79,6 +79,7 @@ void oracle_system_get_path(OracleSystem *s, int copy, double *path);
 void oracle_system_set_mode(OracleSystem *s, int copy);
 /* InitRandomFixed (InitPaths.cc:966-999) from the World stream of `seed`. */
 int oracle_init_random_fixed(OracleSystem *s, uint64_t seed, double radius);
+int oracle_shift_data(OracleSystem *s, int slicesToShift);
 
 double oracle_shortrange_single(OracleSystem *s, int slice1, int slice2, const int *active,
                                 int n_active, int level);

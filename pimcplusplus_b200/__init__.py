@@ -186,6 +186,12 @@ _SIGS = {
     "pimc_batch_synchronize": (_i, [_p]),
     "pimc_batch_stream": (_p, [_p]),
     "pimc_shortrange_single_noalloc": (_i, [_p, _i, _i, _dp, _p, _d, _d, _i, _i, _i, _ip, _i, _i, _p, _p]),
+    "pimc_init_random_fixed": (_i, [_dp, _i, _d, C.c_uint64, _dp]),
+    "pimc_stream_uniform": (_i, [C.c_uint64, C.c_uint32, C.c_uint64, _dp]),
+    "pimc_shift_data": (_i, [_p, _i]),
+    "pimc_shift_move": (_i, [_p, _ip]),
+    "pimc_checkpoint_write": (_i, [_p, C.c_char_p]),
+    "pimc_checkpoint_read": (_i, [_p, C.c_char_p]),
 }
 for _name, (_res, _args) in _SIGS.items():
     _f = getattr(_lib, _name)
@@ -290,6 +296,27 @@ class PathData:
         out = np.empty((self.S, self.N, 3))
         self._check(_lib.pimc_get_path(self.h, copy, _dptr(out)), "get_path")
         return out
+
+    def seed(self, seed):
+        """Seeds every RNG stream of the chain (pimc_rng_seed)."""
+        self._check(_lib.pimc_rng_seed(self.h, C.c_uint64(seed)), "rng_seed")
+
+    def ShiftData(self, slices_to_shift):
+        """PathClass::ShiftPathData (PathClass.cc:1026-1110) on both copies."""
+        self._check(_lib.pimc_shift_data(self.h, int(slices_to_shift)), "shift_data")
+
+    def ShiftMove(self):
+        """ShiftMoveClass::MakeMove (MetaMoves.cc:39-65); returns the slices shifted."""
+        n = C.c_int()
+        self._check(_lib.pimc_shift_move(self.h, C.byref(n)), "shift_move")
+        return n.value
+
+    def write_checkpoint(self, filename):
+        """Both path copies, RNG stream positions and move counters, flat binary."""
+        self._check(_lib.pimc_checkpoint_write(self.h, os.fsencode(filename)), "checkpoint_write")
+
+    def read_checkpoint(self, filename):
+        self._check(_lib.pimc_checkpoint_read(self.h, os.fsencode(filename)), "checkpoint_read")
 
     # ---- pair actions ----
     def pa_david_from_dm(self, dm_path, num_offdiag_terms=0):
@@ -650,6 +677,25 @@ def coulomb_breakup(box, z1z2, smallest_beta, num_levels, num_knots, kcutoff, kv
         raise PimcError(rc, "pimc_coulomb_breakup")
     out["rmax"] = float(rmax[0])
     return out
+
+
+def init_random_fixed(box, num_particles, radius, seed):
+    """PathClass::InitRandomFixed (InitPaths.cc:966-999) positions [N][3] from
+    the World stream of `seed`; raises where the reference aborts."""
+    b = np.ascontiguousarray(box, dtype=np.float64)
+    out = np.zeros((int(num_particles), 3))
+    rc = _lib.pimc_init_random_fixed(_dptr(b), int(num_particles), float(radius), C.c_uint64(seed), _dptr(out))
+    if rc:
+        raise PimcError(rc, "InitRandomFixed: a particle took 1000 tries; decrease the excluded radius"
+                        if rc == 5 else "pimc_init_random_fixed")
+    return out
+
+
+def stream_uniform(seed, stream, index):
+    """Element `index` of the library's Philox stream `stream` under `seed`."""
+    out = C.c_double()
+    _lib.pimc_stream_uniform(C.c_uint64(seed), C.c_uint32(stream), C.c_uint64(index), C.byref(out))
+    return out.value
 
 
 def quintic_spline(h, y):

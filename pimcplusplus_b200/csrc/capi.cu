@@ -688,6 +688,8 @@ int pimc_rng_seed(pimc_context *ctx, uint64_t seed) {
   // concurrent schedule uses kStreamWindow0, the sequential chain kStreamLocal
   cs[0].stream = ctx->bis.schedule == PIMC_SCHEDULE_SEQUENTIAL ? kStreamLocal : kStreamWindow0;
   ctx->rounds = 0;
+  ctx->seed = seed;
+  ctx->shift_draws = 0;
   CK(cudaMemcpy(ctx->d_chain, cs.data(), cs.size() * sizeof(ChainState), cudaMemcpyHostToDevice));
   return PIMC_OK;
 }

@@ -182,6 +182,8 @@ struct pimc_context {
   bool bis_ready = false;
   pimc::ChainState *d_chain = nullptr;  // kMaxWindows states
   unsigned long long rounds = 0;         // concurrent-window rounds run so far
+  uint64_t seed = 0;                     // the key pimc_rng_seed set
+  unsigned long long shift_draws = 0;    // ShiftMove draws taken from stream 3
   pimc_move_record *d_trace = nullptr;
   size_t trace_cap = 0;
   int sm_count = 0;

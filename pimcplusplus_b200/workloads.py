@@ -209,3 +209,166 @@ def c3_chains(count, seed=0, steps_per_block=4, npts=1000, max_levels=4):
                         steps_per_block=steps_per_block, seed=(seed << 20) + 1000 + i,
                         grid=(r_min, float(box[0] / 2.0), npts), u00=u00, tau_pos=0, path=path, T=temp, rho=rho))
     return out
+
+
+# ---------------------------------------------------------------------------
+# PIMC++ input files (the reference's ASCII format) for these workloads.
+# ---------------------------------------------------------------------------
+def write_pair_action_david(path, dm_path, species_type="He", lam=HE4_LAMBDA, num_offdiag_terms=0):
+    """A DavidFit `.PairAction` file naming a squarer `.dm` file."""
+    from .iosection import IOSectionClass
+    io = IOSectionClass()
+    io.NewFile(path)
+    io.NewSection("Fits")
+    io.WriteVar("Type", "DavidFit")
+    io.WriteVar("NumOffDiagonalTerms", int(num_offdiag_terms))
+    for k, lm in (("Particle1", lam), ("Particle2", 0.0)):
+        io.NewSection(k)
+        io.WriteVar("Name", species_type)
+        io.WriteVar("lambda", float(lm))
+        io.WriteVar("Ndim", 3)
+        io.CloseSection()
+    io.WriteVar("Daviddmfile", dm_path)
+    io.CloseSection()
+    io.WriteFile(path)
+    return path
+
+
+def write_pair_action_tricubic(path, tabs, smallest_beta, species_type="He", lam=HE4_LAMBDA):
+    """A tricubicfit `.PairAction` file in the ASCII format, laid out as
+    PAtricubicFitClass::Read reads it: Particle1/2, a Spline Potential, and
+    Fits with q/y/t grids and one Fit section (beta, Umat, dUmat) per level."""
+    from .iosection import IOSectionClass
+    qg, yg, tg, umat, dumat, pot_grid, pot_data = tabs
+    io = IOSectionClass()
+    io.NewFile(path)
+    for k, lm in (("Particle1", lam), ("Particle2", 0.0)):
+        io.NewSection(k)
+        io.WriteVar("Name", species_type)
+        io.WriteVar("lambda", float(lm))
+        io.WriteVar("Ndim", 3)
+        io.CloseSection()
+    io.NewSection("Potential")
+    io.WriteVar("Type", "Spline")
+    io.NewSection("Grid")
+    io.WriteVar("Type", "Linear")
+    io.WriteVar("Start", float(pot_grid[0]))
+    io.WriteVar("End", float(pot_grid[1]))
+    io.WriteVar("NumPoints", int(pot_grid[2]))
+    io.CloseSection()
+    io.WriteVar("SplineData", np.asarray(pot_data, dtype=np.float64))
+    io.CloseSection()
+    io.NewSection("Fits")
+    io.WriteVar("Type", "tricubicfit")
+    for name, g in (("qGrid", qg), ("yGrid", yg), ("tGrid", tg)):
+        io.NewSection(name)
+        io.WriteVar("Type", "Linear")
+        io.WriteVar("Start", float(g[0]))
+        io.WriteVar("End", float(g[1]))
+        io.WriteVar("NumPoints", int(g[2]))
+        io.CloseSection()
+    for lev in range(umat.shape[0]):
+        io.NewSection("Fit")
+        io.WriteVar("beta", float(smallest_beta * 2.0 ** lev))
+        io.WriteVar("Umat", np.asarray(umat[lev], dtype=np.float64))
+        io.WriteVar("dUmat", np.asarray(dumat[lev], dtype=np.float64))
+        io.CloseSection()
+    io.CloseSection()
+    io.WriteFile(path)
+    return path
+
+
+def write_pimc_input(path, cfg, pair_action_files, seed, init=("RANDOMFIXED", 0.45 * LJ_SIGMA), num_images=0,
+                     steps_per_block=1, loop_steps=10, shift=False, observe_energy=False, species_type="He",
+                     lam=HE4_LAMBDA, use_density=False):
+    """A PIMC++ simulation input for one LJ-style chain of `cfg` (N, M, T, rho,
+    levels): System, Action (Kinetic + ShortRange), a BisectionBlock move
+    (and a ShiftMove), optional Energy observable, and an Algorithm loop."""
+    from .iosection import IOSectionClass
+    tau, box = derived(cfg)
+    io = IOSectionClass()
+    io.NewFile(path)
+    io.NewSection("Parallel")
+    io.WriteVar("ProcsPerClone", 1)
+    io.WriteVar("Seed", int(seed))
+    io.CloseSection()
+    io.NewSection("System")
+    io.WriteVar("tau", float(tau))
+    io.WriteVar("NumTimeSlices", int(cfg["M"]))
+    if use_density:
+        io.WriteVar("Box", np.ones(3))
+        io.WriteVar("Density", float(cfg["rho"]))
+    else:
+        io.WriteVar("Box", np.asarray(box, dtype=np.float64))
+    io.WriteVar("IsPeriodic", np.array([True, True, True]))
+    io.NewSection("Particles")
+    io.NewSection("Species")
+    io.WriteVar("Name", "He4")
+    io.WriteVar("Type", species_type)
+    io.WriteVar("lambda", float(lam))
+    io.WriteVar("Statistics", "BOLTZMANNON")
+    io.WriteVar("NumParticles", int(cfg["N"]))
+    io.WriteVar("NumDim", 3)
+    io.WriteVar("InitPaths", init[0])
+    if init[0] == "RANDOMFIXED":
+        io.WriteVar("Radius", float(init[1]))
+    elif init[0] == "FIXED":
+        io.WriteVar("Positions", np.asarray(init[1], dtype=np.float64))
+    else:
+        io.WriteVar("File", str(init[1]))
+    io.CloseSection()
+    io.CloseSection()
+    io.CloseSection()
+    io.NewSection("Action")
+    io.WriteVar("MaxLevels", int(cfg["levels"]) + 1)
+    io.WriteVar("NumImages", int(num_images))
+    io.WriteVar("PairActionFiles", np.array(list(pair_action_files), dtype=object))
+    for t, n in (("Kinetic", "Kinetic"), ("ShortRange", "ShortRange")):
+        io.NewSection("Action")
+        io.WriteVar("Type", t)
+        io.WriteVar("Name", n)
+        io.CloseSection()
+    io.CloseSection()
+    if observe_energy:
+        io.NewSection("Observables")
+        io.NewSection("Observable")
+        io.WriteVar("Type", "Energy")
+        io.WriteVar("Name", "Energy")
+        io.WriteVar("Frequency", 1)
+        io.CloseSection()
+        io.CloseSection()
+    io.NewSection("Moves")
+    io.NewSection("Move")
+    io.WriteVar("Type", "BisectionBlock")
+    io.WriteVar("Name", "BisectionBlock")
+    io.WriteVar("PermuteType", "NONE")
+    io.WriteVar("Species", "He4")
+    io.WriteVar("NumLevels", int(cfg["levels"]))
+    io.WriteVar("StepsPerBlock", int(steps_per_block))
+    io.WriteVar("SamplingActions", np.array(["ShortRange"], dtype=object))
+    io.WriteVar("HigherLevelActions", np.array(["ShortRange"], dtype=object))
+    io.CloseSection()
+    if shift:
+        io.NewSection("Move")
+        io.WriteVar("Type", "ShiftMove")
+        io.WriteVar("Name", "Shift")
+        io.CloseSection()
+    io.CloseSection()
+    io.NewSection("Algorithm")
+    io.NewSection("Loop")
+    io.WriteVar("Steps", int(loop_steps))
+    io.NewSection("Move")
+    io.WriteVar("Name", "BisectionBlock")
+    io.CloseSection()
+    if shift:
+        io.NewSection("Move")
+        io.WriteVar("Name", "Shift")
+        io.CloseSection()
+    if observe_energy:
+        io.NewSection("Observe")
+        io.WriteVar("Name", "Energy")
+        io.CloseSection()
+    io.CloseSection()
+    io.CloseSection()
+    io.WriteFile(path)
+    return path
