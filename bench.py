@@ -693,6 +693,8 @@ def run_c4(args, P, torch, flush, local, rank, world, agg):
     secs = ms32 / 1000.0 / args.steps
     achieved = ((st32["pair_evals"] / world / args.steps) * 72 +
                 r32["rhok_updates_per_s"] / world * secs * 32 * nk) / secs / 1e9
+    evals_per_launch = st32["pair_evals"] / world / (args.steps * rounds)
+    traffic = _traffic_per_launch("bisection_c4_traffic.json", evals_per_launch)
     return {
         "workload": f"jellium N={n}, r_s=4 bohr, beta=8 Ry^-1, M={m}, classical Coulomb action with optimized "
                     f"breakup (49 knots), {nk} k-vectors, bisection level {L}, concurrent windows, "
@@ -703,7 +705,9 @@ def run_c4(args, P, torch, flush, local, rank, world, agg):
                       "p99": float(np.quantile(rel, 0.99)) if rel.size else None, "stages": int(rel.size),
                       "flip_rate": sh["flips"] / max(1, sh["stages_attempted"])},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "traffic": None, "peak_kind": peak_kind,
+                     "traffic": traffic, "peak_kind": peak_kind, "evals_per_launch": evals_per_launch,
+                     "ms_per_launch": ms32 / (args.steps * rounds),
+                     "traffic_source": "profiles/bisection_c4_traffic.json (ncu, one launch) scaled by evals",
                      "kernel": "bisection_kernel<PA_COULOMB,float> with LongRange"},
         "_launches": 2 * args.steps * rounds,
     }
@@ -778,6 +782,7 @@ def run_c5(args, P, torch, flush, local, rank, world, agg):
                "ms_per_step": ms / args.steps}
         if proposals:
             out["redone_per_move"] = st["redone"] / st["moves"]
+        out["_per_launch"] = (st["pair_evals"] / world / (args.steps * rounds), ms / (args.steps * rounds))
         return out
 
     lists32 = timed(P.MIXED, args.c5_skin)
@@ -789,6 +794,21 @@ def run_c5(args, P, torch, flush, local, rank, world, agg):
     prop64 = timed(P.FP64, args.c5_skin, pp)
     progress("C5 proposals done")
     wide32 = timed(P.MIXED, args.c5_skin, args.c5_proposals_wide) if args.c5_proposals_wide else None
+    # roofline of the neighbour-list mixed kernel: 1-D FP32 pair eval = partner
+    # at two slices (24 B) + two spline cells (32 B); lists and bounds kernels
+    # are small beside it
+    evals_per_launch, ms_per_launch = lists32["_per_launch"]
+    peak, peak_kind = load_peaks()
+    achieved = evals_per_launch * 56 / (ms_per_launch / 1000.0) / 1e9
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                "traffic": _traffic_per_launch("bisection_c5_traffic.json", evals_per_launch),
+                "peak_kind": peak_kind, "bytes_per_eval": 56, "evals_per_launch": evals_per_launch,
+                "ms_per_launch": ms_per_launch,
+                "traffic_source": "profiles/bisection_c5_traffic.json (ncu, one launch) scaled by evals",
+                "kernel": "bisection_kernel<PA_DAVID,float>, windows, neighbour lists"}
+    for leg in (lists32, lists64, plain32, prop32, prop64, wide32):
+        if leg:
+            leg.pop("_per_launch", None)
     return {
         "workload": f"{n} LJ He-4, rho 0.02186/A^3, T=1 K, M={m}, LJ truncated/shifted at 2.5 sigma, level {L}, "
                     f"{m >> L} concurrent windows x {args.c5_cluster}-CTA clusters, {spb * rounds} moves per "
@@ -801,11 +821,21 @@ def run_c5(args, P, torch, flush, local, rank, world, agg):
         "mixed_over_fp64": lists32["accepted_moves_per_s"] / lists64["accepted_moves_per_s"],
         "proposals_over_one_per_window": prop32["accepted_moves_per_s"] / lists32["accepted_moves_per_s"],
         "proposals_mixed_over_fp64": prop32["accepted_moves_per_s"] / prop64["accepted_moves_per_s"],
-        "skin": args.c5_skin, "proposals": pp,
+        "skin": args.c5_skin, "proposals": pp, "roofline": roofline,
         # per round: one bisection launch per variant, plus the three neighbour
         # list kernels (bounds, fill, clear) of each variant with lists
         "_launches": (6 + 5 * 3 if args.c5_proposals_wide else 5 + 4 * 3) * args.steps * rounds,
     }
+
+
+def _traffic_per_launch(name, evals_per_launch):
+    """DRAM bytes of one launch: an ncu capture's bytes per pair evaluation
+    (profiles/<name>) times this run's pair evaluations per launch."""
+    prof = os.path.join(ROOT, "profiles", name)
+    if not os.path.exists(prof):
+        return None
+    with open(prof) as f:
+        return json.load(f).get("dram_bytes_per_pair_eval_mixed", 0) * evals_per_launch
 
 
 def nb_launches(schedule, blocks):

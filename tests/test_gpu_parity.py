@@ -397,3 +397,32 @@ def test_bisection_neighbor_lists_match_all_partner_oracle(tmp_path, schedule, s
                for r, _ in live)
     if skin >= 1.0:
         assert stats["pair_evals"] < 0.8 * full, (stats["pair_evals"], full)
+
+
+def test_shortrange_single_edge_cases(tmp_path):
+    """Empty and degenerate calls, repeated movers, the largest active list,
+    and the argument errors the reference would assert on."""
+    cfg, tau, box, dm = lj_case(tmp_path, n=80, m=16, levels=2, npts=400)
+    n, slices = cfg["N"], cfg["M"] + 1
+    o, d, _, _ = make_pair(n, slices, box, tau, W.HE4_LAMBDA, 61, 0.35)
+    o.set_pa(O.PairAction.from_dm(dm, tau, 0))
+    d.pa_david_from_dm(dm, 0)
+    sr, kin = P.ShortRangeClass(d), P.KineticClass(d)
+    assert sr.SingleAction(0, 8, [], 0) == 0.0 == o.shortrange_single(0, 8, [], 0)
+    assert kin.SingleAction(0, 8, [], 0) == 0.0
+    assert sr.SingleAction(5, 5, [1, 2], 0) == 0.0 == o.shortrange_single(5, 5, [1, 2], 0)
+    # a particle listed twice: DoPtcl leaves it visited, its partners are summed again
+    for act in ([3, 5, 3], [7, 7]):
+        ref = o.shortrange_single(0, 16, act, 1)
+        assert rel_err(sr.SingleAction(0, 16, act, 1), ref) <= REL64
+    # the largest active list, moved-moved pairs counted once, whole path
+    act = np.arange(64, dtype=np.int32)[::-1].copy()
+    for mode in (P.OLDMODE, P.NEWMODE):
+        d.SetMode(mode)
+        ref = o.shortrange_single(0, 16, act, 0, copy=mode)
+        assert rel_err(sr.SingleAction(0, 16, act, 0), ref) <= REL64
+    d.SetMode(P.OLDMODE)
+    for args in ((0, 8, [n], 0), (0, 8, [-1], 0), (0, 8, [1], 8), (0, slices, [1], 0), (4, 2, [1], 0),
+                 (0, 8, list(range(65)), 0)):
+        with pytest.raises(P.PimcError):
+            sr.SingleAction(*args)
