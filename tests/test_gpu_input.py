@@ -133,3 +133,79 @@ def test_tricubic_pair_action_file(tmp_path):
         ref = o.shortrange_single(s1, s2, act, lev)
         assert rel_err(sr.SingleAction(s1, s2, act, lev), ref) < 1e-12
     sim.close()
+
+
+JELLIUM_IN = """
+Section (Parallel) {{ int Seed = 5; }}
+Section (System)
+{{
+  double tau = {tau!r};
+  int NumTimeSlices = {m};
+  Array<double,1> Box(3) = [{L!r}, {L!r}, {L!r}];
+  Array<bool,1> IsPeriodic(3) = [true, true, true];
+  double kCutoff = 1.2;
+  Section (Particles)
+  {{
+    Section (Species)
+    {{
+      string Name = "e"; string Type = "e"; double lambda = 1.0; int NumParticles = {n}; int NumDim = 3;
+      string InitPaths = "FIXED";
+      Array<double,2> Positions({n},3) = [{pos}];
+    }}
+  }}
+}}
+Section (Action)
+{{
+  int MaxLevels = 3; int NumImages = 0;
+  Array<string,1> PairActionFiles(1) = ["ee.PairAction"];
+  bool UseLongRange = true; bool UseBackground = true; int NumBreakupKnots = 20;
+  Section (Action) {{ string Type = "Kinetic"; string Name = "Kinetic"; }}
+  Section (Action) {{ string Type = "ShortRange"; string Name = "ShortRange"; }}
+}}
+Section (Moves)
+{{
+  Section (Move)
+  {{
+    string Type = "BisectionBlock"; string Name = "Bisect"; string PermuteType = "NONE"; string Species = "e";
+    int NumLevels = 2; int StepsPerBlock = 2; Array<string,1> SamplingActions(1) = ["ShortRange"];
+  }}
+}}
+"""
+
+EE_PAIRACTION = """Section (Fits)
+{
+  string Type = "classical";
+  Section (Particle1) { string Name = "e"; double lambda = 1.0; int Ndim = 3; }
+  Section (Particle2) { string Name = "e"; double lambda = 1.0; int Ndim = 3; }
+  Section (Potential) { string Type = "Coulomb"; double Z1Z2 = 2.0; }
+}
+"""
+
+
+def test_jellium_input_matches_direct_setup(tmp_path):
+    """A classical Coulomb PairAction with the long-range breakup, set up from
+    an input file, against the same chain built through PathData directly."""
+    n, m, tau = 16, 16, 0.125
+    L = (4.0 * math.pi / 3.0 * n) ** (1.0 / 3.0) * 4.0
+    box = np.array([L, L, L])
+    pos = (np.random.default_rng(3).random((n, 3)) - 0.5) * L
+    (tmp_path / "ee.PairAction").write_text(EE_PAIRACTION)
+    inp = tmp_path / "jellium.in"
+    inp.write_text(JELLIUM_IN.format(tau=tau, m=m, L=float(L), n=n,
+                                     pos=", ".join(repr(float(x)) for x in pos.reshape(-1))))
+    sim = Simulation(str(inp), device=0)
+    assert sim.use_longrange and "LongRange" in sim.actions
+    d = P.PathData(n, m + 1, box, tau, 1.0, 0, device=0)
+    d.pa_coulomb(2.0, 3)
+    assert d.setup_kvecs(1.2) == sim.path_data.num_k
+    d.longrange_coulomb(20, True)
+    d.set_path(np.broadcast_to(pos, (m + 1, n, 3)).copy())
+    assert sim.path_data.energy() == d.energy()
+    bb = P.BisectionBlock(d, 2, 2, shortrange_at_higher_levels=False, use_longrange=True)
+    bb.seed(5)
+    want, _ = bb.MakeMoves(6)
+    got, _ = sim.moves["Bisect"].MakeMoves(6)
+    assert np.array_equal(got, want)
+    assert np.array_equal(sim.path_data.get_path(0), d.get_path(0))
+    d.close()
+    sim.close()
