@@ -1,0 +1,111 @@
+"""The oracle's composition of the action sums, pinned against a second,
+independent numpy statement of the reference's formulas (no shared code with
+the oracle beyond the spline tables it is given):
+
+* PathClass::DistDisp (PIMC++/src/PathClass.h:696-746): dispA by nearbyint
+  minimum image, dispB on the image consistent with dispA;
+* MultiCubicSpline::operator()(i, x) (Common/Splines/CubicSpline.h:470-501)
+  with LinearGrid::ReverseMap (Grid.h:81-84) and the [0, N-2] clamp;
+* DavidPAClass::calcUsqzFast without off-diagonal terms (DavidPAClass.cc:468-489);
+* ShortRangeClass::SingleAction (PIMC++/src/Actions/ShortRangeClass.cc:191-236)
+  with DoPtcl's count-once rule over links [slice1, slice2) step 2^level;
+* KineticClass::SingleAction (PIMC++/src/Actions/KineticClass.cc:33-90) with
+  PathClass::Velocity's PutInBox (PathClass.h:831-865) and the image sums.
+"""
+import numpy as np
+import pytest
+
+import oracle as O
+from helpers import lj_case, random_walk_path
+from pimcplusplus_b200 import workloads as W
+
+
+def spline_eval(start, end, n, y, d2y, x):
+    delta = (end - start) / (n - 1)
+    hi = np.rint((x - start) / delta - 0.5).astype(np.int64) + 1
+    lo = hi - 1
+    lo = np.where(lo < 0, 0, lo)
+    hi = np.where(lo == 0, np.maximum(hi, 1), hi)
+    over = hi > n - 1
+    hi = np.where(over, n - 1, hi)
+    lo = np.where(over, n - 2, lo)
+    xs = start + np.arange(n) * delta
+    h = xs[hi] - xs[lo]
+    a = (xs[hi] - x) / h
+    b = (x - xs[lo]) / h
+    return a * y[lo] + b * y[hi] + ((a ** 3 - a) * d2y[lo] + (b ** 3 - b) * d2y[hi]) * (h * h / 6.0)
+
+
+def dist_disp(pa1, pa2, pb1, pb2, box):
+    dA = pa2 - pa1
+    dB = pb2 - pb1
+    dA = dA + (-np.rint(dA / box)) * box
+    dB = dB + np.rint((dA - dB) / box) * box
+    return np.sqrt(np.sum(dA * dA, -1)), np.sqrt(np.sum(dB * dB, -1))
+
+
+def shortrange_single(path, box, active, s1, s2, level, grid, y, d2y):
+    start, end, n = grid
+    skip = 1 << level
+    N = path.shape[1]
+    total = 0.0
+    visited = np.zeros(N, dtype=bool)
+    for p1 in active:
+        visited[p1] = True
+        partners = np.nonzero(~visited)[0]
+        for s in range(s1, s2, skip):
+            r, rp = dist_disp(path[s, p1], path[s, partners], path[s + skip, p1], path[s + skip, partners], box)
+            r = np.minimum(r, end)
+            rp = np.minimum(rp, end)
+            low = (r < start) | (rp < start)
+            u = 0.5 * (spline_eval(start, end, n, y, d2y, r) + spline_eval(start, end, n, y, d2y, rp))
+            u = np.where(low, spline_eval(start, end, n, y, d2y, np.array([start]))[0], u)
+            total += float(np.sum(u))
+    return total
+
+
+def kinetic_single(path, box, active, s1, s2, level, lam, tau, num_images):
+    skip = 1 << level
+    f = 1.0 / (4.0 * lam * tau * skip)
+    total = 0.0
+    for p in active:
+        for s in range(s1, s2, skip):
+            v = path[s + skip, p] - path[s, p]
+            v = v - np.floor(v / box + 0.5) * box
+            imgs = np.arange(-num_images, num_images + 1)[:, None] * box[None, :]
+            total -= np.log(np.prod(np.sum(np.exp(-(v[None, :] + imgs) ** 2 * f), axis=0)))
+    return total
+
+
+def test_oracle_shortrange_composition(tmp_path):
+    cfg, tau, box, dm = lj_case(tmp_path, n=24, m=16, levels=3, npts=400)
+    n, slices = cfg["N"], cfg["M"] + 1
+    pa = O.PairAction.from_dm(dm, tau, 0)
+    info = pa.info()
+    o = O.System(n, slices, box, tau, W.HE4_LAMBDA, 0)
+    o.set_pa(pa)
+    rng = np.random.default_rng(4)
+    for trial in range(3):
+        path = random_walk_path(n, slices, box, 0.35, seed=70 + trial, far=0.2)
+        o.set_path(path)
+        for s1, s2, level, active in ((0, 16, 0, [5]), (4, 12, 1, [2, 9, 2]), (0, 16, 2, list(rng.permutation(n)[:6])),
+                                      (8, 16, 3, [0, 23])):
+            y = pa.table(0, level)[:, 1]
+            d2y = pa.table(1, level)[:, 1]
+            grid = (info["grid_start"], info["grid_end"], info["num_grid"])
+            want = shortrange_single(path, box, active, s1, s2, level, grid, y, d2y)
+            got = o.shortrange_single(s1, s2, np.array(active, dtype=np.int32), level)
+            assert abs(got - want) <= 1e-12 * max(1.0, abs(want)), (trial, s1, s2, level, active, got, want)
+
+
+@pytest.mark.parametrize("num_images", [0, 1])
+def test_oracle_kinetic_composition(num_images):
+    n, slices, tau, lam = 10, 17, 0.02, 6.0596
+    box = np.array([6.0, 7.0, 8.0])
+    o = O.System(n, slices, box, tau, lam, num_images)
+    path = random_walk_path(n, slices, box, 0.5, seed=3, far=0.3)
+    o.set_path(path)
+    for s1, s2, level, active in ((0, 16, 0, [1]), (2, 10, 1, [0, 4]), (0, 16, 3, [9, 3, 5])):
+        want = kinetic_single(path, box, active, s1, s2, level, lam, tau, num_images)
+        got = o.kinetic_single(s1, s2, np.array(active, dtype=np.int32), level)
+        assert abs(got - want) <= 1e-12 * max(1.0, abs(want)), (s1, s2, level, active, got, want)
