@@ -109,3 +109,45 @@ def test_oracle_kinetic_composition(num_images):
         want = kinetic_single(path, box, active, s1, s2, level, lam, tau, num_images)
         got = o.kinetic_single(s1, s2, np.array(active, dtype=np.int32), level)
         assert abs(got - want) <= 1e-12 * max(1.0, abs(want)), (s1, s2, level, active, got, want)
+
+
+def shortrange_dbeta(path, box, s1, s2, level, grid, tabs):
+    """ShortRangeClass::d_dBeta (ShortRangeClass.cc:316-355) over all pairs
+    p2 < p1 with DavidPAClass::calcUsqz's diagonal part (DavidPAClass.cc:291-366):
+    r, r' clamped to [rmin, End], dU = ½(du₁(r)+du₁(r')) + ½(V(r)+V(r')), V the column 0."""
+    start, end, n = grid
+    (uy, ud2), (dy, dd2) = tabs
+    skip = 1 << level
+    N = path.shape[1]
+    total = 0.0
+    for p1 in range(N):
+        p2 = np.arange(p1)
+        if p2.size == 0:
+            continue
+        for s in range(s1, s2, skip):
+            r, rp = dist_disp(path[s, p1], path[s, p2], path[s + skip, p1], path[s + skip, p2], box)
+            r = np.clip(r, start, end)
+            rp = np.clip(rp, start, end)
+            v = 0.5 * (spline_eval(start, end, n, uy[:, 0], ud2[:, 0], r) +
+                       spline_eval(start, end, n, uy[:, 0], ud2[:, 0], rp))
+            du = 0.5 * (spline_eval(start, end, n, dy[:, 1], dd2[:, 1], r) +
+                        spline_eval(start, end, n, dy[:, 1], dd2[:, 1], rp))
+            total += float(np.sum(du + v))
+    return total
+
+
+def test_oracle_shortrange_dbeta_composition(tmp_path):
+    cfg, tau, box, dm = lj_case(tmp_path, n=20, m=16, levels=2, npts=400)
+    n, slices = cfg["N"], cfg["M"] + 1
+    pa = O.PairAction.from_dm(dm, tau, 0)
+    info = pa.info()
+    grid = (info["grid_start"], info["grid_end"], info["num_grid"])
+    o = O.System(n, slices, box, tau, W.HE4_LAMBDA, 0)
+    o.set_pa(pa)
+    path = random_walk_path(n, slices, box, 0.35, seed=91, far=0.2)
+    o.set_path(path)
+    for s1, s2, level in ((0, 16, 0), (4, 12, 1), (0, 16, 2)):
+        tabs = ((pa.table(0, level), pa.table(1, level)), (pa.table(2, level), pa.table(3, level)))
+        want = shortrange_dbeta(path, box, s1, s2, level, grid, tabs)
+        got = o.shortrange_dbeta(s1, s2, level)
+        assert abs(got - want) <= 1e-12 * max(1.0, abs(want)), (s1, s2, level, got, want)
