@@ -329,6 +329,13 @@ class PathData:
         self._check(_lib.pimc_pa_david(self.h, 0, 0, grid_type, grid_start, grid_end, ng, nc, nt, _dptr(ukj),
                                        _dptr(dukj), tau_pos, num_offdiag_terms), "pa_david")
 
+    def pa_zero(self, num_levels):
+        """PAzeroFitClass (Common/PairAction/PAzeroFit.cc): U = dU = V = 0, as a
+        DavidPA table of zeros on a two-point grid, so the sums are exactly zero."""
+        end = float(np.sqrt(np.sum(self.box * self.box)))
+        z = np.zeros((int(num_levels), 2, 2))
+        self.pa_david(GRID_LINEAR, 0.0, end, z, z, 0, 0)
+
     def pa_tricubic(self, qgrid, ygrid, tgrid, smallest_beta, umat, dumat, pot_grid, pot_data):
         umat = np.ascontiguousarray(umat, dtype=np.float64)
         dumat = np.ascontiguousarray(dumat, dtype=np.float64)

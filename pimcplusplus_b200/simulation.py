@@ -12,8 +12,8 @@ the device objects behind them:
   MaxLevels, NumImages, the `Action` sections of type Kinetic and
   ShortRange, PairActionFiles read by ReadPAFit
   (Common/PairAction/PAFit.h:30-72) with fit types "DavidFit"
-  (Daviddmfile, NumOffDiagonalTerms), "tricubicfit" (an ASCII fit file) and
-  "classical" (a Coulomb potential), and the long-range breakup when the
+  (Daviddmfile, NumOffDiagonalTerms), "tricubicfit" (an ASCII fit file),
+  "classical" (a Coulomb potential) and "zerofit", and the long-range breakup when the
   system has a kCutoff and UseLongRange is true (UseBackground,
   NumBreakupKnots).
 * `Moves`   -> BisectionBlockClass::Read (PIMC++/src/Moves/BisectionBlock.cc:27-128)
@@ -138,9 +138,14 @@ def read_pair_action(filename, smallest_beta, num_levels):
         io.CloseSection()
         out["umat"] = np.stack(umats)
         out["dumat"] = np.stack(dumats)
+    elif ftype == "zerofit":
+        # PAzeroFitClass::Read (Common/PairAction/PAzeroFit.cc:43-66): particles only
+        io.OpenSection("Fits")
+        particles()
+        io.CloseSection()
     else:
         raise _err(f"pair action fit type {ftype!r} is not on this library's path "
-                   "(DavidFit, tricubicfit, classical)", filename)
+                   "(DavidFit, tricubicfit, classical, zerofit)", filename)
     return out
 
 
@@ -345,6 +350,8 @@ class Simulation:
                 d.pa_david_from_dm(pa["Daviddmfile"], pa["NumOffDiagonalTerms"])
             elif pa["type"] == "classical":
                 d.pa_coulomb(pa["Z1Z2"], self.max_levels)
+            elif pa["type"] == "zerofit":
+                d.pa_zero(self.max_levels)
             else:
                 q, y, t = pa["grids"]
                 d.pa_tricubic(q, y, t, self.tau, pa["umat"], pa["dumat"], pa["pot_grid"], pa["pot_data"])

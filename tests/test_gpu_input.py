@@ -209,3 +209,38 @@ def test_jellium_input_matches_direct_setup(tmp_path):
     assert np.array_equal(sim.path_data.get_path(0), d.get_path(0))
     d.close()
     sim.close()
+
+
+ZERO_PAIRACTION = """Section (Fits)
+{
+  string Type = "zerofit";
+  Section (Particle1) { string Name = "He"; double lambda = 6.0596; int Ndim = 3; }
+  Section (Particle2) { string Name = "He"; double lambda = 0.0; int Ndim = 3; }
+}
+"""
+
+
+def test_zerofit_input_is_free_particles(tmp_path):
+    """PAzeroFitClass: the ShortRange sums are exactly zero and the chain is
+    the kinetic-only chain of the oracle with a zero table."""
+    cfg = dict(N=12, M=16, T=2.0, rho=0.02186, levels=2)
+    tau, box = W.derived(cfg)
+    (tmp_path / "zero.PairAction").write_text(ZERO_PAIRACTION)
+    path = W.write_pimc_input(str(tmp_path / "z.in"), cfg, ["zero.PairAction"], 9, loop_steps=5, steps_per_block=2)
+    sim = Simulation(path, device=0)
+    sim.run()
+    o = O.System(12, 17, box, tau, W.HE4_LAMBDA, 0)
+    z = np.zeros((3, 2, 2))
+    pa = O.PairAction.david_arrays(0.0, float(np.sqrt(np.sum(box * box))), z, z, 0, 0)
+    o.set_pa(pa)
+    o.init_random_fixed(9, 0.45 * W.LJ_SIGMA)
+    o.bisection_config(2, 2, True)
+    o.rng_seed(9)
+    recs = o.run_bisection(5)
+    st = sim.moves["BisectionBlock"].stats()
+    assert st["moves"] == 10 and st["accepted"] == sum(r.accepted for r in recs)
+    assert np.max(np.abs(sim.path_data.get_path(0) - o.get_path(0))) < 1e-9
+    sr = sim.actions["ShortRange"]
+    assert sr.SingleAction(0, 16, [1, 4], 0) == 0.0
+    assert sr.d_dBeta(0, 16, 0) == 0.0
+    sim.close()

@@ -155,9 +155,15 @@ def test_pair_action_files(tmp_path):
         '  Section (Potential) { string Type = "Coulomb"; double Z1Z2 = 2.0; } }\n')
     pa = read_pair_action(str(tmp_path / "ee.PairAction"), 0.1, 3)
     assert pa["type"] == "classical" and pa["Z1Z2"] == 2.0
-    (tmp_path / "z.PairAction").write_text('Section (Fits) { string Type = "zerofit"; }')
-    with pytest.raises(InputError, match="zerofit"):
-        read_pair_action(str(tmp_path / "z.PairAction"), 0.1, 3)
+    (tmp_path / "z.PairAction").write_text(
+        'Section (Fits) { string Type = "zerofit";\n'
+        '  Section (Particle1) { string Name = "p"; double lambda = 1.0; int Ndim = 3; }\n'
+        '  Section (Particle2) { string Name = "p"; double lambda = 1.0; int Ndim = 3; } }\n')
+    pa = read_pair_action(str(tmp_path / "z.PairAction"), 0.1, 3)
+    assert pa["type"] == "zerofit" and pa["Particle2"]["Name"] == "p"
+    (tmp_path / "bc.PairAction").write_text('Section (Fits) { string Type = "coulombBCfit"; }')
+    with pytest.raises(InputError, match="coulombBCfit"):
+        read_pair_action(str(tmp_path / "bc.PairAction"), 0.1, 3)
 
 
 def _input(tmp_path, **kw):
