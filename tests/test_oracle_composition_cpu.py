@@ -151,3 +151,43 @@ def test_oracle_shortrange_dbeta_composition(tmp_path):
         want = shortrange_dbeta(path, box, s1, s2, level, grid, tabs)
         got = o.shortrange_dbeta(s1, s2, level)
         assert abs(got - want) <= 1e-12 * max(1.0, abs(want)), (s1, s2, level, got, want)
+
+
+def longrange_single(path, kv, s1, s2, level, ulong_k, ulong_r0, ushort_k0, ulong_k0, use_background):
+    """LongRangeClass::SingleAction (LongRangeClass.cc:273-371), one species:
+    rho_k(slice) = sum_i exp(i k.r_i) computed directly (CalcRho_ks_Fast builds
+    the same phases by recurrence), ends of [slice1, slice2] weighted 1/2."""
+    skip = 1 << level
+    N = path.shape[1]
+    homo = background = k0 = 0.0
+    for s in range(s1, s2 + 1, skip):
+        f = 0.5 if s in (s1, s2) else 1.0
+        rho = np.exp(1j * (path[s] @ kv.T)).sum(axis=0)
+        homo += f * 0.5 * 2.0 * float(np.sum(np.abs(rho) ** 2 * ulong_k[level]))
+        homo -= f * 0.5 * N * ulong_r0[level]
+        background -= f * 0.5 * N * N * ushort_k0[level]
+        k0 += f * 0.5 * N * N * ulong_k0[level]
+    return homo + (background if use_background else k0)
+
+
+@pytest.mark.parametrize("use_background", [True, False])
+def test_oracle_longrange_composition(use_background):
+    n, m, levels = 12, 16, 3
+    box = np.array([7.0, 8.0, 9.0])
+    o = O.System(n, m + 1, box, 0.05, 0.5, 0)
+    pa = O.PairAction.classical_coulomb(0.05, levels, 2.0)  # IsLongRange: the k sum is taken
+    o.set_pa(pa)
+    path = random_walk_path(n, m + 1, box, 0.4, seed=17, far=0.2)
+    o.set_path(path)
+    nk = o.setup_kvecs(2.2)
+    kv, _ = o.kvecs()
+    rng = np.random.default_rng(5)
+    tabs = dict(ulong_k=rng.normal(size=(levels, nk)), ulong_r0=rng.normal(size=levels),
+                ushort_k0=rng.normal(size=levels), ulong_k0=rng.normal(size=levels))
+    o.set_longrange(tabs["ulong_k"], tabs["ulong_r0"], tabs["ushort_k0"], tabs["ulong_k0"],
+                    np.zeros((levels, nk)), np.zeros(levels), np.zeros(levels), np.zeros(levels), use_background)
+    o.calc_rhok_all()
+    for s1, s2, level in ((0, 8, 0), (4, 12, 1), (0, 16, 2)):
+        want = longrange_single(path, kv, s1, s2, level, use_background=use_background, **tabs)
+        got = o.longrange_single(s1, s2, np.array([3], dtype=np.int32), level)
+        assert abs(got - want) <= 1e-11 * max(1.0, abs(want)), (s1, s2, level, got, want)
