@@ -622,7 +622,7 @@ def run_c4(args, P, torch, flush, local, rank, world, agg):
     box = np.array([boxl] * 3)
     tau = 8.0 / m
     start = initial_path(n, m + 1, box, 41 + rank, 0.0)
-    spb = 16
+    spb = args.c4_steps_per_block
 
     def make(precision, shadow=False, schedule=None):
         d = P.PathData(n, m + 1, box, tau, 1.0, 0, device=local)
@@ -728,7 +728,7 @@ def run_c5(args, P, torch, flush, local, rank, world, agg):
     tau, box = W.derived(cfg)
     n, m, L = cfg["N"], cfg["M"], cfg["levels"]
     dm = W.make_dm_for(cfg, tempfile.mkdtemp())
-    spb = 16
+    spb = args.c5_steps_per_block
     start = W.lattice_path(n, m + 1, box, np.random.default_rng(5 + rank))
 
     def make(precision, skin, path, proposals=0):
@@ -868,6 +868,8 @@ def main():
     ap.add_argument("--c5-proposals-wide", type=int, default=16, help="a second proposals shape (0: none)")
     ap.add_argument("--c5-prop-threads", type=int, default=512)
     ap.add_argument("--c4-cluster", type=int, default=8)
+    ap.add_argument("--c4-steps-per-block", type=int, default=16)
+    ap.add_argument("--c5-steps-per-block", type=int, default=16)
     ap.add_argument("--c3-chains", type=int, default=1024)
     ap.add_argument("--c3-blocks", type=int, default=4)
     ap.add_argument("--c3-steps-per-block", type=int, default=4)
