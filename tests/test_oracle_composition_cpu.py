@@ -12,6 +12,8 @@ the oracle beyond the spline tables it is given):
 * KineticClass::SingleAction (PIMC++/src/Actions/KineticClass.cc:33-90) with
   PathClass::Velocity's PutInBox (PathClass.h:831-865) and the image sums.
 """
+import math
+
 import numpy as np
 import pytest
 
@@ -191,3 +193,52 @@ def test_oracle_longrange_composition(use_background):
         want = longrange_single(path, kv, s1, s2, level, use_background=use_background, **tabs)
         got = o.longrange_single(s1, s2, np.array([3], dtype=np.int32), level)
         assert abs(got - want) <= 1e-11 * max(1.0, abs(want)), (s1, s2, level, got, want)
+
+
+def log_spline_eval(r0, spacing, n, y, d2y, x):
+    """MultiCubicSpline::operator()(col, x) on a LogGrid: nodes r0·spacing^i,
+    ReverseMap floor(log(x/r0)/log(spacing)) (Grid.h:527-530), cell clamped."""
+    xs = np.array([r0 * spacing ** i for i in range(n)])
+    lo = int(math.floor(math.log(x / r0) / math.log(spacing)))
+    lo = min(max(lo, 0), n - 2)
+    hi = lo + 1
+    h = xs[hi] - xs[lo]
+    a = (xs[hi] - x) / h
+    b = (x - xs[lo]) / h
+    return a * y[lo] + b * y[hi] + ((a ** 3 - a) * d2y[lo] + (b ** 3 - b) * d2y[hi]) * (h * h / 6.0)
+
+
+def david_U(q, z, s, level_tables, r0, spacing, n, end, num_terms):
+    """DavidPAClass::calcUsqzFast (DavidPAClass.cc:468-511) with off-diagonal
+    terms u_kj(q) z^{2j} s^{2(k-j)}, column k(k+1)/2 + j + 1."""
+    y, d2y = level_tables
+    col = lambda c, x: log_spline_eval(r0, spacing, n, y[:, c], d2y[:, c], x)
+    r, rp = min(q + 0.5 * z, end), min(q - 0.5 * z, end)
+    if rp < r0 or r < r0:
+        return col(1, r0)
+    U = 0.5 * (col(1, r) + col(1, rp))
+    if s > 0.0 and q < end:
+        for k in range(1, num_terms + 1):
+            for j in range(k + 1):
+                U += col(k * (k + 1) // 2 + j + 1, q) * z ** (2 * j) * s ** (2 * (k - j))
+    return U
+
+
+def test_oracle_david_offdiagonal_log_grid(tmp_path):
+    from helpers import write_testcoul_dm
+    tau = 1.0 / 64
+    pa = O.PairAction.from_dm(write_testcoul_dm(str(tmp_path / "tc.dm")), tau, 2)
+    info = pa.info()
+    assert info["grid_type"] == 1
+    n, r0, end = info["num_grid"], info["grid_start"], info["grid_end"]
+    spacing = (end / r0) ** (1.0 / (n - 1))
+    rng = np.random.default_rng(12)
+    for level in range(3):
+        tabs = (pa.table(0, level), pa.table(1, level))
+        for _ in range(150):
+            q = rng.uniform(0.5 * r0, 1.1 * end)
+            z = rng.uniform(-1.0, 1.0) * min(q, 2.0)
+            s = abs(z) + rng.uniform(0.0, 1.0)
+            want = david_U(q, z, s, tabs, r0, spacing, n, end, 2)
+            got = pa.U(q, z, s * s, level)
+            assert abs(got - want) <= 1e-11 * max(1.0, abs(want)), (level, q, z, s, got, want)
