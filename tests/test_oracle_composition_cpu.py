@@ -242,3 +242,71 @@ def test_oracle_david_offdiagonal_log_grid(tmp_path):
             want = david_U(q, z, s, tabs, r0, spacing, n, end, 2)
             got = pa.U(q, z, s * s, level)
             assert abs(got - want) <= 1e-11 * max(1.0, abs(want)), (level, q, z, s, got, want)
+
+
+def kinetic_dbeta(path, box, s1, s2, level, lam, tau, num_images):
+    """KineticClass::d_dBeta (KineticClass.cc:187-256): 3/(2 τ_l) per link plus
+    the image-summed spring term Σ_dim (∂ ln Z_dim) of each link."""
+    skip = 1 << level
+    lt = tau * skip
+    f = 1.0 / (4.0 * lam * lt)
+    spring = 0.0
+    imgs = np.arange(-num_images, num_images + 1)
+    for p in range(path.shape[1]):
+        for s in range(s1, s2, skip):
+            spring += 1.5 / lt
+            v = path[s + skip, p] - path[s, p]
+            v = v - np.floor(v / box + 0.5) * box
+            d = v[:, None] + imgs[None, :] * box[:, None]
+            e = np.exp(-d * d * f)
+            gauss = e.sum(axis=1)
+            num = (-(d * d * f) / lt * e).sum(axis=1)
+            spring += sum(num[k] * np.prod(np.delete(gauss, k)) for k in range(3)) / np.prod(gauss)
+    return spring
+
+
+@pytest.mark.parametrize("num_images", [0, 1])
+def test_oracle_kinetic_dbeta_composition(num_images):
+    n, slices, tau, lam = 10, 17, 0.02, 6.0596
+    box = np.array([6.0, 7.0, 8.0])
+    o = O.System(n, slices, box, tau, lam, num_images)
+    path = random_walk_path(n, slices, box, 0.5, seed=8, far=0.3)
+    o.set_path(path)
+    for s1, s2, level in ((0, 16, 0), (4, 12, 1), (0, 16, 2)):
+        want = kinetic_dbeta(path, box, s1, s2, level, lam, tau, num_images)
+        got = o.kinetic_dbeta(s1, s2, level)
+        assert abs(got - want) <= 1e-11 * max(1.0, abs(want)), (s1, s2, level, got, want)
+
+
+def test_oracle_energy_composition(tmp_path):
+    """ActionsClass::Energy (ActionsClass.cc:812-871) as EnergyClass::Accumulate
+    sums it (ObservableEnergy.cc:31-73): kinetic and dUShort over links [0, M),
+    vShort = ShortRangePotClass::V summed over slices with ½ at 0 and M
+    (ShortRangePotClass.cc:28-47; one-slice DistDisp, PathClass.h:636-662;
+    DavidPAClass::V = column 0 of the first tau table, r clamped to the grid)."""
+    cfg, tau, box, dm = lj_case(tmp_path, n=14, m=16, levels=2, npts=400)
+    n, S = cfg["N"], cfg["M"] + 1
+    M = S - 1
+    pa = O.PairAction.from_dm(dm, tau, 0)
+    info = pa.info()
+    grid = (info["grid_start"], info["grid_end"], info["num_grid"])
+    o = O.System(n, S, box, tau, W.HE4_LAMBDA, 0)
+    o.set_pa(pa)
+    path = random_walk_path(n, S, box, 0.35, seed=29, far=0.2)
+    o.set_path(path)
+    e = o.energy()
+    kin = kinetic_dbeta(path, box, 0, M, 0, W.HE4_LAMBDA, tau, 0)
+    tabs = ((pa.table(0, 0), pa.table(1, 0)), (pa.table(2, 0), pa.table(3, 0)))
+    dus = shortrange_dbeta(path, box, 0, M, 0, grid, tabs)
+    v = 0.0
+    y0, d2y0 = pa.table(0, 0)[:, 0], pa.table(1, 0)[:, 0]
+    for s in range(S):
+        f = 0.5 if s in (0, M) else 1.0
+        for p1 in range(n):
+            d = path[s, :p1] - path[s, p1]
+            d = d - np.rint(d / box) * box
+            r = np.clip(np.sqrt(np.sum(d * d, axis=1)), grid[0], grid[1])
+            v += f * float(np.sum(spline_eval(*grid, y0, d2y0, r)))
+    for got, want in ((e["kinetic"], kin), (e["du_short"], dus), (e["v_short"], v),
+                      (e["total"], (kin + dus) / M)):
+        assert abs(got - want) <= 1e-11 * max(1.0, abs(want)), (got, want)
