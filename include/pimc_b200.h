@@ -162,7 +162,8 @@ int pimc_shift_move(pimc_context *ctx, int *slices_shifted);
  * checks that N, slices, box, tau and lambda equal the context's
  * (PIMC_E_ARG otherwise, PIMC_E_FILE for a missing or malformed file); a
  * chain continued from its checkpoint makes the same moves as the chain
- * that wrote it. */
+ * that wrote it.  Read it after pimc_bisection_setup and pimc_rng_seed: setup
+ * clears the move counters and seeding resets the streams. */
 int pimc_checkpoint_write(pimc_context *ctx, const char *filename);
 int pimc_checkpoint_read(pimc_context *ctx, const char *filename);
 

@@ -110,6 +110,7 @@ class PathData {
   void WriteCheckpoint(const std::string &file) const {
     check(pimc_checkpoint_write(ctx_, file.c_str()), "pimc_checkpoint_write");
   }
+  /* After BisectionBlockClass set-up and Seed, which clear the counters and streams it restores. */
   void ReadCheckpoint(const std::string &file) { check(pimc_checkpoint_read(ctx_, file.c_str()), "pimc_checkpoint_read"); }
 
   /* PathClass::SetupkVecs3D and the Coulomb breakup of LongRangeClass::Init. */
