@@ -316,6 +316,8 @@ class PathData:
         self._check(_lib.pimc_checkpoint_write(self.h, os.fsencode(filename)), "checkpoint_write")
 
     def read_checkpoint(self, filename):
+        """Restores a chain written by write_checkpoint; call it after the
+        BisectionBlock is set up and seeded (both reset what it restores)."""
         self._check(_lib.pimc_checkpoint_read(self.h, os.fsencode(filename)), "checkpoint_read")
 
     # ---- pair actions ----
