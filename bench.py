@@ -386,7 +386,8 @@ def run_ours(args):
     rec, sh = bb.MakeMoves(max(1, args.accuracy_moves // args.steps_per_block), trace=True)
     d.close()
     m = rec["dS_shadow"] != 0.0
-    rel = np.abs(rec["dS"][m] - rec["dS_shadow"][m]) / np.abs(rec["dS_shadow"][m])
+    absd = np.abs(rec["dS"][m] - rec["dS_shadow"][m])
+    rel = absd / np.abs(rec["dS_shadow"][m])
     flip_rate = sh["flips"] / max(1, sh["stages_attempted"])
 
     # end to end through the public API: host path in, moves, path + counters out
@@ -464,7 +465,11 @@ def run_ours(args):
             "dS_relerr": {"median": float(np.median(rel)) if rel.size else None,
                           "p99": float(np.quantile(rel, 0.99)) if rel.size else None,
                           "max": float(np.max(rel)) if rel.size else None, "stages": int(rel.size),
-                          "flip_rate": flip_rate},
+                          "flip_rate": flip_rate,
+                          # the relative error is large only where dS itself is near 0;
+                          # the absolute error is what moves a Metropolis decision
+                          "abs_median": float(np.median(absd)) if absd.size else None,
+                          "abs_max": float(np.max(absd)) if absd.size else None},
             "e2e": {"value": e2e_evals_timed / e2e_t if e2e_t else None, "unit": UNIT,
                     "h2d_bytes_per_step": path_bytes, "d2h_bytes_per_step": path_bytes + 48},
             "gpu_launches": args.steps * 2 * nb_launches(args.schedule, blocks),
