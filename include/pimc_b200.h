@@ -419,8 +419,9 @@ int pimc_gofr_reset(pimc_context *ctx);
 /* ---- allocation-free ShortRange SingleAction ----
  * No counterpart in the reference: it exists for callers that cannot call
  * cudaMalloc (an application whose memory pool owns every device
- * allocation, an embedding that forbids allocation after start-up, code
- * running while a stream is being captured).  It needs no context: every
+ * allocation, an embedding that forbids allocation after start-up, a
+ * latency-critical loop that must not pay for cudaMalloc's implicit device
+ * synchronisation).  It needs no context: every
  * buffer is the caller's device memory — path [num_time_slices][N][3]
  * doubles, diag the (y, d2y) pairs of u_00 for this level [num_grid][2] on a
  * LINEAR grid {grid_start, grid_end, num_grid} (DavidPA, no off-diagonal

@@ -2,8 +2,9 @@
 //
 // Some callers may not call cudaMalloc at all: code running inside a
 // host-side memory pool or arena that owns every device allocation, an
-// embedding that forbids allocation after start-up, or a stream that is
-// being captured where an allocation would break the capture.  For them,
+// embedding that forbids allocation after start-up, or a latency-critical
+// loop that must not pay for cudaMalloc's implicit device synchronisation.
+// For them,
 // pimc_shortrange_single_noalloc evaluates ShortRangeClass::SingleAction for
 // a DavidPA pair action on a linear grid with no off-diagonal terms, from
 // device buffers the caller already owns (the path, the (y, d2y) table of

@@ -2,7 +2,8 @@
 
 pimc_shortrange_single_noalloc serves callers that may not allocate device
 memory (a memory pool that owns every allocation, an embedding that forbids
-allocation after start-up, code running during stream capture): every
+allocation after start-up, a latency-critical loop that must not pay for
+cudaMalloc's implicit device synchronisation): every
 buffer is the caller's, and its scratch is a fixed array inside the library.
 It is called here through the C ABI on device buffers this test owns and
 compared with the context-based pimc_single_action on the same path, on two
