@@ -8,6 +8,8 @@
 #include <cstdlib>
 #include <cstring>
 #include <fstream>
+#include <new>
+#include <stdexcept>
 #include <sstream>
 #include <string>
 #include <vector>
@@ -195,6 +197,13 @@ bool find_line(std::istream &in, const char *key, LineCursor &lc) {
   return false;
 }
 
+// Sizes a squarer file may declare: anything larger is a damaged file, not
+// a table (the reference's reader would allocate it or read past its arrays).
+constexpr long kMaxDmGrid = 1L << 24;     // grid points
+constexpr long kMaxDmColumns = 4096;      // u_kj columns of one fit
+constexpr long kMaxDmTau = 64;            // tau values
+constexpr long kMaxDmValues = 1L << 27;   // values in one table block
+
 struct FitBlock {
   int ng = 0, nukj = 0, ntau = 0, nmax = 0, derv = 0;
   double tau_min = 0;
@@ -207,13 +216,23 @@ bool read_block(std::istream &in, FitBlock &b, std::string &err) {
   do {
     if (!find_line(in, "RANK", lc)) { err = "missing RANK 3 block"; return false; }
   } while (lc.integer() != 3);
-  b.ng = (int)lc.integer();
-  b.nukj = (int)lc.integer();
-  b.ntau = (int)lc.integer();
+  const long ng = lc.integer(), nukj = lc.integer(), ntau = lc.integer();
+  if (ng < 2 || ng > kMaxDmGrid || nukj < 1 || nukj > kMaxDmColumns || ntau < 1 || ntau > kMaxDmTau ||
+      ng * nukj * ntau > kMaxDmValues) {
+    err = "RANK 3 block sizes out of range";
+    return false;
+  }
+  b.ng = (int)ng;
+  b.nukj = (int)nukj;
+  b.ntau = (int)ntau;
   if (!find_line(in, "GRID 1", lc)) { err = "missing GRID 1"; return false; }
   lc.word(); lc.word();
   std::string type = lc.word();
   double g0 = lc.real(), g1 = lc.real();
+  if (!(g1 > g0) || !std::isfinite(g0) || !std::isfinite(g1) || (type == "LOG" && !(g0 > 0.0))) {
+    err = "bad r grid bounds";
+    return false;
+  }
   if (type == "LINEAR") {
     b.grid.init_linear(g0, g1, b.ng);
   } else if (type == "LOG") {
@@ -227,6 +246,10 @@ bool read_block(std::istream &in, FitBlock &b, std::string &err) {
   if (lc.word() != "LOG") { err = "tau grid is not LOG"; return false; }
   b.tau_min = lc.real();
   double tau_max = lc.real();
+  if (!(b.tau_min > 0.0) || !(tau_max >= b.tau_min) || !std::isfinite(tau_max)) {
+    err = "bad tau grid bounds";
+    return false;
+  }
   int ntau_calc = (int)std::floor(std::log(tau_max / b.tau_min) / std::log(2.0) + 0.5 + 1.0);
   if (ntau_calc != b.ntau) { err = "tau count inconsistent with tau grid"; return false; }
   if (!find_line(in, "BEGIN density matrix table", lc)) { err = "missing table"; return false; }
@@ -244,7 +267,8 @@ bool read_block(std::istream &in, FitBlock &b, std::string &err) {
 }
 }  // namespace
 
-int read_dm_file(const char *path, double desired_tau, int num_terms, DavidTables &out, std::string &err) {
+static int read_dm_file_checked(const char *path, double desired_tau, int num_terms, DavidTables &out,
+                                std::string &err) {
   std::ifstream in(path);
   if (!in) {
     err = std::string("cannot open ") + path;
@@ -253,11 +277,14 @@ int read_dm_file(const char *path, double desired_tau, int num_terms, DavidTable
   LineCursor lc;
   if (!find_line(in, "SQUARER", lc)) { err = "no SQUARER line"; return PIMC_E_FILE; }
   for (int i = 0; i < 4; i++) lc.word();
-  const int num_fits = (int)lc.integer();
+  const long num_fits_l = lc.integer();
+  if (num_fits_l < 0 || num_fits_l > 64) { err = "bad number of fits"; return PIMC_E_FILE; }
+  const int num_fits = (int)num_fits_l;
   if (!find_line(in, "RANK", lc)) { err = "no potential block"; return PIMC_E_FILE; }
   lc.word(); lc.word();
-  const int npot = (int)lc.integer();
-  if (npot < 2) { err = "bad potential size"; return PIMC_E_FILE; }
+  const long npot_l = lc.integer();
+  if (npot_l < 2 || npot_l > kMaxDmGrid) { err = "bad potential size"; return PIMC_E_FILE; }
+  const int npot = (int)npot_l;
   std::vector<double> potential(npot);
   if (!find_line(in, "potential", lc)) { err = "no potential table"; return PIMC_E_FILE; }
   for (int i = 0; i < npot; i++)
@@ -306,6 +333,20 @@ int read_dm_file(const char *path, double desired_tau, int num_terms, DavidTable
   out.num_terms = num_terms;
   build_david(out, tables[0].data(), tables[1].data());
   return PIMC_OK;
+}
+
+// No exception crosses the C ABI: a file that still makes the reader throw
+// (an allocation it cannot get) is reported as a status.
+int read_dm_file(const char *path, double desired_tau, int num_terms, DavidTables &out, std::string &err) {
+  try {
+    return read_dm_file_checked(path, desired_tau, num_terms, out, err);
+  } catch (const std::bad_alloc &) {
+    err = std::string("out of host memory reading ") + path;
+    return PIMC_E_NOMEM;
+  } catch (const std::exception &e) {
+    err = std::string("reading ") + path + ": " + e.what();
+    return PIMC_E_FILE;
+  }
 }
 
 }  // namespace pimc
