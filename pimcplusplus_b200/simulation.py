@@ -20,8 +20,9 @@ the device objects behind them:
   with PermuteType "NONE", and ShiftMoveClass (MetaMoves.cc:39-65).
 * `Observables` -> EnergyClass and PairCorrelationClass (Frequency, Name,
   Species1/2 and a Linear Grid); other observables are listed in `skipped`.
-* `Algorithm` -> LoopClass (PIMC++/src/LoopClass.cc:70-126): nested Loop
-  sections of Move and Observe events.
+* `Algorithm` -> LoopClass (PIMC++/src/LoopClass.cc:30-126): nested Loop
+  sections of Move and Observe events, the MaxWallTime limit and per-event
+  wall time.
 
 The random seed is the `Seed` variable of the `Parallel` section or of the
 top level (PathDataClass.cc:270-281).  Anything else the reference would
@@ -223,9 +224,16 @@ class Simulation:
         self._read_moves(io)
         io.CloseSection()
         self.algorithm = None
+        self.max_wall_time = None
         if io.OpenSection("Algorithm"):
+            # PIMCClass::ReadAlgorithm (PIMCClass.cc:438-450): seconds, -1 or absent = no limit
+            mwt = io.ReadVar("MaxWallTime")
+            self.max_wall_time = None if mwt is None or int(mwt) < 0 else int(mwt)
             self.algorithm = self._read_loop(io, 1)
             io.CloseSection()
+        self.start_wall_time = time.monotonic()
+        self.time_spent = {}
+        self.exceeded_wall_time = False
 
     def build(self, device=0, precision=FP64, schedule=SEQUENTIAL, cluster_ctas=0, threads_per_cta=0):
         """Creates the device chain: path, pair action, actions, moves, the
@@ -500,20 +508,40 @@ class Simulation:
             io.CloseSection()
         return (steps, events)
 
+    def exceeded_wall_time_limit(self):
+        """PathDataClass::ExceededWallTime (PathDataClass.cc:433-438)."""
+        return self.max_wall_time is not None and time.monotonic() - self.start_wall_time > self.max_wall_time
+
     def run(self, loop=None):
-        """Runs the Algorithm section (LoopClass::DoEvent)."""
+        """Runs the Algorithm section (LoopClass::DoEvent, LoopClass.cc:30-60).
+
+        Before every event the wall-clock limit (Algorithm MaxWallTime) is
+        checked; past it the run stops and `exceeded_wall_time` is set.  The
+        wall time of every Move and Observe event is added to
+        `time_spent[name]` (EventClass::TimeSpent).  Returns False when the
+        limit stopped the run."""
         loop = self.algorithm if loop is None else loop
         if loop is None:
             raise _err("no Algorithm section", self.filename)
         steps, events = loop
         for _ in range(steps):
             for kind, what in events:
+                if self.exceeded_wall_time_limit():
+                    self.exceeded_wall_time = True
+                    return False
+                t0 = time.monotonic()
                 if kind == "Move":
                     self.make_move(what)
                 elif kind == "Observe":
                     self.observe(what)
                 elif kind == "Loop":
-                    self.run(what)
+                    if not self.run(what):
+                        return False
+                    continue
+                else:
+                    continue
+                self.time_spent[what] = self.time_spent.get(what, 0.0) + time.monotonic() - t0
+        return True
 
     def close(self):
         self.moves.clear()

@@ -280,7 +280,7 @@ def write_pair_action_tricubic(path, tabs, smallest_beta, species_type="He", lam
 
 def write_pimc_input(path, cfg, pair_action_files, seed, init=("RANDOMFIXED", 0.45 * LJ_SIGMA), num_images=0,
                      steps_per_block=1, loop_steps=10, shift=False, observe_energy=False, species_type="He",
-                     lam=HE4_LAMBDA, use_density=False):
+                     lam=HE4_LAMBDA, use_density=False, max_wall_time=None):
     """A PIMC++ simulation input for one LJ-style chain of `cfg` (N, M, T, rho,
     levels): System, Action (Kinetic + ShortRange), a BisectionBlock move
     (and a ShiftMove), optional Energy observable, and an Algorithm loop."""
@@ -355,6 +355,8 @@ def write_pimc_input(path, cfg, pair_action_files, seed, init=("RANDOMFIXED", 0.
         io.CloseSection()
     io.CloseSection()
     io.NewSection("Algorithm")
+    if max_wall_time is not None:
+        io.WriteVar("MaxWallTime", int(max_wall_time))
     io.NewSection("Loop")
     io.WriteVar("Steps", int(loop_steps))
     io.NewSection("Move")

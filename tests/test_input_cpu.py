@@ -246,3 +246,34 @@ def test_oracle_shift_data_is_a_cyclic_slice_shift(shift):
     assert np.array_equal(o.get_path(0), want) and np.array_equal(o.get_path(1), want)
     with pytest.raises(ValueError):
         o.shift_data(m + 1)
+
+
+def test_algorithm_wall_time_limit_and_event_times(tmp_path):
+    """LoopClass: the run stops before the first event past MaxWallTime
+    (PathDataClass::ExceededWallTime) and accumulates each event's wall time.
+    The moves here are host stand-ins, so no GPU is needed."""
+    import time as _time
+    cfg, tau, box, path = _input(tmp_path, loop_steps=1000, shift=True, max_wall_time=1)
+    sim = Simulation.read(path)
+    assert sim.max_wall_time == 1
+    calls = []
+
+    def fake_move(name, n=1):
+        calls.append(name)
+        _time.sleep(0.02)
+
+    sim.make_move = fake_move
+    sim.start_wall_time = _time.monotonic()
+    t0 = _time.monotonic()
+    assert sim.run() is False and sim.exceeded_wall_time
+    elapsed = _time.monotonic() - t0
+    assert 1.0 <= elapsed < 2.0
+    assert 20 < len(calls) < 2000 and set(calls) == {"BisectionBlock", "Shift"}
+    assert abs(sum(sim.time_spent.values()) - elapsed) < 0.2
+    # no limit: the loop runs to the end
+    cfg, tau, box, path = _input(tmp_path, loop_steps=7)
+    sim = Simulation.read(path)
+    assert sim.max_wall_time is None
+    calls.clear()
+    sim.make_move = fake_move
+    assert sim.run() is True and calls == ["BisectionBlock"] * 7
