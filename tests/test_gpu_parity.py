@@ -426,3 +426,38 @@ def test_shortrange_single_edge_cases(tmp_path):
                  (0, 8, list(range(65)), 0)):
         with pytest.raises(P.PimcError):
             sr.SingleAction(*args)
+
+
+def test_nan_in_the_path_is_a_status(tmp_path):
+    """A NaN position (a damaged input, not a device fault) comes back as
+    PIMC_E_NAN from SingleAction and from the device moves' status word, and
+    the context keeps working: every index derived from a NaN is clamped."""
+    cfg, tau, box, dm = lj_case(tmp_path, n=16, m=16, levels=2, npts=200)
+    n, slices = cfg["N"], cfg["M"] + 1
+    path = random_walk_path(n, slices, box, 0.3, seed=5)
+    path[slices - 1] = path[0]
+    bad = path.copy()
+    bad[5, 3, 1] = np.nan
+    d = P.PathData(n, slices, box, tau, W.HE4_LAMBDA, 0)
+    d.pa_david_from_dm(dm, 0)
+    d.set_path(bad)
+    sr = P.ShortRangeClass(d)
+    with pytest.raises(P.PimcError) as e:
+        sr.SingleAction(0, 8, [3], 0)
+    assert e.value.status == 3
+    with pytest.raises(P.PimcError) as e:
+        sr.SingleAction(0, 8, [7], 0)  # 3 is a partner of 7
+    assert e.value.status == 3
+    d.set_path(path)
+    assert np.isfinite(sr.SingleAction(0, 8, [3], 0))
+    d.set_path(bad)
+    bb = P.BisectionBlock(d, cfg["levels"], 4)
+    bb.seed(3)
+    with pytest.raises(P.PimcError) as e:
+        bb.MakeMoves(20)
+    assert e.value.status == 3
+    d.set_path(path)
+    bb = P.BisectionBlock(d, cfg["levels"], 4)
+    bb.seed(3)
+    _, st = bb.MakeMoves(5)
+    assert st["status"] == 0 and st["moves"] == 20
