@@ -14,12 +14,17 @@
  * Common/Splines/TestMyTricubic.cc, and the identities the reference checks in
  * debug builds (incremental rho_k == full recompute, LongRangeClass.cc:283-305;
  * DistDisp == while-loop wrap, PathClass.h:664-676).  No reference-generated
- * SingleAction value exists anywhere, so action values are pinned only through
- * those pieces.
+ * SingleAction value exists anywhere, so action values are pinned through
+ * those pieces and through second, independent numpy/Python statements of the
+ * reference's formulas (tests/test_oracle_composition_cpu.py,
+ * test_oracle_tricubic_cpu.py, test_oracle_bisection_cpu.py), not against
+ * outputs of the reference itself.
  *
- * The RNG: the reference draws from SPRNG 2 (unpinned version, absent here).
- * Both this oracle and the CUDA library use the Philox-4x32-10 stream defined
- * in oracle_philox_uniform() instead, consumed in the reference's order.
+ * The RNG: the reference draws from SPRNG 2 (unpinned version, absent here),
+ * so the random stream is parity unpinned.  Both this oracle and the CUDA
+ * library use the Philox-4x32-10 stream defined in oracle_philox_uniform()
+ * instead (pinned by its published known answers), consumed in the
+ * reference's order.
  */
 #ifndef PIMC_ORACLE_H
 #define PIMC_ORACLE_H
