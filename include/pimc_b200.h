@@ -5,7 +5,10 @@
  * The library owns device copies of the path (OLD/NEW mirrored, like
  * MirroredClass), the pair-action tables and the rho_k cache, and evaluates
  * the actions a bisection move needs.  Plain pointers and sizes only; every
- * entry point returns an int status (0 = PIMC_OK) and never throws.  A
+ * entry point returns an int status (0 = PIMC_OK) and never throws (a set-up
+ * call that cannot get host memory for the tables it builds is the one case
+ * not turned into a status, except in the file readers, which return
+ * PIMC_E_NOMEM).  A
  * context is not thread-safe: one context per host thread, one CUDA stream
  * per context.
  *
