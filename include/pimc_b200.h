@@ -5,11 +5,10 @@
  * The library owns device copies of the path (OLD/NEW mirrored, like
  * MirroredClass), the pair-action tables and the rho_k cache, and evaluates
  * the actions a bisection move needs.  Plain pointers and sizes only; every
- * entry point returns an int status (0 = PIMC_OK) and never throws (a set-up
- * call that cannot get host memory for the tables it builds is the one case
- * not turned into a status, except in the file readers, which return
- * PIMC_E_NOMEM).  A
- * context is not thread-safe: one context per host thread, one CUDA stream
+ * entry point returns an int status (0 = PIMC_OK) instead of throwing.  The
+ * one failure not turned into a status is a set-up call running out of host
+ * memory for the tables it builds, which ends the process; the file readers
+ * return PIMC_E_NOMEM for that too.  A context is not thread-safe: one context per host thread, one CUDA stream
  * per context.
  *
  * Path layout everywhere: row-major [slice][particle][3] doubles, with
