@@ -8,8 +8,8 @@
  * entry point returns an int status (0 = PIMC_OK) instead of throwing.  The
  * one failure not turned into a status is a set-up call running out of host
  * memory for the tables it builds, which ends the process; the file readers
- * return PIMC_E_NOMEM for that too.  A context is not thread-safe: one context per host thread, one CUDA stream
- * per context.
+ * return PIMC_E_NOMEM for that too.  A context is not thread-safe: one
+ * context per host thread, one CUDA stream per context.
  *
  * Path layout everywhere: row-major [slice][particle][3] doubles, with
  * num_time_slices = M+1 rows, the layout of PathClass::Path (Blitz
