@@ -253,6 +253,20 @@ typedef struct pimc_bisection_desc {
    * a particle with more partners uses all of them. */
   double neighbor_skin;
   int neighbor_max;
+  /* PIMC_MIXED only.  0 (default): every stage whose Metropolis decision
+   * could come out differently on the FP64 sums — |logAcceptProb - log u|
+   * within the mixed sums' rigorous error bound — is evaluated again in FP64
+   * and decided on those sums, so the decisions, the trace and the path are
+   * the FP64 path's; stats.reevaluated counts those stages.  1: decide on the
+   * mixed sums alone. */
+  int mixed_unguarded;
+  /* Tries of the table-staging wait (a bounded spin on an mbarrier) before a
+   * launch gives up with PIMC_E_CAP; 0 = 2^22.  test_wait > 0 additionally
+   * waits that many tries on a barrier that nothing arrives at, after the
+   * table copy has landed, so the give-up path and its status can be tested
+   * without a fault; 0 in normal use. */
+  int wait_cap;
+  int test_wait;
 } pimc_bisection_desc;
 
 /* One move: the fields the accept trace is compared on. */
@@ -261,8 +275,12 @@ typedef struct pimc_move_record {
   int32_t ptcl;
   int32_t accepted;       /* whole move accepted */
   int32_t stages_passed;  /* bisection stages accepted */
-  double dS[8];           /* S_new - S_old per stage attempted, highest level first */
+  double dS[8];           /* S_new - S_old per stage attempted, highest level first, in the
+                             run's precision (PIMC_MIXED: the mixed sums) */
   double dS_shadow[8];    /* the same in the other precision (shadow mode), else 0 */
+  float dS_bound[8];      /* PIMC_MIXED: bound on |dS - dS of the FP64 sums|, else 0 */
+  int32_t reevaluated;    /* bit i: stage i was decided on its FP64 re-evaluation */
+  int32_t pad;
 } pimc_move_record;
 
 typedef struct pimc_bisection_stats {
@@ -274,6 +292,7 @@ typedef struct pimc_bisection_stats {
   int32_t status;         /* device status word: 0, PIMC_E_NAN, PIMC_E_STAGING, PIMC_E_CAP */
   int32_t pad;
   int64_t redone;         /* PROPOSALS: moves discarded and made again (not in moves) */
+  int64_t reevaluated;    /* PIMC_MIXED: stages decided on their FP64 re-evaluation */
 } pimc_bisection_stats;
 
 int pimc_bisection_setup(pimc_context *ctx, const pimc_bisection_desc *desc);
@@ -357,6 +376,10 @@ int pimc_batch_run_async(pimc_batch *b, int n_blocks);
 int pimc_batch_autotune(pimc_batch *b, int n_blocks, int *threads_per_cta, int *ctas, int *max_split,
                         double *split_ratio, double *ms);
 int pimc_batch_get_stats(pimc_batch *b, int chain /* -1: all */, pimc_bisection_stats *stats);
+/* PIMC_MIXED: on (1, the default) decides a stage on its FP64 re-evaluation
+ * whenever the mixed sums' error bound could change the decision, as
+ * pimc_bisection_desc.mixed_unguarded = 0; off (0): the mixed sums alone. */
+int pimc_batch_set_guard(pimc_batch *b, int on);
 int pimc_batch_get_path(pimc_batch *b, int chain, double *path);
 int pimc_batch_synchronize(pimc_batch *b);
 /* The batch's CUDA stream (cudaStream_t) for event timing and ordering. */

@@ -76,6 +76,9 @@ class BisectionDesc(C.Structure):
         ("schedule", C.c_int),
         ("neighbor_skin", C.c_double),
         ("neighbor_max", C.c_int),
+        ("mixed_unguarded", C.c_int),
+        ("wait_cap", C.c_int),
+        ("test_wait", C.c_int),
     ]
 
 
@@ -117,6 +120,7 @@ class BisectionStats(C.Structure):
         ("status", C.c_int32),
         ("pad", C.c_int32),
         ("redone", C.c_int64),
+        ("reevaluated", C.c_int64),
     ]
 
     def as_dict(self):
@@ -126,6 +130,7 @@ class BisectionStats(C.Structure):
 MOVE_RECORD = np.dtype([
     ("slice1", np.int32), ("ptcl", np.int32), ("accepted", np.int32), ("stages_passed", np.int32),
     ("dS", np.float64, (8,)), ("dS_shadow", np.float64, (8,)),
+    ("dS_bound", np.float32, (8,)), ("reevaluated", np.int32), ("pad", np.int32),
 ])
 
 _d, _i, _p = C.c_double, C.c_int, C.c_void_p
@@ -182,6 +187,7 @@ _SIGS = {
     "pimc_batch_autotune": (_i, [_p, _i, C.POINTER(_i), C.POINTER(_i), C.POINTER(_i), C.POINTER(_d),
                                  C.POINTER(_d)]),
     "pimc_batch_get_stats": (_i, [_p, _i, C.POINTER(BisectionStats)]),
+    "pimc_batch_set_guard": (_i, [_p, _i]),
     "pimc_batch_get_path": (_i, [_p, _i, _dp]),
     "pimc_batch_synchronize": (_i, [_p]),
     "pimc_batch_stream": (_p, [_p]),
@@ -518,7 +524,7 @@ class BisectionBlock:
 
     def __init__(self, path_data: PathData, num_levels, steps_per_block=1, shortrange_at_higher_levels=True,
                  precision=FP64, shadow=False, cluster_ctas=0, threads_per_cta=0, schedule=SEQUENTIAL,
-                 use_longrange=False, neighbor_skin=0.0, neighbor_max=0):
+                 use_longrange=False, neighbor_skin=0.0, neighbor_max=0, guard=True, wait_cap=0, test_wait=0):
         self.PathData = path_data
         d = BisectionDesc()
         d.num_levels = num_levels
@@ -532,6 +538,9 @@ class BisectionBlock:
         d.schedule = schedule
         d.neighbor_skin = neighbor_skin
         d.neighbor_max = neighbor_max
+        d.mixed_unguarded = 0 if guard else 1
+        d.wait_cap = wait_cap
+        d.test_wait = test_wait
         self.desc = d
         self.steps_per_block = steps_per_block
         path_data._check(_lib.pimc_bisection_setup(path_data.h, C.byref(d)), "bisection_setup")
@@ -639,6 +648,10 @@ class BatchChains:
     @property
     def stream(self):
         return _lib.pimc_batch_stream(self.h)
+
+    def set_guard(self, on=True):
+        """Mixed precision: decide near-threshold stages on their FP64 re-evaluation (on by default)."""
+        self._check(_lib.pimc_batch_set_guard(self.h, 1 if on else 0), "batch_set_guard")
 
     def autotune(self, n_blocks=1):
         """Pick threads_per_cta and the CTA count by timing; chains keep their state."""

@@ -220,6 +220,7 @@ int pimc_batch_create(int device, int n_chains, const pimc_chain_desc *chains, p
     j.steps_per_block = c.steps_per_block;
     j.sr_higher = 1;
     j.concurrent = 0;
+    j.guard = 1;
     cs[i].seed = c.seed;
     cs[i].stream = kStreamLocal;
   }
@@ -495,8 +496,20 @@ int pimc_batch_get_stats(pimc_batch *b, int chain, pimc_bisection_stats *stats) 
     stats->stages_attempted += (int64_t)c.stages;
     stats->pair_evals += (int64_t)c.pair_evals;
     stats->flips += (int64_t)c.flips;
+    stats->reevaluated += (int64_t)c.reevals;
     if (c.status && !stats->status) stats->status = c.status;
   }
+  return PIMC_OK;
+}
+
+int pimc_batch_set_guard(pimc_batch *b, int on) {
+  if (!b || (on != 0 && on != 1)) return PIMC_E_ARG;
+  BCK(cudaSetDevice(b->device));
+  BCK(cudaStreamSynchronize(b->stream));
+  for (auto &j : b->jobs) j.guard = on;
+  BCK(cudaMemcpy(b->d_jobs, b->jobs.data(), b->jobs.size() * sizeof(BisectionArgs), cudaMemcpyHostToDevice));
+  drop_graph(b);
+  b->cfg_version++;
   return PIMC_OK;
 }
 

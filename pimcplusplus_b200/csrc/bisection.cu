@@ -198,23 +198,51 @@ __device__ __forceinline__ double2 rho_new_k(double2 ro, const double *kv, const
 
 // OLD and NEW action sums of one stage level over this CTA's share of the
 // (partner, link) items, plus the moved particle's kinetic links on cluster
-// rank 0.  Partner positions are read once and serve both copies.  Returns
-// (S_old, S_new) in the evaluation precision R and, with SHADOW, the same in
+// rank 0.  Partner positions are read once and serve both copies.
+//  * R = double: the FP64 path; SHADOW adds the mixed-path sums alongside.
+//  * R = float, the mixed path: FP64 geometry, FP32 table arithmetic
+//    (pa_U_mixed), each term two-sum accumulated into FP64, and eb, a bound
+//    on |sums - FP64 sums| (kMixedErr times the terms' magnitudes, plus the
+//    FP32 phases of the long-range part); SHADOW adds the FP64 sums.
+// dg: this level's diagonal (y, d2y) pairs in R (DavidPA), dgs: the same in
 // the other precision.
+struct StageSums {
+  double so, sn, eb, so2, sn2;
+};
+// Bound on the error of one FP32 e^{ik.r}: the FP64 phase reduced to
+// [-pi, pi] and rounded to FP32 (<= 2^-22) and sincosf (2 ulp), doubled.
+constexpr double kCisErr = 2.0e-6;
+
 template <int KIND, typename R, bool SHADOW>
-__device__ __forceinline__ double4 stage_sums(const BisectionArgs &a, const double (*w_old)[3],
-                                              const double (*w_new)[3], const typename Pair2<R>::T *dg,
-                                              const void *dgs, int lv, int slice1, int ptcl, unsigned rank,
-                                              unsigned CL, int etid, int ethreads, const int *plist, int np) {
-  typedef typename std::conditional<std::is_same<R, double>::value, float, double>::type RS;
-  typedef typename Pair2<RS>::T P2S;
+__device__ __forceinline__ StageSums stage_sums(const BisectionArgs &a, const double (*w_old)[3],
+                                                const double (*w_new)[3], const void *dg, const void *dgs, int lv,
+                                                int slice1, int ptcl, unsigned rank, unsigned CL, int etid,
+                                                int ethreads, const int *plist, int np) {
+  constexpr bool MIX = std::is_same<R, float>::value;
   const DevSystem &sys = a.sys;
   const int N = sys.N;
   const int span = 1 << a.num_levels;
   const int skip = 1 << lv;
   const int nlinks = span >> lv;
-  double so = 0.0, sn = 0.0, so2 = 0.0, sn2 = 0.0;
-  if (rank == 0 && sys.lambda != 0.0) {  // KineticClass::SingleAction on the moved particle
+  const double2 *dg64 = reinterpret_cast<const double2 *>(MIX ? dgs : dg);
+  const float2 *dg32 = reinterpret_cast<const float2 *>(MIX ? dg : dgs);
+  // mb: sum of the terms' magnitudes m (FP32: a relative shortfall of
+  // 2^-24 per addition is far inside the factor kMixedErr leaves spare)
+  double so = 0.0, sn = 0.0, so2 = 0.0, sn2 = 0.0, eb = 0.0;
+  float co = 0.0f, cn = 0.0f, mb = 0.0f;
+  // one term of each copy: the run's precision into (so, sn), the other into the shadow
+  auto add_terms = [&](const LinkGeom<double> &g, bool is_new, int part, int nparts) {
+    if (MIX) {
+      const MixedU t = pa_U_mixed<KIND>(a.pa, dg32, g, lv, part, nparts);
+      two_sum_add(is_new ? sn : so, is_new ? cn : co, t.v);
+      mb += t.m;
+      if (SHADOW) (is_new ? sn2 : so2) += pa_U_part<double, KIND>(a.pa, dg64, g, lv, part, nparts);
+    } else {
+      (is_new ? sn : so) += pa_U_part<double, KIND>(a.pa, dg64, g, lv, part, nparts);
+      if (SHADOW) (is_new ? sn2 : so2) += pa_U_mixed<KIND>(a.pa, dg32, g, lv, part, nparts).v;
+    }
+  };
+  if (rank == 0 && sys.lambda != 0.0) {  // KineticClass::SingleAction on the moved particle (FP64 in both paths)
     const double levelTau = sys.tau * (1 << lv);
     const double F = 1.0 / (4.0 * sys.lambda * levelTau);
     for (int k = etid; k < nlinks; k += ethreads) {
@@ -226,8 +254,13 @@ __device__ __forceinline__ double4 stage_sums(const BisectionArgs &a, const doub
       put_in_box(vo, sys);
       put_in_box(vn, sys);
       const double ko = kinetic_link(vo, F, sys.num_images, sys), kn = kinetic_link(vn, F, sys.num_images, sys);
-      so += ko;
-      sn += kn;
+      if (MIX) {
+        two_sum_add(so, co, ko);
+        two_sum_add(sn, cn, kn);
+      } else {
+        so += ko;
+        sn += kn;
+      }
       so2 += ko;
       sn2 += kn;
     }
@@ -297,13 +330,8 @@ __device__ __forceinline__ double4 stage_sums(const BisectionArgs &a, const doub
           double dAo[3], dBo[3], dAn[3], dBn[3];
           dist_disp(w_old[r0], a2[u], w_old[r0 + skip], b2[u], sys, dAo, dBo);
           dist_disp(w_new[r0], a2[u], w_new[r0 + skip], b2[u], sys, dAn, dBn);
-          so += (double)pa_U<R, KIND>(a.pa, dg, link_geom<R>(dAo, dBo), lv);
-          sn += (double)pa_U<R, KIND>(a.pa, dg, link_geom<R>(dAn, dBn), lv);
-          if (SHADOW) {
-            const P2S *d2 = reinterpret_cast<const P2S *>(dgs);
-            so2 += (double)pa_U<RS, KIND>(a.pa, d2, link_geom<RS>(dAo, dBo), lv);
-            sn2 += (double)pa_U<RS, KIND>(a.pa, d2, link_geom<RS>(dAn, dBn), lv);
-          }
+          add_terms(link_geom<double>(dAo, dBo), false, 0, 1);
+          add_terms(link_geom<double>(dAn, dBn), true, 0, 1);
         }
       }
     } else {
@@ -322,18 +350,7 @@ __device__ __forceinline__ double4 stage_sums(const BisectionArgs &a, const doub
         const double b2[3] = {__ldcg(pb_), __ldcg(pb_ + 1), __ldcg(pb_ + 2)};
         double dA[3], dB[3];
         dist_disp(w[r0], a2, w[r0 + skip], b2, sys, dA, dB);
-        const double v = (double)pa_U_part<R, KIND>(a.pa, dg, link_geom<R>(dA, dB), lv, part, nparts);
-        double v2 = 0.0;
-        if (SHADOW)
-          v2 = (double)pa_U_part<RS, KIND>(a.pa, reinterpret_cast<const P2S *>(dgs), link_geom<RS>(dA, dB), lv,
-                                           part, nparts);
-        if (is_new) {
-          sn += v;
-          sn2 += v2;
-        } else {
-          so += v;
-          so2 += v2;
-        }
+        add_terms(link_geom<double>(dA, dB), is_new, part, nparts);
       }
     }
   }
@@ -355,16 +372,62 @@ __device__ __forceinline__ double4 stage_sums(const BisectionArgs &a, const doub
       const double u = __ldg(&a.ulong_k0[k]);
       const double2 rn = rho_new_k<R>(ro, kv, w_new[rel], w_old[rel]);
       const double o2 = ro.x * ro.x + ro.y * ro.y, n2 = rn.x * rn.x + rn.y * rn.y;
-      so += f * o2 * u;
-      sn += f * n2 * u;
+      if (MIX) {
+        two_sum_add(so, co, f * o2 * u);
+        two_sum_add(sn, cn, f * n2 * u);
+        // |rho_new - its FP64 value| <= 2 kCisErr (one new and one old phase)
+        const double dr = 2.0 * kCisErr;
+        eb += f * fabs(u) * (2.0 * sqrt(n2) * dr + dr * dr);
+      } else {
+        so += f * o2 * u;
+        sn += f * n2 * u;
+      }
       if (SHADOW) {
-        const double2 rs = rho_new_k<RS>(ro, kv, w_new[rel], w_old[rel]);
+        const double2 rs = rho_new_k<typename std::conditional<MIX, double, float>::type>(ro, kv, w_new[rel],
+                                                                                            w_old[rel]);
         so2 += f * o2 * u;
         sn2 += f * (rs.x * rs.x + rs.y * rs.y) * u;
       }
     }
   }
-  return make_double4(so, sn, so2, sn2);
+  StageSums r;
+  r.so = so + (double)co;
+  r.sn = sn + (double)cn;
+  r.eb = eb + kMixedErr * (1.0 + 1e-5) * (double)mb;
+  r.so2 = so2;
+  r.sn2 = sn2;
+  return r;
+}
+
+// The mixed path's FP64 re-evaluation of a stage (and, with need_prev, of the
+// stage before it, at level + 1 with its partner set): the FP64 path's
+// stage_sums with its item split, so the sums are the FP64 path's bit for
+// bit.  Returns (S_old, S_new, previous S_old, previous S_new) of this CTA.
+template <int KIND>
+__device__ __forceinline__ double4 stage_sums_reeval(const BisectionArgs &a, const double (*w_old)[3],
+                                                     const double (*w_new)[3], int lv, int slice1, int ptcl,
+                                                     unsigned rank, unsigned CL, int etid, int ethreads,
+                                                     const int *plist, int np, int need_prev,
+                                                     const int *prev_plist, int prev_np) {
+  const DDavid<double> &d64 = a.pa.d64;
+  auto dgl = [&](int l) -> const void * {
+    return KIND == PA_DAVID ? reinterpret_cast<const double2 *>(d64.diag) + (size_t)(d64.tau_pos + l) * d64.diag_stride
+                            : nullptr;
+  };
+  double4 r = make_double4(0.0, 0.0, 0.0, 0.0);
+  for (int k = 0; k < 1 + need_prev; k++) {  // one loop body: the FP64 evaluation is inlined once
+    const int l = lv + k;
+    const StageSums v = stage_sums<KIND, double, false>(a, w_old, w_new, dgl(l), nullptr, l, slice1, ptcl, rank, CL,
+                                                        etid, ethreads, k ? prev_plist : plist, k ? prev_np : np);
+    if (k) {
+      r.z = v.so;
+      r.w = v.sn;
+    } else {
+      r.x = v.so;
+      r.y = v.sn;
+    }
+  }
+  return r;
 }
 
 // Committed or speculative position of a chain's Local stream.
@@ -406,12 +469,16 @@ __device__ __forceinline__ void rng_store(RngSnap &s, const DevRandom &r) {
 //    the move ends at this stage (a rejection, or acceptance at level 0),
 //    unless the accepted particle was drawn again, whose window changes.
 // The draw order is therefore exactly the reference's.
+// Values reduced over a cluster per stage: S_old, S_new, the mixed bound and
+// the two shadow sums.
+constexpr int kRed = 5;
+
 // Shared state of one CTA while it runs a job.
 struct KernelShared {
   double win_old[2][kMaxWindow][3], win_new[2][kMaxWindow][3];
   double gbuf[2][3 * 32];
-  double sh_red[16][4];  // per warp: S_old, S_new, and their shadows
-  double xchg[2][kMaxCluster][4];
+  double sh_red[16][kRed];  // per warp: S_old, S_new, the mixed bound, the shadows
+  double xchg[2][kMaxCluster][kRed];
   double s_logsr[kMaxLevels], s_logu[kMaxLevels];
   int s_ctl[4];   // slice1, ptcl, stage accepted, status
   int s_next[4];  // next move speculated: valid, slice1, ptcl
@@ -431,6 +498,8 @@ struct KernelShared {
   int4 s_pub[kMaxCluster];
   int s_redo[kMaxCluster], s_redo_local;
   int s_commit[4];  // first slot to redo, stop, any committed move left its sphere
+  int s_need[2];    // mixed path: re-evaluate this stage in FP64; also the previous stage
+  uint64_t test_bar;  // an mbarrier nothing arrives at (the give-up test of the staging wait)
 };
 
 // Whether any of the window's span+1 NEW positions lies outside the moved
@@ -582,12 +651,25 @@ __device__ void run_job(const BisectionArgs &a, ChainState *cs, int window, unsi
       }
     }
     G.sync();
-    int ok = 0;
-    for (int it = 0; it < (1 << 22); it++)
+    // Bounded wait for the copy; with test_wait, a further bounded wait on a
+    // barrier that nothing arrives at once the copy has landed, which always
+    // runs out and takes the give-up path below.
+    const int cap = a.wait_cap > 0 ? a.wait_cap : (1 << 22);
+    int landed = 0;
+    for (int it = 0; it < cap; it++)
       if (mbar_try_wait(&s_bar, phase)) {
-        ok = 1;
+        landed = 1;
         break;
       }
+    int ok = landed;
+    if (ok && a.test_wait > 0) {
+      ok = 0;
+      for (int it = 0; it < a.test_wait; it++)
+        if (mbar_try_wait(&S.test_bar, 0)) {
+          ok = 1;
+          break;
+        }
+    }
     if (tid == 0) S.s_ok = 1;
     G.sync();
     if (!ok) S.s_ok = 0;
@@ -600,8 +682,9 @@ __device__ void run_job(const BisectionArgs &a, ChainState *cs, int window, unsi
       for (unsigned r = 0; r < CL; r++) all_ok &= (xchg[1][r][0] != 0.0);
     }
     if (!all_ok) {
-      // Give a late copy a second bounded chance to land before this CTA exits.
-      for (int it = 0; it < (1 << 22) && !ok; it++) ok = mbar_try_wait(&s_bar, phase);
+      // Let a late copy land (bounded) before this CTA moves on or exits:
+      // shared memory must not be left with a copy in flight.
+      for (int it = 0; it < (1 << 22) && !landed; it++) landed = mbar_try_wait(&s_bar, phase);
       if (lead) atomicExch(&cs->status, PIMC_E_CAP);
       if (CL > 1) cluster.sync();
       phase ^= 1u;
@@ -625,7 +708,7 @@ __device__ void run_job(const BisectionArgs &a, ChainState *cs, int window, unsi
     S.tab = tab_mem;
     S.tab.W = 0;  // filled below
   }
-  unsigned long long moves = 0, accepted = 0, stages = 0, pair_evals = 0, flips = 0, redone = 0;
+  unsigned long long moves = 0, accepted = 0, stages = 0, pair_evals = 0, flips = 0, redone = 0, reevals = 0;
   int status = 0;
   double *path = a.path;
   unsigned xc = 0;  // exchange parity counter
@@ -673,9 +756,9 @@ __device__ void run_job(const BisectionArgs &a, ChainState *cs, int window, unsi
     const int blk = prop ? 0 : m / a.steps_per_block, step = prop ? pstep : m - blk * a.steps_per_block;
     const bool active = !prop || (int)rank >= pfirst;
     // this move's work: counted at once, or with proposals when the move is kept
-    unsigned long long mv_stages = 0, mv_pairs = 0, mv_flips = 0;
+    unsigned long long mv_stages = 0, mv_pairs = 0, mv_flips = 0, mv_reevals = 0;
     unsigned long long &c_stages = PROP ? mv_stages : stages, &c_pairs = PROP ? mv_pairs : pair_evals,
-                       &c_flips = PROP ? mv_flips : flips;
+                       &c_flips = PROP ? mv_flips : flips, &c_reevals = PROP ? mv_reevals : reevals;
     bool acc_all = true;
     int move_far = 0;  // some stage of this move sampled outside the moved particle's sphere
     int mptcl = 0;     // the moved particle
@@ -733,12 +816,21 @@ __device__ void run_job(const BisectionArgs &a, ChainState *cs, int window, unsi
       double(*w_old)[3] = win_old[cur];
       double(*w_new)[3] = win_new[cur];
 
-      double prevDS = 0.0, prevDS_s = 0.0;
+      // prevDS: the previous stage's dS as the decision used it; prevE: a
+      // bound on its error against the FP64 sums (0 when it is FP64's)
+      double prevDS = 0.0, prevDS_s = 0.0, prevE = 0.0;
+      int prev_np = 0;
+      const int *prev_plist = nullptr;
       int passed = 0;
       if (lead) {
         rec.slice1 = slice1;
         rec.ptcl = ptcl;
-        for (int i = 0; i < 8; i++) rec.dS[i] = rec.dS_shadow[i] = 0.0;
+        for (int i = 0; i < 8; i++) {
+          rec.dS[i] = rec.dS_shadow[i] = 0.0;
+          rec.dS_bound[i] = 0.0f;
+        }
+        rec.reevaluated = 0;
+        rec.pad = 0;
       }
       int si = 0;
       for (int level = L - 1; level >= 0; level--, si++) {
@@ -761,16 +853,17 @@ __device__ void run_job(const BisectionArgs &a, ChainState *cs, int window, unsi
         if (evaluator) {
           const size_t st = KIND == PA_DAVID ? (size_t)david_of<R>(a.pa).diag_stride : 0;
           const size_t sts = (KIND == PA_DAVID && SHADOW) ? (size_t)david_of<RS>(a.pa).diag_stride : 0;
-          const double4 v = stage_sums<KIND, R, SHADOW>(a, w_old, w_new, diag_smem ? diag_smem + level * st : nullptr,
-                                                        diag_smem_s ? diag_smem_s + level * sts : nullptr, level,
-                                                        slice1, ptcl, erank, ECL, tid, ethreads, plist, np);
-          const double o1 = warp_sum(v.x), n1 = warp_sum(v.y);
-          const double o2 = SHADOW ? warp_sum(v.z) : 0.0, n2 = SHADOW ? warp_sum(v.w) : 0.0;
+          const StageSums v = stage_sums<KIND, R, SHADOW>(a, w_old, w_new, diag_smem ? diag_smem + level * st : nullptr,
+                                                          diag_smem_s ? diag_smem_s + level * sts : nullptr, level,
+                                                          slice1, ptcl, erank, ECL, tid, ethreads, plist, np);
+          const double r0 = warp_sum(v.so), r1 = warp_sum(v.sn), r2 = warp_sum(v.eb);
+          const double r3 = SHADOW ? warp_sum(v.so2) : 0.0, r4 = SHADOW ? warp_sum(v.sn2) : 0.0;
           if (lane == 0) {
-            sh_red[warp][0] = o1;
-            sh_red[warp][1] = n1;
-            sh_red[warp][2] = o2;
-            sh_red[warp][3] = n2;
+            sh_red[warp][0] = r0;
+            sh_red[warp][1] = r1;
+            sh_red[warp][2] = r2;
+            sh_red[warp][3] = r3;
+            sh_red[warp][4] = r4;
           }
         } else {
           if (warp == sampler && level > 0) {
@@ -817,39 +910,62 @@ __device__ void run_job(const BisectionArgs &a, ChainState *cs, int window, unsi
               rng_store(s_spec2, spec);
             }
           }
-          if (lane < 4) sh_red[warp][lane] = 0.0;
+          if (lane < kRed) sh_red[warp][lane] = 0.0;
         }
         // Counted as the reference performs them: OLD + NEW of the stage's links.
         if (lead && (level == 0 || a.sr_higher)) c_pairs += 2ull * (unsigned long long)np * (span >> level);
         G.sync();
         // ---- reduce: warps -> CTA (warp 0) -> cluster (DSMEM, rank order) ----
-        const int par = xc & 1;
-        xc++;
-        if (warp == 0 && lane < 4) {
-          double v = 0.0;
-          for (int w = 0; w < nwarps; w++) v += sh_red[w][lane];
+        // The sums are bitwise the same in every CTA of the cluster, so every
+        // CTA takes the same decision (and the same re-evaluation request).
+        auto reduce = [&]() -> double {
+          const int par = xc & 1;
+          xc++;
+          if (warp == 0 && lane < kRed) {
+            double v = 0.0;
+            for (int w = 0; w < nwarps; w++) v += sh_red[w][lane];
+            if (ECL > 1)
+              for (unsigned r = 0; r < CL; r++) cluster.map_shared_rank(&xchg[par][rank][0], r)[lane] = v;
+            else
+              xchg[par][0][lane] = v;
+          }
           if (ECL > 1)
-            for (unsigned r = 0; r < CL; r++) cluster.map_shared_rank(&xchg[par][rank][0], r)[lane] = v;
+            cluster.sync();
           else
-            xchg[par][0][lane] = v;
-        }
-        if (ECL > 1)
-          cluster.sync();
-        else
-          __syncwarp();
-        if (warp == 0) {
+            __syncwarp();
           double v = 0.0;
-          if (lane < 4)
+          if (warp == 0 && lane < kRed)
             for (unsigned r = 0; r < ECL; r++) v += xchg[par][r][lane];
-          const double so = __shfl_sync(0xffffffffu, v, 0);
-          const double sn = __shfl_sync(0xffffffffu, v, 1);
-          const double so2 = __shfl_sync(0xffffffffu, v, 2);
-          const double sn2 = __shfl_sync(0xffffffffu, v, 3);
-          // ---- Metropolis test, identical in every CTA ----
+          return v;
+        };
+        // ---- Metropolis test, identical in every CTA (warp 0) ----
+        // exact: so/sn are the FP64 sums (the FP64 path, or the mixed path's
+        // re-evaluation).  Otherwise the mixed sums decide when the decision
+        // cannot change within their bound E (the stage's bound, the previous
+        // stage's, and 1e-12 of the sums for the FP64 path's own rounding);
+        // when it could, warp 0 asks for the stage's FP64 re-evaluation (and
+        // the previous stage's, if its dS was mixed) and decides on those.
+        auto decide = [&](double so, double sn, double eb, double so2, double sn2, bool exact) {
           const double currActionChange = sn - so;
           const double logsr = s_logsr[level];
-          const double logAcceptProb = logsr - currActionChange + prevDS;
           const double logu = s_logu[level];
+          if (!exact && a.guard) {
+            const double logAcceptProb = logsr - currActionChange + prevDS;
+            const double E = eb + prevE + 1e-12 * (fabs(so) + fabs(sn));
+            if (!(fabs(logAcceptProb - logu) > E) && isfinite(currActionChange)) {
+              if (lane == 0) {
+                S.s_need[0] = 1;
+                S.s_need[1] = prevE > 0.0 ? 1 : 0;
+              }
+              if (lead && si < 8) {
+                rec.dS[si] = currActionChange;
+                rec.dS_bound[si] = (float)eb;
+                rec.reevaluated |= 1 << si;
+              }
+              return;
+            }
+          }
+          const double logAcceptProb = logsr - currActionChange + prevDS;
           bool toAccept = logAcceptProb >= logu;
           if (toAccept && (fabs(sn) > 1e50 || fabs(so) > 1e50)) {  // StageClass.cc:74-85
             toAccept = false;
@@ -864,13 +980,18 @@ __device__ void run_job(const BisectionArgs &a, ChainState *cs, int window, unsi
             if (lead && si < 8) rec.dS_shadow[si] = dss;
           }
           prevDS = currActionChange;
-          if (lead && si < 8) rec.dS[si] = currActionChange;
+          prevE = exact ? 0.0 : eb;
+          if (lead && si < 8) {
+            if (!exact || !(rec.reevaluated & (1 << si))) rec.dS[si] = currActionChange;
+            if (!exact) rec.dS_bound[si] = (float)eb;
+          }
           // commit the stream position the outcome selects
           const bool ends = !toAccept || level == 0 || status != 0;
           // neighbour lists: whether the next stage's NEW positions (the level
           // sampled speculatively into w_new) leave the moved particle's sphere
           const int far_next = (a.nbr_on && !ends) ? window_outside(w_new, span, S.s_cb, sys, lane) : 0;
           if (lane == 0) {
+            S.s_need[0] = 0;
             s_ctl[2] = toAccept ? 1 : 0;
             s_ctl[3] = status;
             int nv = 0;
@@ -889,9 +1010,51 @@ __device__ void run_job(const BisectionArgs &a, ChainState *cs, int window, unsi
             }
             s_next[0] = nv;
           }
+        };
+        {
+          const double v = reduce();
+          if (warp == 0) {
+            const double so = __shfl_sync(0xffffffffu, v, 0), sn = __shfl_sync(0xffffffffu, v, 1);
+            const double eb = __shfl_sync(0xffffffffu, v, 2);
+            const double so2 = __shfl_sync(0xffffffffu, v, 3), sn2 = __shfl_sync(0xffffffffu, v, 4);
+            decide(so, sn, std::is_same<R, float>::value ? eb : 0.0, so2, sn2, !std::is_same<R, float>::value);
+          }
         }
         G.sync();
+        if (std::is_same<R, float>::value && S.s_need[0]) {
+          // FP64 re-evaluation of this stage (and of the previous stage, whose
+          // sums read only slices that are multiples of 2^(level+1), unchanged
+          // since), with the FP64 path's item split and reduction: its sums are
+          // the FP64 path's bit for bit.
+          const int need_prev = S.s_need[1];
+          if (evaluator) {
+            const double4 v = stage_sums_reeval<KIND>(a, w_old, w_new, level, slice1, ptcl, erank, ECL, tid, ethreads,
+                                                      plist, np, need_prev, prev_plist, prev_np);
+            const double r0 = warp_sum(v.x), r1 = warp_sum(v.y), r2 = warp_sum(v.z), r3 = warp_sum(v.w);
+            if (lane == 0) {
+              sh_red[warp][0] = r0;
+              sh_red[warp][1] = r1;
+              sh_red[warp][2] = r2;
+              sh_red[warp][3] = r3;
+              sh_red[warp][4] = 0.0;
+            }
+          } else if (lane < kRed) {
+            sh_red[warp][lane] = 0.0;
+          }
+          if (lead) c_reevals++;
+          G.sync();
+          const double v = reduce();
+          if (warp == 0) {
+            const double so = __shfl_sync(0xffffffffu, v, 0), sn = __shfl_sync(0xffffffffu, v, 1);
+            const double pso = __shfl_sync(0xffffffffu, v, 2), psn = __shfl_sync(0xffffffffu, v, 3);
+            if (need_prev) prevDS = psn - pso;
+            decide(so, sn, 0.0, so, sn, true);
+          }
+          G.sync();
+        }
         if (tid == 0) c_stages++;
+        prev_np = np;
+        prev_plist = plist;
         if (!s_ctl[2] || s_ctl[3]) {
           acc_all = false;
           break;
@@ -910,17 +1073,18 @@ __device__ void run_job(const BisectionArgs &a, ChainState *cs, int window, unsi
     auto accept_copy = [&](bool write_path) {
       if (a.use_lr) {
         // AcceptCopy of rho_k (PathClass.cc:797-863): the NEW rho_k of the
-        // window, recomputed with the arithmetic of the stage sums, from the
-        // positions before PutInBoxFast as UpdateRho_ks saw them.  Split over
-        // the cluster's CTAs; with concurrent windows only interior slices are
-        // written (end slices are shared with the neighbouring windows, and
-        // their update is rounding only).
+        // window from the positions before PutInBoxFast as UpdateRho_ks saw
+        // them, in FP64 on both paths (the mixed path's FP32 phases serve its
+        // decisions only, so the chain state stays the FP64 path's).  Split
+        // over the cluster's CTAs; with concurrent windows only interior
+        // slices are written (end slices are shared with the neighbouring
+        // windows, and their update is rounding only).
         const int lo = a.concurrent ? 1 : 0, hi = a.concurrent ? span - 1 : span;
         const int nk = a.nk, total = (hi - lo + 1) * nk;
         for (int it = (int)erank * G.size + tid; it < total; it += (int)ECL * G.size) {
           const int rel = lo + it / nk, k = it - (it / nk) * nk;
           double2 *p2 = &a.rhok[(size_t)(slice1 + rel) * nk + k];
-          const double2 rn = rho_new_k<R>(__ldcg(p2), a.kvec + 3 * k, win_new[cur][rel], win_old[cur][rel]);
+          const double2 rn = rho_new_k<double>(__ldcg(p2), a.kvec + 3 * k, win_new[cur][rel], win_old[cur][rel]);
           __stcg(p2, rn);
         }
       }
@@ -941,6 +1105,7 @@ __device__ void run_job(const BisectionArgs &a, ChainState *cs, int window, unsi
         stages += mv_stages;
         pair_evals += mv_pairs;
         flips += mv_flips;
+        reevals += mv_reevals;
       }
       if (a.trace) a.trace[a.trace_offset + at] = rec;
     };
@@ -1050,6 +1215,7 @@ __device__ void run_job(const BisectionArgs &a, ChainState *cs, int window, unsi
     cs->pair_evals += pair_evals;
     cs->flips += flips;
     cs->redone += redone;
+    cs->reevals += reevals;
     if (status) cs->status = status;
   }
   if (CL > 1) cluster.sync();
@@ -1071,6 +1237,7 @@ __global__ void __launch_bounds__(512, 1) bisection_kernel(BisectionArgs a) {
   const int window = (int)(blockIdx.x / CL);
   if (threadIdx.x == 0) {
     mbar_init(&s_bar, 1);
+    mbar_init(&S.test_bar, 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   __syncthreads();
@@ -1111,6 +1278,7 @@ __global__ void __launch_bounds__(512, 1) batch_kernel(BatchArgs b) {
   cg::cluster_group cluster = cg::this_cluster();
   if (threadIdx.x < kSlots) {
     mbar_init(&s_bar[threadIdx.x], 1);
+    mbar_init(&S[threadIdx.x].test_bar, 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   __syncthreads();

@@ -35,6 +35,14 @@ struct BisectionArgs {
   const double4 *nbr_cb;
   const int *nbr_cnt, *nbr_idx;
   int *nbr_dirty;
+  // Mixed path: 1 = decide on the FP64 re-evaluation of a stage whenever the
+  // decision could differ from the FP64 sums' within the mixed sums' error
+  // bound (decisions identical to the FP64 path's); 0 = the mixed sums alone.
+  int guard;
+  // Tries of the table-staging wait before it gives up with PIMC_E_CAP;
+  // test_wait > 0 also waits that many tries on a barrier nothing arrives at
+  // (after the copy has landed), to exercise the give-up path.
+  int wait_cap, test_wait;
 };
 
 // Neighbour lists for the device moves (neighbors.cu): rebuilt from the

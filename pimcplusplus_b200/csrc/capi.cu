@@ -411,6 +411,30 @@ int pimc_pa_tricubic(pimc_context *ctx, int sp1, int sp2, const double qgrid[3],
     std::vector<float> df32(dF.begin(), dF.end());
     if ((rc = upload(ctx, df32.data(), df32.size(), &t32.dU))) return rc;
   }
+  {
+    // Error bound of the mixed path: per cell (low node ix, iy, iz) the sum
+    // over its 8 nodes of |F| + hx|Fx| + hy|Fy| + hz|Fz| + hx hy|Fxy| +
+    // hx hz|Fxz| + hy hz|Fyz| + hx hy hz|Fxyz| (component order of the
+    // node), rounded up to FP32.
+    const int nq = hg[0].n, ny = hg[1].n, nt = hg[2].n;
+    const double hx = hg[0].delta, hy = hg[1].delta, hz = hg[2].delta;
+    const double hs[8] = {1.0, hx, hy, hz, hx * hy, hx * hz, hy * hz, hx * hy * hz};
+    std::vector<float> mb(nodes * num_betas, 0.0f);
+    for (int b = 0; b < num_betas; b++)
+      for (int ix = 0; ix + 1 < nq; ix++)
+        for (int iy = 0; iy + 1 < ny; iy++)
+          for (int iz = 0; iz + 1 < nt; iz++) {
+            double m = 0.0;
+            for (int c = 0; c < 8; c++) {
+              const size_t node = ((size_t)(ix + (c >> 2)) * ny + (iy + ((c >> 1) & 1))) * nt + (iz + (c & 1));
+              const double *f = F.data() + ((size_t)b * nodes + node) * 8;
+              for (int k = 0; k < 8; k++) m += std::fabs(f[k]) * hs[k];
+            }
+            mb[(size_t)b * nodes + ((size_t)ix * ny + iy) * nt + iz] = (float)(m * (1.0 + 1e-6));
+          }
+    if ((rc = upload(ctx, mb.data(), mb.size(), &t32.mbound))) return rc;
+    t64.mbound = nullptr;
+  }
   upload_grid(ctx, pg, t64.pot_grid);
   upload_grid(ctx, pg, t32.pot_grid);
   if ((rc = upload(ctx, pot_data, (size_t)pot_n, &t64.pot_y))) return rc;
@@ -637,6 +661,8 @@ int pimc_bisection_setup(pimc_context *ctx, const pimc_bisection_desc *d) {
   }
   if (int rc2 = pa_levels_ok(ctx, d->num_levels)) return rc2;
   if (d->neighbor_skin < 0.0 || d->neighbor_max < 0) return fail(ctx, PIMC_E_ARG, "bad neighbour-list settings");
+  if ((d->mixed_unguarded != 0 && d->mixed_unguarded != 1) || d->wait_cap < 0 || d->test_wait < 0)
+    return fail(ctx, PIMC_E_ARG, "bad guard / wait settings");
   if (d->neighbor_skin > 0.0) {
     if (ctx->pa.kind != PA_DAVID) return fail(ctx, PIMC_E_ARG, "neighbour lists need a DavidPA table");
     if (ctx->sys.N > 65536) return fail(ctx, PIMC_E_ARG, "neighbour lists support up to 65536 particles");
@@ -664,7 +690,7 @@ int pimc_bisection_setup(pimc_context *ctx, const pimc_bisection_desc *d) {
   std::vector<ChainState> cs(kMaxChainStates);
   CK(cudaMemcpy(cs.data(), ctx->d_chain, cs.size() * sizeof(ChainState), cudaMemcpyDeviceToHost));
   for (auto &c : cs) {
-    c.moves = c.accepted = c.stages = c.pair_evals = c.flips = c.redone = 0;
+    c.moves = c.accepted = c.stages = c.pair_evals = c.flips = c.redone = c.reevals = 0;
     c.status = 0;
   }
   CK(cudaMemcpy(ctx->d_chain, cs.data(), cs.size() * sizeof(ChainState), cudaMemcpyHostToDevice));
@@ -734,6 +760,9 @@ static int run_bisection(pimc_context *ctx, int n_blocks, pimc_move_record *devi
   a.nbr_cnt = ctx->d_nbr_cnt;
   a.nbr_idx = ctx->d_nbr_idx;
   a.nbr_dirty = ctx->d_nbr_dirty;
+  a.guard = ctx->bis.mixed_unguarded ? 0 : 1;
+  a.wait_cap = ctx->bis.wait_cap;
+  a.test_wait = ctx->bis.test_wait;
   if (a.use_lr && !ctx->rhok_valid) {  // PathClass::UpdateRho_ks() of the current OLD path
     CK(launch_rhok_full(ctx->stream, ctx->d_path[0], ctx->sys.N, ctx->sys.S, lr_desc(ctx), ctx->d_rhok[0]));
     ctx->rhok_valid = true;
@@ -795,7 +824,15 @@ int pimc_run_bisection(pimc_context *ctx, int n_blocks, pimc_move_record *trace,
   rc = pimc_bisection_get_stats(ctx, &st);
   if (rc) return rc;
   if (stats) *stats = st;
-  if (st.status) return fail(ctx, st.status, std::string("device status: ") + pimc_status_string(st.status));
+  if (st.status) {
+    // The status belongs to this call: clear it so that the next call on the
+    // context starts clean (the chains' counters and streams are kept).
+    std::vector<ChainState> cs(kMaxChainStates);
+    CK(cudaMemcpy(cs.data(), ctx->d_chain, cs.size() * sizeof(ChainState), cudaMemcpyDeviceToHost));
+    for (auto &c : cs) c.status = 0;
+    CK(cudaMemcpy(ctx->d_chain, cs.data(), cs.size() * sizeof(ChainState), cudaMemcpyHostToDevice));
+    return fail(ctx, st.status, std::string("device status: ") + pimc_status_string(st.status));
+  }
   return PIMC_OK;
 }
 
@@ -813,6 +850,7 @@ int pimc_bisection_get_stats(pimc_context *ctx, pimc_bisection_stats *stats) {
     stats->pair_evals += (int64_t)c.pair_evals;
     stats->flips += (int64_t)c.flips;
     stats->redone += (int64_t)c.redone;
+    stats->reevaluated += (int64_t)c.reevals;
     if (c.status && !stats->status) stats->status = c.status;
   }
   return PIMC_OK;

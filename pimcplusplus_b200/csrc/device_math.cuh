@@ -501,6 +501,248 @@ __device__ __forceinline__ const DDavid<double> &david_of<double>(const DevPA &p
 template <>
 __device__ __forceinline__ const DDavid<float> &david_of<float>(const DevPA &pa) { return pa.d32; }
 
+// ---- mixed precision: FP64 geometry and cell search, FP32 table arithmetic ----
+// The mixed path forms r, r', s, q, z, the grid cell and the position inside
+// the cell in FP64 — the same operations as the FP64 path, so the same cell
+// and bit-identical in-cell coordinates — and rounds only the in-cell
+// coordinate (a number in [0, 1]) to FP32.  The spline / tricubic polynomial
+// then runs in FP32 on the FP32 copy of the table.  Each term comes with a
+// magnitude m >= sum_j |c_j| |b_j| over its coefficients c_j and basis values
+// b_j, so that |v - U| <= kMixedErr * m, U the FP64 evaluation of the same
+// term: table rounding (2^-24 each), the FP32 rounding of the in-cell
+// coordinate and of the basis, and the O(10) FP32 operations of the
+// polynomial add up to fewer than 64 units of 2^-24 relative to m.
+struct MixedU {
+  double v;  // FP32 result (plus any FP64-evaluated addend)
+  float m;   // magnitude bound
+};
+constexpr double kMixedErr = 64.0 * 5.9604644775390625e-8;  // 64 * 2^-24
+
+// Cell and in-cell weight b = (x - x_low) / h of MultiCubicSpline::operator()
+// in FP64, as spline_cell<double>; then the cubic in FP32 on (y, d2y) pairs.
+__device__ __forceinline__ MixedU spline_pairs_mixed(const DGrid<double> &g, const float2 *tab, double x) {
+  int low, hi;
+  double xl, xh, h;
+  if (g.type == PIMC_GRID_LINEAR) {
+    const double rm = round_even_magic(rsub(rmul(rsub(x, g.start), g.deltainv), 0.5));
+    const double lowf = fmin(fmax(rm, 0.0), (double)(g.n - 2));
+    low = int_of_integral(lowf);
+    hi = low + 1;
+    xl = radd(g.start, rmul(lowf, g.delta));
+    xh = 0.0;
+    h = g.delta;
+  } else {
+    hi = reverse_map(g, x) + 1;
+    low = hi - 1;
+    if (low < 0) { low = 0; hi = 1; }
+    if (hi > (g.n - 1)) { hi = g.n - 1; low = hi - 1; }
+    xl = grid_x(g, low);
+    xh = grid_x(g, hi);
+    h = xh - xl;
+  }
+  const bool lin = g.type == PIMC_GRID_LINEAR;
+  const double hinv = lin ? g.deltainv : 1.0 / h;
+  const float b = (float)((x - xl) * hinv);
+  const float a = lin ? 1.0f - b : (float)((xh - x) * hinv);
+  const float h26 = (float)(h * h * 0.1666666666666666666);
+  const float a3 = a * a * a - a, b3 = b * b * b - b;
+  const float2 lo = tab[low], hv = tab[hi];
+  MixedU r;
+  r.v = (double)(a * lo.x + b * hv.x + (a3 * lo.y + b3 * hv.y) * h26);
+  // |a|, |b| <= 1 and |a^3 - a|, |b^3 - b| <= 0.385 on the cell
+  r.m = fabsf(lo.x) + fabsf(hv.x) + h26 * (fabsf(lo.y) + fabsf(hv.y));
+  return r;
+}
+
+// DavidPAClass::calcUsqzFast (DavidPAClass.cc:468-511) on the mixed path:
+// the diagonal u_00 columns in FP32 (diag: FP32 (y, d2y) pairs of this
+// level), the clamps on FP64 r, r'; off-diagonal u_kj terms, when the fit has
+// them, in FP64 on the FP64 tables.
+__device__ __forceinline__ MixedU david_U_mixed(const DDavid<double> &d, const float2 *diag, double s2, double q,
+                                                double z, int level) {
+  level = level + d.tau_pos;
+  const DGrid<double> &g = d.grid;
+  const double rmin = g.start;
+  double r = q + 0.5 * z;
+  double rprime = q - 0.5 * z;
+  if (r > g.end) r = g.end;
+  if (rprime > g.end) rprime = g.end;
+  if ((rprime < rmin) || (r < rmin)) return spline_pairs_mixed(g, diag, rmin);
+  const MixedU a = spline_pairs_mixed(g, diag, r), b = spline_pairs_mixed(g, diag, rprime);
+  MixedU U;
+  U.v = (double)(0.5f * ((float)a.v + (float)b.v));
+  U.m = 0.5f * (a.m + b.m);
+  if (d.num_terms > 0 && s2 > 0.0 && q < g.end) {
+    const double off = david_offdiag_add<double>(g, d.uy + (size_t)level * g.n * d.ncols,
+                                                 d.ud2 + (size_t)level * g.n * d.ncols, d.ncols, d.num_terms, 0.0,
+                                                 s2, q, z);
+    U.v += off;
+    // The FP64 path adds the same terms onto its diagonal value: the two
+    // FP64 sums differ by a few 2^-53 of |off|, far below 1e-9 kMixedErr |off|.
+    U.m += (float)(1e-9 * fabs(off));
+  }
+  return U;
+}
+
+// MyTricubicSpline::operator() (MyTricubicSpline.h:197-334) with the cell and
+// the in-cell coordinates in FP64 and the Hermite basis and contraction in
+// FP32 over (x-node, y-node) pairs [k0, k1) of the cell.
+__device__ __forceinline__ float tricubic_eval_mixed(const float *__restrict__ F, const DGrid<double> &gx,
+                                                     const DGrid<double> &gy, const DGrid<double> &gz, double x,
+                                                     double y, double z, int ny, int nt, int &cell, int k0 = 0,
+                                                     int k1 = 4) {
+  int ix = reverse_map(gx, x), iy = reverse_map(gy, y), iz = reverse_map(gz, z);
+  ix = max(0, ix); ix = min(ix, gx.n - 2);
+  iy = max(0, iy); iy = min(iy, gy.n - 2);
+  iz = max(0, iz); iz = min(iz, gz.n - 2);
+  float a[4], b[4], c[4];
+  hermite4((float)((x - grid_x(gx, ix)) * gx.deltainv), (float)gx.delta, a);
+  hermite4((float)((y - grid_x(gy, iy)) * gy.deltainv), (float)gy.delta, b);
+  hermite4((float)((z - grid_x(gz, iz)) * gz.deltainv), (float)gz.delta, c);
+  cell = (ix * ny + iy) * nt + iz;
+  const size_t sy = (size_t)nt * 8, sx = (size_t)ny * sy;
+  const float *base = F + (size_t)cell * 8;
+  float val = 0.0f;
+#pragma unroll
+  for (int k = 0; k < 4; k++) {
+    if (k < k0 || k >= k1) continue;
+    const int dx = k >> 1, dy = k & 1;
+    const float *p = base + dx * sx + dy * sy;
+    Node8<float> n0, n1;
+    n0.load(p);
+    n1.load(p + 8);
+    const float A0 = a[dx], A1 = a[2 + dx], B0 = b[dy], B1 = b[2 + dy];
+    const float C00 = c[0], C01 = c[2], C10 = c[1], C11 = c[3];
+    const float s00 = n0.v[0] * C00 + n0.v[3] * C01 + n1.v[0] * C10 + n1.v[3] * C11;
+    const float s01 = n0.v[2] * C00 + n0.v[6] * C01 + n1.v[2] * C10 + n1.v[6] * C11;
+    const float s10 = n0.v[1] * C00 + n0.v[5] * C01 + n1.v[1] * C10 + n1.v[5] * C11;
+    const float s11 = n0.v[4] * C00 + n0.v[7] * C01 + n1.v[4] * C10 + n1.v[7] * C11;
+    val += A0 * (B0 * s00 + B1 * s01) + A1 * (B0 * s10 + B1 * s11);
+  }
+  return val;
+}
+
+// SplinePot::V on the mixed path (cell in FP64, cubic in FP32); zero beyond End.
+__device__ __forceinline__ MixedU pot_V_mixed(const DTricubic<double> &t64, const DTricubic<float> &t32, double r) {
+  const DGrid<double> &g = t64.pot_grid;
+  const double x = r <= g.end ? r : g.end;
+  const double rm = round_even_magic(rsub(rmul(rsub(x, g.start), g.deltainv), 0.5));
+  const double lowf = fmin(fmax(rm, 0.0), (double)(g.n - 2));
+  const int low = int_of_integral(lowf);
+  const double xl = radd(g.start, rmul(lowf, g.delta));
+  const float b = (float)((x - xl) * g.deltainv), a = 1.0f - b;
+  const float h26 = (float)(g.delta * g.delta * 0.1666666666666666666);
+  const float a3 = a * a * a - a, b3 = b * b * b - b;
+  const float yl = __ldg(&t32.pot_y[low]), yh = __ldg(&t32.pot_y[low + 1]);
+  const float dl = __ldg(&t32.pot_d2[low]), dh = __ldg(&t32.pot_d2[low + 1]);
+  MixedU u;
+  const bool in = r <= g.end;
+  u.v = in ? (double)(a * yl + b * yh + (a3 * dl + b3 * dh) * h26) : 0.0;
+  u.m = in ? fabsf(yl) + fabsf(yh) + h26 * (fabsf(dl) + fabsf(dh)) : 0.0f;
+  return u;
+}
+
+// PAtricubicFitClass::U (PAtricubicFit.cc:659-721) on the mixed path; the
+// region test, (q, y, t) and the primitive's r, r' in FP64.  The magnitude of
+// a tricubic term is the cell's precomputed bound (t32.mbound: the sum over
+// the cell's 8 nodes of |F| + h|F_x| + ... + h_x h_y h_z |F_xyz|, which
+// bounds sum_j |c_j||b_j| anywhere in the cell since the Hermite basis
+// satisfies |p| <= 1, |q| <= 4h/27).  Parts as tricubic_pa.
+__device__ __forceinline__ MixedU tricubic_pa_mixed(const DTricubic<double> &t64, const DTricubic<float> &t32,
+                                                    double q, double z, double s2, int level, int part = 0,
+                                                    int nparts = 1) {
+  z = fabs(z);
+  const double smax = 2.0 * q;
+  const double s = sqrt(s2);
+  const bool inside = (q <= t64.qmax) && (z < smax) && (s < smax);
+  const bool nonzero = inside && q != 0.0;
+  const double xq = nonzero ? q : 0.0;
+  const double xy = nonzero ? z / smax : 0.0;
+  const double xt = nonzero ? (s - z) / (smax - z) : 0.0;
+  const size_t lvl = (size_t)level * t32.nq * t32.ny * t32.nt;
+  const int k0 = (4 * part) / nparts, k1 = (4 * (part + 1)) / nparts;
+  int cell;
+  const float tri = tricubic_eval_mixed(t32.U + lvl * 8, t64.qg, t64.yg, t64.tg, xq, xy, xt, t32.ny, t32.nt, cell,
+                                        k0, k1);
+  const float trim = part == 0 ? __ldg(&t32.mbound[lvl + cell]) : 0.0f;
+  const double r = q + 0.5 * z, rp = q - 0.5 * z;
+  double beta = t64.smallest_beta;
+  for (int i = 0; i < level; i++) beta *= 2.0;
+  const float hb = (float)(0.5 * beta);
+  MixedU prim;
+  if (nparts == 1) {
+    const MixedU va = pot_V_mixed(t64, t32, r), vb = pot_V_mixed(t64, t32, rp);
+    prim.v = (double)(hb * ((float)va.v + (float)vb.v));
+    prim.m = hb * (va.m + vb.m);
+  } else if (part < 2) {
+    const MixedU va = pot_V_mixed(t64, t32, part == 0 ? r : rp);
+    prim.v = (double)(hb * (float)va.v);
+    prim.m = hb * va.m;
+  } else {
+    prim.v = 0.0;
+    prim.m = 0.0f;
+  }
+  MixedU u;
+  u.v = inside ? (double)tri : prim.v;
+  u.m = inside ? trim : prim.m;
+  return u;
+}
+
+// QuinticSpline::operator() on the mixed path: interval and P = x - x_I in
+// FP64, Horner in FP32; the magnitude is Horner on |coefficients| and |P|.
+__device__ __forceinline__ MixedU quintic_mixed(const DCoulomb<double> &c, const float *tab, double x) {
+  const double rm = round_even_magic(rsub(rmul(x, c.hinv), 0.5));
+  const double lowf = fmin(fmax(rm, 0.0), (double)(c.np - 2));
+  const int i = int_of_integral(lowf);
+  const float *t = tab + (size_t)i * 6;
+  const float P = (float)(x - rmul(lowf, c.h)), aP = fabsf(P);
+  MixedU u;
+  u.v = (double)(((((t[5] * P + t[4]) * P + t[3]) * P + t[2]) * P + t[1]) * P + t[0]);
+  u.m = ((((fabsf(t[5]) * aP + fabsf(t[4])) * aP + fabsf(t[3])) * aP + fabsf(t[2])) * aP + fabsf(t[1])) * aP +
+        fabsf(t[0]);
+  return u;
+}
+// PAclassicalFitClass::U minus the long-range part (ShortRangeClass.cc:211-214)
+// on the mixed path: beta Z1Z2 / q by one FP32 division of FP64-formed operands.
+__device__ __forceinline__ MixedU coulomb_U_mixed(const DCoulomb<double> &c64, const DCoulomb<float> &c32,
+                                                  const LinkGeom<double> &g, int level) {
+  double beta = c64.smallest_beta;
+  for (int i = 0; i < level; i++) beta *= 2.0;
+  const float t0 = (float)(beta * c64.z1z2) / (float)g.q;
+  MixedU u;
+  u.v = (double)t0;
+  u.m = fabsf(t0);
+  if (c64.long_range) {
+    const float *tab = c32.ulong + (size_t)level * c32.np * 6;
+    const MixedU a = quintic_mixed(c64, tab, g.rmag), b = quintic_mixed(c64, tab, g.rpmag);
+    u.v = (double)(t0 - 0.5f * ((float)a.v + (float)b.v));
+    u.m += 0.5f * (a.m + b.m);
+  }
+  return u;
+}
+
+// U of one pair-link on the mixed path from the FP64 geometry; diag: the FP32
+// (y, d2y) pairs of this level's u_00 column (DavidPA).  Part `part` of
+// `nparts` as pa_U_part.
+template <int KIND>
+__device__ __forceinline__ MixedU pa_U_mixed(const DevPA &pa, const float2 *diag, const LinkGeom<double> &g,
+                                             int level, int part = 0, int nparts = 1) {
+  if (KIND == PA_TRICUBIC) return tricubic_pa_mixed(pa.t64, pa.t32, g.q, g.z, g.s2, level, part, nparts);
+  if (part != 0) return MixedU{0.0, 0.0f};
+  if (KIND == PA_DAVID) return david_U_mixed(pa.d64, diag, g.s2, g.q, g.z, level);
+  return coulomb_U_mixed(pa.c64, pa.c32, g, level);
+}
+
+// Two-sum accumulation (Knuth): s + c carries the running sum of the terms
+// with the exact rounding error of each FP64 addition gathered in c (FP32
+// suffices for c: each error is below 2^-53 |s|).
+__device__ __forceinline__ void two_sum_add(double &s, float &c, double x) {
+  const double t = s + x;
+  const double bp = t - s;
+  c += (float)((s - (t - bp)) + (x - bp));
+  s = t;
+}
+
 // dU (energy estimator), FP64 only.
 template <int KIND>
 __device__ __forceinline__ double pa_dU(const DevPA &pa, const LinkGeom<double> &g, int level);

@@ -78,6 +78,9 @@ struct DTricubic {
   const R *dU;  // same
   DGrid<R> pot_grid;
   const R *pot_y, *pot_d2;  // SplinePot natural cubic spline
+  // Mixed path: per level and cell (indexed by the cell's low node, [beta][nq][ny][nt])
+  // a bound on sum_j |c_j| |b_j| of the U evaluation anywhere in the cell
+  const float *mbound;
 };
 
 enum PAKind : int { PA_NONE = 0, PA_DAVID = 1, PA_TRICUBIC = 2, PA_COULOMB = 3 };
@@ -150,6 +153,7 @@ struct ChainState {
   int32_t pad;
   unsigned long long moves, accepted, stages, pair_evals, flips;
   unsigned long long redone;  // concurrent proposals: moves discarded and made again
+  unsigned long long reevals; // mixed path: stages decided on their FP64 re-evaluation
 };
 
 struct DeviceBuffer {

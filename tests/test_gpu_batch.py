@@ -64,12 +64,44 @@ def test_batch_matches_oracle_per_chain(threads, max_split, ratio):
     b.close()
 
 
-def test_batch_mixed_runs_and_accepts():
+@pytest.mark.parametrize("threads,max_split", [(128, 0), (512, 2)])
+def test_batch_mixed_matches_oracle_per_chain(threads, max_split):
+    """The guarded mixed batch (FP32 pair terms; a stage whose decision lies
+    within the mixed sums' bound is decided on its FP64 re-evaluation) makes
+    each chain's oracle moves: identical trace, path within 1e-9, and each
+    mixed dS within its reported bound of the oracle's FP64 dS."""
     chains = make_chains()
-    b = P.BatchChains(chains, precision=P.MIXED, threads_per_cta=128)
-    _, stats = b.run(40)
+    b = P.BatchChains(chains, precision=P.MIXED, threads_per_cta=threads, ctas=5, max_split=max_split,
+                      split_ratio=0.5)
+    n_blocks = 25
+    trace, stats = b.run(n_blocks, trace=True)
+    for i, c in enumerate(chains):
+        ref, ref_path, _ = oracle_run(c, n_blocks)
+        got = trace[i]
+        for k, r in enumerate(ref):
+            g = got[k]
+            assert (r.slice1, r.ptcl, r.accepted, r.stages_passed) == (
+                int(g["slice1"]), int(g["ptcl"]), int(g["accepted"]), int(g["stages_passed"])), (i, k)
+            for j in range(8):
+                assert abs(r.dS[j] - g["dS"][j]) <= float(g["dS_bound"][j]) + 1e-9 * max(1.0, abs(r.dS[j])), (i, k, j)
+        assert np.max(np.abs(b.path(i) - ref_path)) < 1e-9, i
     assert stats["status"] == 0
     assert 0.02 < stats["accepted"] / stats["moves"] < 0.98
+    b.close()
+
+
+def test_batch_mixed_shadow_bound_and_flips():
+    """Batched mixed chains with the FP64 sums alongside: the bound holds on
+    every stage and no decision flips."""
+    chains = make_chains()
+    b = P.BatchChains(chains, precision=P.MIXED, shadow=True, threads_per_cta=256)
+    trace, stats = b.run(20, trace=True)
+    rec = trace.reshape(-1)
+    mask = rec["dS_shadow"] != 0.0
+    err = np.abs(rec["dS"][mask] - rec["dS_shadow"][mask])
+    assert mask.sum() > 100
+    assert np.all(err <= rec["dS_bound"][mask].astype(np.float64) + 1e-12)
+    assert stats["flips"] == 0 and stats["status"] == 0
     b.close()
 
 

@@ -105,23 +105,28 @@ def compare(ref, got, stats, tol=1e-9):
     for i, (r, g) in enumerate(zip(ref, got)):
         assert (r.slice1, r.ptcl, r.accepted, r.stages_passed) == (
             int(g["slice1"]), int(g["ptcl"]), int(g["accepted"]), int(g["stages_passed"])), i
-        for k in range(8):
-            assert abs(r.dS[k] - g["dS"][k]) <= tol * max(1.0, abs(r.dS[k])), (i, k, r.dS[k], g["dS"][k])
+        for k in range(8):  # FP64: within tol; mixed: within the stage's reported bound
+            assert abs(r.dS[k] - g["dS"][k]) <= float(g["dS_bound"][k]) + tol * max(1.0, abs(r.dS[k])), (
+                i, k, r.dS[k], g["dS"][k])
         n_acc += r.accepted
     assert stats["status"] == 0 and stats["accepted"] == n_acc
     return n_acc
 
 
+@pytest.mark.parametrize("precision", [P.FP64, P.MIXED])
 @pytest.mark.parametrize("cluster", [1, 2])
-def test_bisection_jellium_longrange_trace(cluster):
+def test_bisection_jellium_longrange_trace(cluster, precision):
     """Device moves with LongRange in the lowest stage (rho_k updated per
-    moved slice, written back on acceptance) replay the oracle's trace."""
+    moved slice, written back on acceptance) replay the oracle's trace; the
+    guarded mixed path too (its near-threshold stages decided in FP64, its
+    accepted rho_k written in FP64)."""
     o, d, m, levels = jellium_moves()
     L, spb = 3, 4
     o.bisection_config(L, spb, use_longrange=True)
     o.rng_seed(5)
     ref = o.run_bisection(40)
-    bb = P.BisectionBlock(d, L, spb, cluster_ctas=cluster, threads_per_cta=128, use_longrange=True)
+    bb = P.BisectionBlock(d, L, spb, cluster_ctas=cluster, threads_per_cta=128, use_longrange=True,
+                          precision=precision)
     bb.seed(5)
     got, stats = bb.MakeMoves(40)
     assert compare(ref, got, stats) > 10
@@ -156,18 +161,23 @@ def test_bisection_jellium_longrange_windows():
     d.close()
 
 
-def test_bisection_jellium_mixed_shadow():
+@pytest.mark.parametrize("guard", [True, False])
+def test_bisection_jellium_mixed_shadow(guard):
     """Mixed path (FP32 pair terms and FP32 sincos of reduced phases, FP64
-    sums): per-stage dS relative error against the FP64 terms, and flips."""
+    sums) with the FP64 sums alongside: every stage's mixed dS within its
+    rigorous bound of the FP64 dS; guarded, no flipped decision."""
     o, d, m, levels = jellium_moves(seed=29)
     bb = P.BisectionBlock(d, 3, 4, precision=P.MIXED, shadow=True, cluster_ctas=1, threads_per_cta=128,
-                          use_longrange=True)
+                          use_longrange=True, guard=guard)
     bb.seed(3)
     rec, stats = bb.MakeMoves(100)
     mask = rec["dS_shadow"] != 0.0
-    rel = np.abs(rec["dS"][mask] - rec["dS_shadow"][mask]) / np.maximum(np.abs(rec["dS_shadow"][mask]), 1e-3)
+    err = np.abs(rec["dS"][mask] - rec["dS_shadow"][mask])
+    assert np.all(err <= rec["dS_bound"][mask].astype(np.float64) + 1e-12), np.max(err - rec["dS_bound"][mask])
+    rel = err / np.maximum(np.abs(rec["dS_shadow"][mask]), 1e-3)
     assert np.median(rel) < 1e-5, np.median(rel)
-    assert stats["flips"] <= 0.01 * stats["stages_attempted"] + 1
+    if guard:
+        assert stats["flips"] == 0
     d.close()
 
 

@@ -9,6 +9,10 @@ Tolerances:
   * Bisection moves: identical accept trace (slice, particle, accepted,
     stages passed) and per-stage dS within 1e-9 absolute, final path within
     1e-9 (positions are O(10)).
+  * Mixed-precision bisection moves (FP64 re-evaluation of every stage whose
+    decision lies within the mixed sums' error bound): the same identical
+    trace and final path, and each stage's mixed dS within its own reported
+    bound (plus 1e-9) of the oracle's FP64 dS.
 """
 import numpy as np
 import pytest
@@ -185,20 +189,26 @@ def run_trace_pair(o, d, levels, steps, n_blocks, seed, **kw):
     return ref, got, stats
 
 
+def dS_close(r_dS, g, k, tol):
+    """|oracle dS - device dS| within tol (FP64), or within the stage's bound (mixed)."""
+    return abs(r_dS - g["dS"][k]) <= float(g["dS_bound"][k]) + tol * max(1.0, abs(r_dS))
+
+
 def compare_traces(ref, got, stats, tol=1e-9):
     assert len(ref) == len(got)
     for i, (r, g) in enumerate(zip(ref, got)):
         assert (r.slice1, r.ptcl, r.accepted, r.stages_passed) == (
             int(g["slice1"]), int(g["ptcl"]), int(g["accepted"]), int(g["stages_passed"])), i
         for k in range(8):
-            assert abs(r.dS[k] - g["dS"][k]) <= tol * max(1.0, abs(r.dS[k])), (i, k, r.dS[k], g["dS"][k])
+            assert dS_close(r.dS[k], g, k, tol), (i, k, r.dS[k], g["dS"][k], g["dS_bound"][k])
     assert stats["moves"] == len(ref)
     assert stats["accepted"] == sum(r.accepted for r in ref)
     assert stats["status"] == 0
 
 
+@pytest.mark.parametrize("precision", [P.FP64, P.MIXED])
 @pytest.mark.parametrize("cluster", [1, 4])
-def test_bisection_trace_david(tmp_path, cluster):
+def test_bisection_trace_david(tmp_path, cluster, precision):
     cfg, tau, box, dm = lj_case(tmp_path)
     n, slices = cfg["N"], cfg["M"] + 1
     pa = O.PairAction.from_dm(dm, tau, 0)
@@ -209,13 +219,15 @@ def test_bisection_trace_david(tmp_path, cluster):
     d = P.PathData(n, slices, box, tau, W.HE4_LAMBDA, 0)
     d.set_path(start)
     d.pa_david_from_dm(dm, 0)
-    ref, got, stats = run_trace_pair(o, d, 3, 2, 400, 99, cluster_ctas=cluster, threads_per_cta=128)
+    ref, got, stats = run_trace_pair(o, d, 3, 2, 400, 99, cluster_ctas=cluster, threads_per_cta=128,
+                                     precision=precision)
     compare_traces(ref, got, stats)
     assert np.max(np.abs(d.get_path(P.OLDMODE) - o.get_path(0))) < 1e-9
     assert np.array_equal(d.get_path(P.OLDMODE), d.get_path(P.NEWMODE))
 
 
-def test_bisection_trace_tricubic():
+@pytest.mark.parametrize("precision", [P.FP64, P.MIXED])
+def test_bisection_trace_tricubic(precision):
     cfg, tau, box, tabs = tricubic_case()
     qg, yg, tg, umat, dumat, pg, pot = tabs
     n, slices = cfg["N"], cfg["M"] + 1
@@ -225,14 +237,16 @@ def test_bisection_trace_tricubic():
     d = P.PathData(n, slices, box, tau, W.HE4_LAMBDA, 0)
     d.set_path(o.get_path(0))
     d.pa_tricubic(qg, yg, tg, tau, umat, dumat, pg, pot)
-    ref, got, stats = run_trace_pair(o, d, 3, 1, 300, 7, cluster_ctas=2, threads_per_cta=256)
+    ref, got, stats = run_trace_pair(o, d, 3, 1, 300, 7, cluster_ctas=2, threads_per_cta=256, precision=precision)
     compare_traces(ref, got, stats)
     assert np.max(np.abs(d.get_path(P.OLDMODE) - o.get_path(0))) < 1e-9
 
 
-def test_bisection_mixed_shadow_dS_error(tmp_path):
-    """Mixed path (FP32 pair terms) with the FP64 terms evaluated alongside:
-    per-stage dS relative error and the accept-flip rate."""
+@pytest.mark.parametrize("guard", [True, False])
+def test_bisection_mixed_shadow_dS_error(tmp_path, guard):
+    """Mixed path with the FP64 sums evaluated alongside.  Every stage's mixed
+    dS lies within its reported bound of the FP64 dS (the bound is rigorous);
+    guarded, no decision differs from the FP64 sums' (flips == 0)."""
     cfg, tau, box, dm = lj_case(tmp_path)
     n, slices = cfg["N"], cfg["M"] + 1
     o = O.System(n, slices, box, tau, W.HE4_LAMBDA, 0)
@@ -240,13 +254,18 @@ def test_bisection_mixed_shadow_dS_error(tmp_path):
     d = P.PathData(n, slices, box, tau, W.HE4_LAMBDA, 0)
     d.set_path(o.get_path(0))
     d.pa_david_from_dm(dm, 0)
-    bb = P.BisectionBlock(d, 3, 1, precision=P.MIXED, shadow=True, cluster_ctas=1, threads_per_cta=128)
+    bb = P.BisectionBlock(d, 3, 1, precision=P.MIXED, shadow=True, cluster_ctas=1, threads_per_cta=128, guard=guard)
     bb.seed(3)
     rec, stats = bb.MakeMoves(500)
     mask = rec["dS_shadow"] != 0.0
-    rel = np.abs(rec["dS"][mask] - rec["dS_shadow"][mask]) / np.maximum(np.abs(rec["dS_shadow"][mask]), 1e-3)
-    assert np.median(rel) < 1e-5
-    assert stats["flips"] <= 0.01 * stats["stages_attempted"] + 1
+    err = np.abs(rec["dS"][mask] - rec["dS_shadow"][mask])
+    assert np.all(err <= rec["dS_bound"][mask].astype(np.float64) + 1e-12), np.max(err - rec["dS_bound"][mask])
+    rel = err / np.maximum(np.abs(rec["dS_shadow"][mask]), 1e-3)
+    assert np.median(rel) < 1e-6
+    if guard:
+        assert stats["flips"] == 0
+    else:
+        assert stats["reevaluated"] == 0 and np.all(rec["reevaluated"] == 0)
 
 
 def compare_window_traces(ref, got, stats, tol=1e-9):
@@ -258,13 +277,14 @@ def compare_window_traces(ref, got, stats, tol=1e-9):
         if r.slice1 >= 0:
             n_moves += 1
         for k in range(8):
-            assert abs(r.dS[k] - g["dS"][k]) <= tol * max(1.0, abs(r.dS[k])), (i, k, r.dS[k], g["dS"][k])
+            assert dS_close(r.dS[k], g, k, tol), (i, k, r.dS[k], g["dS"][k], g["dS_bound"][k])
     assert stats["moves"] == n_moves
     assert stats["status"] == 0
 
 
+@pytest.mark.parametrize("precision", [P.FP64, P.MIXED])
 @pytest.mark.parametrize("cluster", [1, 2])
-def test_bisection_trace_windows_david(tmp_path, cluster):
+def test_bisection_trace_windows_david(tmp_path, cluster, precision):
     """Concurrent-window schedule (time-slice parallel) against the oracle's
     sequential replay of the same rounds."""
     cfg, tau, box, dm = lj_case(tmp_path)
@@ -278,7 +298,8 @@ def test_bisection_trace_windows_david(tmp_path, cluster):
     o.bisection_config(3, 2)
     o.rng_seed(41)
     ref = o.run_windows(60)
-    bb = P.BisectionBlock(d, 3, 2, cluster_ctas=cluster, threads_per_cta=128, schedule=P.WINDOWS)
+    bb = P.BisectionBlock(d, 3, 2, cluster_ctas=cluster, threads_per_cta=128, schedule=P.WINDOWS,
+                          precision=precision)
     assert bb.windows == 5
     bb.seed(41)
     got, stats = bb.MakeMoves(60)
@@ -286,7 +307,8 @@ def test_bisection_trace_windows_david(tmp_path, cluster):
     assert np.max(np.abs(d.get_path(P.OLDMODE) - o.get_path(0))) < 1e-9
 
 
-def test_bisection_trace_windows_tricubic():
+@pytest.mark.parametrize("precision", [P.FP64, P.MIXED])
+def test_bisection_trace_windows_tricubic(precision):
     cfg, tau, box, tabs = tricubic_case()
     qg, yg, tg, umat, dumat, pg, pot = tabs
     n, slices = cfg["N"], cfg["M"] + 1
@@ -299,7 +321,7 @@ def test_bisection_trace_windows_tricubic():
     o.bisection_config(3, 1)
     o.rng_seed(47)
     ref = o.run_windows(50)
-    bb = P.BisectionBlock(d, 3, 1, cluster_ctas=4, threads_per_cta=256, schedule=P.WINDOWS, precision=P.FP64)
+    bb = P.BisectionBlock(d, 3, 1, cluster_ctas=4, threads_per_cta=256, schedule=P.WINDOWS, precision=precision)
     bb.seed(47)
     got, stats = bb.MakeMoves(50)
     compare_window_traces(ref, got, stats)
