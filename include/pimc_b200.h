@@ -56,6 +56,19 @@ extern "C" {
 #define PIMC_FP64 0   /* plain FP64 evaluation */
 #define PIMC_MIXED 1  /* FP32 pair terms and phases, FP64 accumulation and Metropolis */
 
+/* Guard of the mixed path (pimc_bisection_desc.mixed_guard, pimc_batch_set_guard).
+ * Every mixed stage sum carries a rigorous bound E on its distance from the
+ * FP64 sums.  DECISION: a stage whose Metropolis decision could come out
+ * differently on the FP64 sums (|logAcceptProb - log u| <= E plus the
+ * previous stage's bound) is evaluated again in FP64 and decided on those
+ * sums, so decisions, trace and path are the FP64 path's.  RELATIVE: as
+ * DECISION, and also every stage with E > 1e-6 |dS| is decided on its FP64
+ * sums, so every dS a decision uses is within 1e-6 relative of FP64's.
+ * NONE: the mixed sums alone. */
+#define PIMC_GUARD_DECISION 0
+#define PIMC_GUARD_NONE 1
+#define PIMC_GUARD_RELATIVE 2
+
 #define PIMC_ACTION_SHORTRANGE 0
 #define PIMC_ACTION_KINETIC 1
 #define PIMC_ACTION_LONGRANGE 2
@@ -253,13 +266,10 @@ typedef struct pimc_bisection_desc {
    * a particle with more partners uses all of them. */
   double neighbor_skin;
   int neighbor_max;
-  /* PIMC_MIXED only.  0 (default): every stage whose Metropolis decision
-   * could come out differently on the FP64 sums — |logAcceptProb - log u|
-   * within the mixed sums' rigorous error bound — is evaluated again in FP64
-   * and decided on those sums, so the decisions, the trace and the path are
-   * the FP64 path's; stats.reevaluated counts those stages.  1: decide on the
-   * mixed sums alone. */
-  int mixed_unguarded;
+  /* PIMC_MIXED only: PIMC_GUARD_DECISION (0, default), PIMC_GUARD_NONE or
+   * PIMC_GUARD_RELATIVE; stats.reevaluated counts the stages decided on
+   * their FP64 re-evaluation. */
+  int mixed_guard;
   /* Tries of the table-staging wait (a bounded spin on an mbarrier) before a
    * launch gives up with PIMC_E_CAP; 0 = 2^22.  test_wait > 0 additionally
    * waits that many tries on a barrier that nothing arrives at, after the
@@ -376,10 +386,9 @@ int pimc_batch_run_async(pimc_batch *b, int n_blocks);
 int pimc_batch_autotune(pimc_batch *b, int n_blocks, int *threads_per_cta, int *ctas, int *max_split,
                         double *split_ratio, double *ms);
 int pimc_batch_get_stats(pimc_batch *b, int chain /* -1: all */, pimc_bisection_stats *stats);
-/* PIMC_MIXED: on (1, the default) decides a stage on its FP64 re-evaluation
- * whenever the mixed sums' error bound could change the decision, as
- * pimc_bisection_desc.mixed_unguarded = 0; off (0): the mixed sums alone. */
-int pimc_batch_set_guard(pimc_batch *b, int on);
+/* PIMC_MIXED: the guard of the batch's chains, PIMC_GUARD_DECISION (the
+ * default), PIMC_GUARD_NONE or PIMC_GUARD_RELATIVE. */
+int pimc_batch_set_guard(pimc_batch *b, int guard);
 int pimc_batch_get_path(pimc_batch *b, int chain, double *path);
 int pimc_batch_synchronize(pimc_batch *b);
 /* The batch's CUDA stream (cudaStream_t) for event timing and ordering. */

@@ -35,6 +35,16 @@ FP64, MIXED = 0, 1
 ACTION_SHORTRANGE, ACTION_KINETIC, ACTION_LONGRANGE, ACTION_DAVIDLONGRANGE = 0, 1, 2, 3
 GRID_LINEAR, GRID_LOG = 0, 1
 SEQUENTIAL, WINDOWS, PROPOSALS = 0, 1, 2
+GUARD_DECISION, GUARD_NONE, GUARD_RELATIVE = 0, 1, 2
+
+
+def guard_value(guard):
+    """PIMC_GUARD_* of a guard argument: one of the constants, or True (decision) / False (none)."""
+    if guard is True:
+        return GUARD_DECISION
+    if guard is False:
+        return GUARD_NONE
+    return int(guard)
 
 STATUS = {
     0: "ok", 1: "invalid argument", 2: "CUDA error", 3: "non-finite action", 4: "index out of range",
@@ -76,7 +86,7 @@ class BisectionDesc(C.Structure):
         ("schedule", C.c_int),
         ("neighbor_skin", C.c_double),
         ("neighbor_max", C.c_int),
-        ("mixed_unguarded", C.c_int),
+        ("mixed_guard", C.c_int),
         ("wait_cap", C.c_int),
         ("test_wait", C.c_int),
     ]
@@ -524,7 +534,8 @@ class BisectionBlock:
 
     def __init__(self, path_data: PathData, num_levels, steps_per_block=1, shortrange_at_higher_levels=True,
                  precision=FP64, shadow=False, cluster_ctas=0, threads_per_cta=0, schedule=SEQUENTIAL,
-                 use_longrange=False, neighbor_skin=0.0, neighbor_max=0, guard=True, wait_cap=0, test_wait=0):
+                 use_longrange=False, neighbor_skin=0.0, neighbor_max=0, guard=GUARD_DECISION, wait_cap=0,
+                 test_wait=0):
         self.PathData = path_data
         d = BisectionDesc()
         d.num_levels = num_levels
@@ -538,7 +549,7 @@ class BisectionBlock:
         d.schedule = schedule
         d.neighbor_skin = neighbor_skin
         d.neighbor_max = neighbor_max
-        d.mixed_unguarded = 0 if guard else 1
+        d.mixed_guard = guard_value(guard)
         d.wait_cap = wait_cap
         d.test_wait = test_wait
         self.desc = d
@@ -649,9 +660,9 @@ class BatchChains:
     def stream(self):
         return _lib.pimc_batch_stream(self.h)
 
-    def set_guard(self, on=True):
-        """Mixed precision: decide near-threshold stages on their FP64 re-evaluation (on by default)."""
-        self._check(_lib.pimc_batch_set_guard(self.h, 1 if on else 0), "batch_set_guard")
+    def set_guard(self, guard=GUARD_DECISION):
+        """Mixed precision: GUARD_DECISION (default), GUARD_NONE or GUARD_RELATIVE (or True / False)."""
+        self._check(_lib.pimc_batch_set_guard(self.h, guard_value(guard)), "batch_set_guard")
 
     def autotune(self, n_blocks=1):
         """Pick threads_per_cta and the CTA count by timing; chains keep their state."""

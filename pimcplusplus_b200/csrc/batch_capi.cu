@@ -220,7 +220,7 @@ int pimc_batch_create(int device, int n_chains, const pimc_chain_desc *chains, p
     j.steps_per_block = c.steps_per_block;
     j.sr_higher = 1;
     j.concurrent = 0;
-    j.guard = 1;
+    j.guard = guard_mode(PIMC_GUARD_DECISION);
     cs[i].seed = c.seed;
     cs[i].stream = kStreamLocal;
   }
@@ -502,11 +502,11 @@ int pimc_batch_get_stats(pimc_batch *b, int chain, pimc_bisection_stats *stats) 
   return PIMC_OK;
 }
 
-int pimc_batch_set_guard(pimc_batch *b, int on) {
-  if (!b || (on != 0 && on != 1)) return PIMC_E_ARG;
+int pimc_batch_set_guard(pimc_batch *b, int guard) {
+  if (!b || guard < 0 || guard > 2) return PIMC_E_ARG;
   BCK(cudaSetDevice(b->device));
   BCK(cudaStreamSynchronize(b->stream));
-  for (auto &j : b->jobs) j.guard = on;
+  for (auto &j : b->jobs) j.guard = guard_mode(guard);
   BCK(cudaMemcpy(b->d_jobs, b->jobs.data(), b->jobs.size() * sizeof(BisectionArgs), cudaMemcpyHostToDevice));
   drop_graph(b);
   b->cfg_version++;

@@ -952,7 +952,9 @@ __device__ void run_job(const BisectionArgs &a, ChainState *cs, int window, unsi
           if (!exact && a.guard) {
             const double logAcceptProb = logsr - currActionChange + prevDS;
             const double E = eb + prevE + 1e-12 * (fabs(so) + fabs(sn));
-            if (!(fabs(logAcceptProb - logu) > E) && isfinite(currActionChange)) {
+            // relative gate: |dS_mixed - dS_64| <= eb <= 1e-6 |dS_64| needs eb (1 + 1e-6) <= 1e-6 |dS_mixed|
+            const bool rel_fail = a.guard == kGuardRelative && !(eb * (1.0 + 1e-6) <= 1e-6 * fabs(currActionChange));
+            if ((rel_fail || !(fabs(logAcceptProb - logu) > E)) && isfinite(currActionChange)) {
               if (lane == 0) {
                 S.s_need[0] = 1;
                 S.s_need[1] = prevE > 0.0 ? 1 : 0;

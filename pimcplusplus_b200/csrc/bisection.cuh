@@ -35,9 +35,10 @@ struct BisectionArgs {
   const double4 *nbr_cb;
   const int *nbr_cnt, *nbr_idx;
   int *nbr_dirty;
-  // Mixed path: 1 = decide on the FP64 re-evaluation of a stage whenever the
-  // decision could differ from the FP64 sums' within the mixed sums' error
-  // bound (decisions identical to the FP64 path's); 0 = the mixed sums alone.
+  // Mixed path: kGuardOff, kGuardDecision (decide on the FP64 re-evaluation
+  // of a stage whenever the decision could differ from the FP64 sums' within
+  // the mixed sums' error bound) or kGuardRelative (also when the bound
+  // exceeds 1e-6 |dS|).
   int guard;
   // Tries of the table-staging wait before it gives up with PIMC_E_CAP;
   // test_wait > 0 also waits that many tries on a barrier nothing arrives at
@@ -49,6 +50,12 @@ struct BisectionArgs {
 // current path when *dirty is set, then *dirty cleared.
 cudaError_t launch_nbr_rebuild(cudaStream_t st, const double *path, const DevSystem &sys, double range, double skin,
                                int kmax, double4 *cb, int *cnt, int *idx, int *dirty);
+
+constexpr int kGuardOff = 0, kGuardDecision = 1, kGuardRelative = 2;
+// The kernel's guard mode of a PIMC_GUARD_* value.
+inline int guard_mode(int pimc_guard) {
+  return pimc_guard == PIMC_GUARD_NONE ? kGuardOff : pimc_guard == PIMC_GUARD_RELATIVE ? kGuardRelative : kGuardDecision;
+}
 
 cudaError_t bisection_occupancy(const BisectionArgs &a, int precision, int shadow, int cluster_ctas, int threads,
                                 int *max_clusters);

@@ -661,7 +661,7 @@ int pimc_bisection_setup(pimc_context *ctx, const pimc_bisection_desc *d) {
   }
   if (int rc2 = pa_levels_ok(ctx, d->num_levels)) return rc2;
   if (d->neighbor_skin < 0.0 || d->neighbor_max < 0) return fail(ctx, PIMC_E_ARG, "bad neighbour-list settings");
-  if ((d->mixed_unguarded != 0 && d->mixed_unguarded != 1) || d->wait_cap < 0 || d->test_wait < 0)
+  if (d->mixed_guard < 0 || d->mixed_guard > 2 || d->wait_cap < 0 || d->test_wait < 0)
     return fail(ctx, PIMC_E_ARG, "bad guard / wait settings");
   if (d->neighbor_skin > 0.0) {
     if (ctx->pa.kind != PA_DAVID) return fail(ctx, PIMC_E_ARG, "neighbour lists need a DavidPA table");
@@ -760,7 +760,7 @@ static int run_bisection(pimc_context *ctx, int n_blocks, pimc_move_record *devi
   a.nbr_cnt = ctx->d_nbr_cnt;
   a.nbr_idx = ctx->d_nbr_idx;
   a.nbr_dirty = ctx->d_nbr_dirty;
-  a.guard = ctx->bis.mixed_unguarded ? 0 : 1;
+  a.guard = guard_mode(ctx->bis.mixed_guard);
   a.wait_cap = ctx->bis.wait_cap;
   a.test_wait = ctx->bis.test_wait;
   if (a.use_lr && !ctx->rhok_valid) {  // PathClass::UpdateRho_ks() of the current OLD path
