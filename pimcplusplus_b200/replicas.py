@@ -27,10 +27,29 @@ from __future__ import annotations
 
 import numpy as np
 
-__all__ = ["ReplicaBlock", "ENERGY_TERMS", "MOVE_COUNTERS"]
+__all__ = ["ReplicaBlock", "ENERGY_TERMS", "MOVE_COUNTERS", "chain_cost", "shard_by_cost"]
 
 ENERGY_TERMS = ("kinetic", "du_short", "du_long", "v_short", "v_long", "total")
 MOVE_COUNTERS = ("moves", "accepted", "stages_attempted", "pair_evals")
+
+
+def chain_cost(chain):
+    """Estimated cost of a chain, N^2 M 2^L: N particles moved per sweep, each
+    move's stages summing N partners over links that grow as 2^L, M slices
+    per sweep.  `chain` is a dict with N, slices (M + 1) and num_levels."""
+    return float(chain["N"]) ** 2 * (chain["slices"] - 1) * (1 << chain["num_levels"])
+
+
+def shard_by_cost(chains, rank, world, cost=chain_cost):
+    """Indices of the chains rank `rank` of `world` runs: all chains sorted by
+    cost, largest first (ties by index), dealt round-robin, so every rank gets
+    a similar share of the work and the shards partition the set.  Each rank
+    runs its shard in one batched launch; nothing is exchanged between ranks
+    until the block's counters are pooled (one all-reduce)."""
+    if not 0 <= rank < world:
+        raise ValueError("rank must be in [0, world)")
+    order = sorted(range(len(chains)), key=lambda i: (-cost(chains[i]), i))
+    return sorted(order[rank::world])
 
 
 class ReplicaBlock:
