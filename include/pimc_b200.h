@@ -454,11 +454,11 @@ int pimc_gofr_reset(pimc_context *ctx);
  * No counterpart in the reference: the read-bandwidth ceiling used to state
  * the bisection kernels' roofline when their tables and path are
  * L2-resident.  Reads `bytes` (1 MiB .. 8 GiB) of a fresh device buffer with
- * 16-byte loads through L2, once untimed, then `reps` times timed with CUDA
- * events; *gbs = bytes * reps / time.  Below the 126 MB L2 this is the L2
- * read bandwidth, far above it the HBM read bandwidth.  Allocates and frees
- * its buffer; synchronous. */
-int pimc_read_bandwidth(int device, size_t bytes, int reps, double *gbs);
+ * 16-byte loads through L2, once untimed, then `reps` launches of `passes`
+ * passes each (1..1024) timed with CUDA events; *gbs = bytes * passes * reps
+ * / time.  Below the 126 MB L2 this is the L2 read bandwidth, far above it
+ * the HBM read bandwidth.  Allocates and frees its buffer; synchronous. */
+int pimc_read_bandwidth(int device, size_t bytes, int passes, int reps, double *gbs);
 
 /* ---- allocation-free ShortRange SingleAction ----
  * No counterpart in the reference: it exists for callers that cannot call

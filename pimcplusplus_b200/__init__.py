@@ -198,7 +198,7 @@ _SIGS = {
                                  C.POINTER(_d)]),
     "pimc_batch_get_stats": (_i, [_p, _i, C.POINTER(BisectionStats)]),
     "pimc_batch_set_guard": (_i, [_p, _i]),
-    "pimc_read_bandwidth": (_i, [_i, C.c_size_t, _i, _dp]),
+    "pimc_read_bandwidth": (_i, [_i, C.c_size_t, _i, _i, _dp]),
     "pimc_batch_get_path": (_i, [_p, _i, _dp]),
     "pimc_batch_synchronize": (_i, [_p]),
     "pimc_batch_stream": (_p, [_p]),
@@ -713,11 +713,11 @@ def coulomb_breakup(box, z1z2, smallest_beta, num_levels, num_knots, kcutoff, kv
     return out
 
 
-def read_bandwidth(device=0, nbytes=64 << 20, reps=50):
+def read_bandwidth(device=0, nbytes=64 << 20, passes=16, reps=10):
     """GB/s of 16-byte loads through L2 over an nbytes buffer (L2 read
     bandwidth below 126 MB, HBM read bandwidth well above it)."""
     v = C.c_double()
-    rc = _lib.pimc_read_bandwidth(device, nbytes, reps, C.byref(v))
+    rc = _lib.pimc_read_bandwidth(device, nbytes, passes, reps, C.byref(v))
     if rc:
         raise PimcError(rc, "read_bandwidth")
     return v.value
