@@ -248,7 +248,7 @@ class CpuChains:
         acc = sum(r[2] for r in res)
         dt = max(r[3] for r in res)
         return dict(value=evals / dt, moves_per_s=moves / dt, accepted_per_s=acc / dt, cores=self.cores,
-                    sample=f"{moves} moves of C2 (FP64 oracle, {self.cores} independent chain(s), {dt:.1f} s)")
+                    sample=f"{moves} C2 moves, FP64 oracle, {self.cores} chain(s), {dt:.1f} s")
 
     def close(self):
         if self.pool is not None:
@@ -575,50 +575,43 @@ def run_ours(args):
             "warmup": args.warmup, "ms_per_step": ms_h / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32 tables, f64 geometry+sums" if head_mixed else "f64",
             "data": "synthetic",
-            "config": {"workload": W_NAME, "value_leg": "mixed, relative guard" if head_mixed else "fp64",
-                       "moves_per_step": st_h["moves"] // world // args.steps, "schedule": args.schedule,
-                       "l2": "flushed between steps (256 MiB write outside the timed events)",
-                       "parallelism": f"replicas x{world}"},
-            "accepted_moves_per_s": st_h["accepted"] / (ms_h / 1000.0),
-            "fp64": _short(r64), "mixed_decision": _short(rd), "mixed_relative": _short(rr),
-            "mixed_decision_over_fp64": vdec / v64, "mixed_relative_over_fp64": vrel / v64,
+            "config": {"workload": "C2: 512 LJ He-4, rho 0.02186, T=1.5 K, M=128, tricubic 200x50x50, level 4, "
+                                   "1 chain", "value_leg": "mixed, relative guard" if head_mixed else "fp64",
+                       "schedule": args.schedule, "l2": "flushed between steps", "parallelism": f"replicas x{world}"},
+            # [pair evals/s, accepted moves/s] of the three C2 legs
+            "legs": {"fp64": _pair(r64), "mixed_decision": _pair(rd), "mixed_relative": _pair(rr)},
             "dS": {"flips": acc["decision"]["flips"] + acc["relative"]["flips"],
-                   "bound_holds": acc["decision"]["bound_holds"] and acc["relative"]["bound_holds"],
-                   "raw_relerr_med": acc["decision"]["raw_relerr"]["median"],
-                   "raw_relerr_p99": acc["decision"]["raw_relerr"]["p99"],
-                   "raw_relerr_max": acc["decision"]["raw_relerr"]["max"],
-                   "used_relerr_max_relative_guard": acc["relative"]["used_relerr_max"],
-                   "reeval_decision": acc["decision"]["reevaluated_per_stage"],
-                   "reeval_relative": acc["relative"]["reevaluated_per_stage"]},
+                   "bound_ok": acc["decision"]["bound_holds"] and acc["relative"]["bound_holds"],
+                   "raw_relerr_med_p99_max": [acc["decision"]["raw_relerr"][k] for k in ("median", "p99", "max")],
+                   "relative_guard_used_max": acc["relative"]["used_relerr_max"],
+                   "reeval_decision_relative": [acc["decision"]["reevaluated_per_stage"],
+                                                acc["relative"]["reevaluated_per_stage"]]},
             "e2e": {"value": e2e_evals / e2e_t if e2e_t else None, "unit": UNIT, "h2d_bytes_per_step": path_bytes,
                     "d2h_bytes_per_step": path_bytes + 48},
             "gpu_launches": launches["n"],
             "roofline": {"bound": "l2", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                         "traffic": traffic, "peak_kind": peak_kind, "l2_peak": l2_gbs,
-                         "l2_frac": achieved / l2_gbs, "bytes_per_eval": bpe,
-                         "kernel": "bisection_kernel<PA_TRICUBIC,%s>" % ("float" if head_mixed else "double")},
+                         "traffic": traffic, "peak_kind": peak_kind, "l2_peak": l2_gbs, "l2_frac": achieved / l2_gbs},
             "clocks": {k: clocks[k] for k in ("sm_mhz", "sm_max_mhz", "reasons")} if clocks else None,
         }
         if c1:
-            line["c1"] = {"fp64_sweeps_per_s": c1["fp64"]["sweeps_per_s"],
-                          "mixed_sweeps_per_s": c1["mixed"]["sweeps_per_s"],
-                          "gpu_time_1e4_sweeps_s": c1["fp64"]["time_1e4_sweeps_s"],
-                          "cpu_time_1e4_sweeps_s": c1.get("cpu_fp64_1core", {}).get("time_1e4_sweeps_s")}
+            line["c1"] = {"sweeps_s_fp64_mixed": [c1["fp64"]["sweeps_per_s"], c1["mixed"]["sweeps_per_s"]],
+                          "t_1e4_sweeps_gpu_cpu1": [c1["fp64"]["time_1e4_sweeps_s"],
+                                                    c1.get("cpu_fp64_1core", {}).get("time_1e4_sweeps_s")]}
         if c3:
-            line["c3"] = {k: c3[k] for k in ("batched_mixed_acc_per_s", "batched_fp64_acc_per_s",
-                                             "plain_fp64_acc_per_s", "batched_mixed_over_plain_fp64",
-                                             "batched_mixed_over_batched_fp64")}
+            line["c3"] = {"acc_s_batched_mixed_fp64_plain_fp64": [c3["batched_mixed_acc_per_s"],
+                                                                  c3["batched_fp64_acc_per_s"],
+                                                                  c3["plain_fp64_acc_per_s"]]}
         if c4:
-            line["c4"] = {"mixed_acc_per_s": c4["mixed"]["accepted_moves_per_s"],
-                          "fp64_acc_per_s": c4["fp64"]["accepted_moves_per_s"],
-                          "rhok_updates_per_s": c4["mixed"]["rhok_updates_per_s"]}
+            line["c4"] = {"acc_s_mixed_fp64": [c4["mixed"]["accepted_moves_per_s"], c4["fp64"]["accepted_moves_per_s"]],
+                          "rhok_upd_s": c4["mixed"]["rhok_updates_per_s"]}
         if c5:
-            line["c5"] = {"lists_mixed_acc_per_s": c5["neighbor_lists_mixed"]["accepted_moves_per_s"],
-                          "lists_fp64_acc_per_s": c5["neighbor_lists_fp64"]["accepted_moves_per_s"],
-                          "proposals_mixed_acc_per_s": c5["proposals_mixed"]["accepted_moves_per_s"]}
+            line["c5"] = {"acc_s_lists_mixed_fp64_prop": [c5["neighbor_lists_mixed"]["accepted_moves_per_s"],
+                                                          c5["neighbor_lists_fp64"]["accepted_moves_per_s"],
+                                                          c5["proposals_mixed"]["accepted_moves_per_s"]]}
         if cpu:
             line["cpu_baseline"] = {"value": cpu["value"], "unit": UNIT, "cores": cpu["cores"], "kind": "port",
                                     "sample": cpu["sample"]}
+        line = _rounded(line)
         detail["line"] = line
         print("bench-detail " + json.dumps(detail), file=sys.stderr, flush=True)
         if args.detail_out:
@@ -630,8 +623,19 @@ def run_ours(args):
         dist.destroy_process_group()
 
 
-def _short(r):
-    return {"evals_per_s": r["pair_evals_per_s"], "acc_moves_per_s": r["accepted_moves_per_s"]}
+def _pair(r):
+    return [r["pair_evals_per_s"], r["accepted_moves_per_s"]]
+
+
+def _rounded(x):
+    """Floats to 4 significant digits (the one stdout line stays short)."""
+    if isinstance(x, float):
+        return float(f"{x:.4g}")
+    if isinstance(x, dict):
+        return {k: _rounded(v) for k, v in x.items()}
+    if isinstance(x, list):
+        return [_rounded(v) for v in x]
+    return x
 
 
 def run_c1(args, P, timer, local, rank, agg, launches):
