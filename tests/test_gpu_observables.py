@@ -133,11 +133,18 @@ def blocked(x, nblocks):
     return b.mean(axis=0), b.std(axis=0, ddof=1) / np.sqrt(nblocks)
 
 
-def test_energy_and_gofr_within_2sigma_mixed_vs_oracle(tmp_path):
+@pytest.mark.parametrize("size", ["small", "C1"])
+def test_energy_and_gofr_within_2sigma_mixed_vs_oracle(tmp_path, size):
     """An independent mixed-precision device chain (concurrent windows, own
     seed) and the FP64 oracle's sequential chain sample the same
-    distribution: energy and g(r) agree within 2 combined sigma."""
-    cfg, tau, box, dm = small_system(tmp_path)
+    distribution: energy and g(r) agree within 2 combined sigma.  Sizes: 32
+    atoms, M = 20, level 2; and C1 (64 atoms, M = 40, T = 2 K, level 3)."""
+    if size == "C1":
+        cfg, tau, box, dm = small_system(tmp_path, n=64, m=40, temp=2.0, levels=3)
+        burn, sweeps, nb = 100, 800, 10
+    else:
+        cfg, tau, box, dm = small_system(tmp_path)
+        burn, sweeps, nb = 150, 1200, 12
     n, slices, L = cfg["N"], cfg["M"] + 1, cfg["levels"]
     windows = (slices - 1) >> L
     per_sweep = n * windows  # one sweep = N ceil(M / 2^L) bisection attempts
@@ -153,7 +160,6 @@ def test_energy_and_gofr_within_2sigma_mixed_vs_oracle(tmp_path):
     d.gofr_setup(0.0, box[0] / 2, 41)
     bb = P.BisectionBlock(d, L, n, precision=P.MIXED, cluster_ctas=1, threads_per_cta=128, schedule=P.WINDOWS)
     bb.seed(202)
-    burn, sweeps, nb = 150, 1200, 12
     e_o, e_d, g_o, g_d = [], [], [], []
     for sw in range(burn + sweeps):
         o.run_bisection(1)
