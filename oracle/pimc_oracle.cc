@@ -1319,7 +1319,14 @@ struct OracleSystem {
       prevActionChange = currActionChange;
     }
     if (toAccept) {
-      AcceptCopy(slice1, slice2, ptcl);
+      // Concurrent windows share their end slices with the neighbouring
+      // windows; those slices never move, and the schedule leaves them as
+      // they are (the reference's PutInBoxFast of an unmoved end slice only
+      // re-wraps its coordinates).
+      if (window_mode)
+        AcceptCopy(slice1 + 1, slice2 - 1, ptcl);
+      else
+        AcceptCopy(slice1, slice2, ptcl);
       rec->accepted = 1;
     } else {
       RejectCopy(slice1, slice2, ptcl);
@@ -1352,6 +1359,7 @@ struct OracleSystem {
   // (PIMC_SCHEDULE_PROPOSALS) every step of a window is slot 0, 1, ..., P-1
   // making one move each in that order, slot p drawing from Local stream
   // 0x100 + 64 p + w; records [window][step][slot].
+  bool window_mode = false;  // MakeMove inside a concurrent-window round
   void MakeRound(OracleMoveRecord *recs, int P = 1) {
     const int span = 1 << NumLevels;
     const int W = std::min((NumSlices - 1) >> NumLevels, 64);
@@ -1371,7 +1379,9 @@ struct OracleSystem {
       for (int st = 0; st < StepsPerBlock; st++)
         for (int p = 0; p < P; p++) {
           std::swap(rng, wrng[(size_t)p * 64 + w]);
+          window_mode = true;
           MakeMove(slice1, slice1 + span, &r[(size_t)st * P + p]);
+          window_mode = false;
           std::swap(rng, wrng[(size_t)p * 64 + w]);
         }
     }

@@ -1090,8 +1090,11 @@ __device__ void run_job(const BisectionArgs &a, ChainState *cs, int window, unsi
           __stcg(p2, rn);
         }
       }
+      // With concurrent windows only the interior slices: the end slices are
+      // shared with the neighbouring windows and never move, and boxing them
+      // here would race with the neighbour's read of the same slice.
       if (write_path)
-        for (int rel = tid; rel <= span; rel += G.size) {
+        for (int rel = (a.concurrent ? 1 : 0) + tid; rel <= (a.concurrent ? span - 1 : span); rel += G.size) {
           double v[3] = {win_new[cur][rel][0], win_new[cur][rel][1], win_new[cur][rel][2]};
           put_in_box_fast(v, sys);
           double *q = path + ((size_t)(slice1 + rel) * N + mptcl) * 3;
