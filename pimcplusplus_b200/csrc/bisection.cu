@@ -197,8 +197,9 @@ __device__ __forceinline__ double2 rho_new_k(double2 ro, const double *kv, const
 }
 
 // OLD and NEW action sums of one stage level over this CTA's share of the
-// (partner, link) items, plus the moved particle's kinetic links on cluster
-// rank 0.  Partner positions are read once and serve both copies.
+// (partner, link) items (the moved particle's kinetic links are summed by
+// the sampler warp, kinetic_sums).  Partner positions are read once and
+// serve both copies.
 //  * R = double: the FP64 path; SHADOW adds the mixed-path sums alongside.
 //  * R = float, the mixed path: FP64 geometry, FP32 table arithmetic
 //    (pa_U_mixed), each term two-sum accumulated into FP64, and eb, a bound
@@ -242,29 +243,6 @@ __device__ __forceinline__ StageSums stage_sums(const BisectionArgs &a, const do
       if (SHADOW) (is_new ? sn2 : so2) += pa_U_mixed<KIND>(a.pa, dg32, g, lv, part, nparts).v;
     }
   };
-  if (rank == 0 && sys.lambda != 0.0) {  // KineticClass::SingleAction on the moved particle (FP64 in both paths)
-    const double levelTau = sys.tau * (1 << lv);
-    const double F = 1.0 / (4.0 * sys.lambda * levelTau);
-    for (int k = etid; k < nlinks; k += ethreads) {
-      double vo[3], vn[3];
-      for (int i = 0; i < 3; i++) {
-        vo[i] = w_old[k * skip + skip][i] - w_old[k * skip][i];
-        vn[i] = w_new[k * skip + skip][i] - w_new[k * skip][i];
-      }
-      put_in_box(vo, sys);
-      put_in_box(vn, sys);
-      const double ko = kinetic_link(vo, F, sys.num_images, sys), kn = kinetic_link(vn, F, sys.num_images, sys);
-      if (MIX) {
-        two_sum_add(so, co, ko);
-        two_sum_add(sn, cn, kn);
-      } else {
-        so += ko;
-        sn += kn;
-      }
-      so2 += ko;
-      sn2 += kn;
-    }
-  }
   if (lv == 0 || a.sr_higher) {  // ShortRangeClass::SingleAction over partners x links
     // partners: all others (plist null, np = N - 1) or the moved particle's
     // neighbour list (np entries, ascending)
@@ -397,6 +375,34 @@ __device__ __forceinline__ StageSums stage_sums(const BisectionArgs &a, const do
   r.so2 = so2;
   r.sn2 = sn2;
   return r;
+}
+
+// KineticClass::SingleAction (KineticClass.cc:33-90) of the moved particle's
+// links at one level, OLD and NEW, by one full warp (a link per lane, a
+// fixed shuffle tree), FP64 on both paths.  The sampler warp computes it
+// while the other warps evaluate the pair terms, so no evaluating thread
+// starts its partner loads late.  The sums are identical in every lane.
+__device__ __forceinline__ double2 kinetic_sums(const double (*w_old)[3], const double (*w_new)[3], int num_levels,
+                                                int lv, const DevSystem &sys, int lane) {
+  double so = 0.0, sn = 0.0;
+  if (sys.lambda != 0.0) {
+    const int skip = 1 << lv;
+    const int nlinks = (1 << num_levels) >> lv;
+    const double levelTau = sys.tau * (1 << lv);
+    const double F = 1.0 / (4.0 * sys.lambda * levelTau);
+    for (int k = lane; k < nlinks; k += 32) {
+      double vo[3], vn[3];
+      for (int i = 0; i < 3; i++) {
+        vo[i] = w_old[k * skip + skip][i] - w_old[k * skip][i];
+        vn[i] = w_new[k * skip + skip][i] - w_new[k * skip][i];
+      }
+      put_in_box(vo, sys);
+      put_in_box(vn, sys);
+      so += kinetic_link(vo, F, sys.num_images, sys);
+      sn += kinetic_link(vn, F, sys.num_images, sys);
+    }
+  }
+  return make_double2(warp_sum(so), warp_sum(sn));
 }
 
 // The mixed path's FP64 re-evaluation of a stage (and, with need_prev, of the
@@ -911,6 +917,17 @@ __device__ void run_job(const BisectionArgs &a, ChainState *cs, int window, unsi
             }
           }
           if (lane < kRed) sh_red[warp][lane] = 0.0;
+          if (warp == sampler && erank == 0) {
+            // the moved particle's kinetic links, once per evaluation group
+            const double2 k = kinetic_sums(w_old, w_new, L, level, sys, lane);
+            __syncwarp();
+            if (lane == 0) {
+              sh_red[warp][0] = k.x;
+              sh_red[warp][1] = k.y;
+              sh_red[warp][3] = k.x;
+              sh_red[warp][4] = k.y;
+            }
+          }
         }
         // Counted as the reference performs them: OLD + NEW of the stage's links.
         if (lead && (level == 0 || a.sr_higher)) c_pairs += 2ull * (unsigned long long)np * (span >> level);
@@ -1040,8 +1057,20 @@ __device__ void run_job(const BisectionArgs &a, ChainState *cs, int window, unsi
               sh_red[warp][3] = r3;
               sh_red[warp][4] = 0.0;
             }
-          } else if (lane < kRed) {
-            sh_red[warp][lane] = 0.0;
+          } else {
+            if (lane < kRed) sh_red[warp][lane] = 0.0;
+            if (warp == sampler && erank == 0) {  // the kinetic links, as in the first pass
+              const double2 k = kinetic_sums(w_old, w_new, L, level, sys, lane);
+              const double2 kp = need_prev ? kinetic_sums(w_old, w_new, L, level + 1, sys, lane)
+                                           : make_double2(0.0, 0.0);
+              __syncwarp();
+              if (lane == 0) {
+                sh_red[warp][0] = k.x;
+                sh_red[warp][1] = k.y;
+                sh_red[warp][2] = kp.x;
+                sh_red[warp][3] = kp.y;
+              }
+            }
           }
           if (lead) c_reevals++;
           G.sync();

@@ -241,24 +241,33 @@ __device__ __forceinline__ void hermite4(R t, R h, R out[4]) {
   out[3] = h * (t * t * tm1);
 }
 
+// One node's 8 components by 256-bit read-only loads (sm_100: 32 bytes per
+// thread per load).  The tables are cudaMalloc'ed (256-byte aligned) and
+// every node starts at a multiple of 8 components, so a node is 64-byte
+// (FP64) / 32-byte (FP32) aligned.  A cell's scattered gather is bound by
+// the L1 requests of its loads, one per lane and load: 32-byte loads halve
+// them against 16-byte ones.
 template <typename R>
 struct Node8;
 template <>
 struct Node8<double> {
   double v[8];
   __device__ __forceinline__ void load(const double *p) {
-    const double2 *q = reinterpret_cast<const double2 *>(p);
-    double2 a = __ldg(q), b = __ldg(q + 1), c = __ldg(q + 2), d = __ldg(q + 3);
-    v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y; v[4] = c.x; v[5] = c.y; v[6] = d.x; v[7] = d.y;
+    asm("ld.global.nc.v4.f64 {%0, %1, %2, %3}, [%4];"
+        : "=d"(v[0]), "=d"(v[1]), "=d"(v[2]), "=d"(v[3])
+        : "l"(p));
+    asm("ld.global.nc.v4.f64 {%0, %1, %2, %3}, [%4];"
+        : "=d"(v[4]), "=d"(v[5]), "=d"(v[6]), "=d"(v[7])
+        : "l"(p + 4));
   }
 };
 template <>
 struct Node8<float> {
   float v[8];
   __device__ __forceinline__ void load(const float *p) {
-    const float4 *q = reinterpret_cast<const float4 *>(p);
-    float4 a = __ldg(q), b = __ldg(q + 1);
-    v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w; v[4] = b.x; v[5] = b.y; v[6] = b.z; v[7] = b.w;
+    asm("ld.global.nc.v8.f32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+        : "=f"(v[0]), "=f"(v[1]), "=f"(v[2]), "=f"(v[3]), "=f"(v[4]), "=f"(v[5]), "=f"(v[6]), "=f"(v[7])
+        : "l"(p));
   }
 };
 
