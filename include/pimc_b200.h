@@ -469,7 +469,9 @@ int pimc_read_bandwidth(int device, size_t bytes, int passes, int reps, double *
  * buffer is the caller's device memory — path [num_time_slices][N][3]
  * doubles, diag the (y, d2y) pairs of u_00 for this level [num_grid][2] on a
  * LINEAR grid {grid_start, grid_end, num_grid} (DavidPA, no off-diagonal
- * terms), out one double — and active/box are host arrays.  Its scratch is a
+ * terms: a table with off-diagonal u_kj terms gives a wrong value, not an
+ * error), out one double — and active/box are host arrays.  An empty link
+ * range (slice1 == slice2) writes 0.  Its scratch is a
  * fixed file-scope device array (2048 block partials, about 16 KB, held by
  * every GPU that loads the library until exit), so n_active * N * links must
  * not exceed 524288 (PIMC_E_ARG otherwise).  Calls share that scratch: calls

@@ -124,7 +124,24 @@ def quintic_coefficients(r, y):
     return np.vstack([c, c[-1:]]), bs
 
 
-def coulomb_breakup(box, z1z2, smallest_beta, num_levels, num_knots, kcut, kvecs):
+def normal_equation_svd(cnk, w, xk, tolerance=1.0e-16):
+    """OptimizedBreakupClass::DoBreakup (Common/Ewald/OptimizedBreakup.cc:196-290)
+    with every coefficient adjustable, as LongRangeClass calls it
+    (LongRangeClass.cc:601,611): A = sum_k w c c^T, b = sum_k w X_k c, the SVD
+    A = U S V^T, singular values below tolerance * S_max dropped, and
+    t = sum_i (U_i . b) / S_i V_i."""
+    A = (cnk * w) @ cnk.T
+    b = (cnk * w) @ xk
+    U, S, Vt = np.linalg.svd(A)
+    smax = S.max()
+    sinv = np.where(S < tolerance * smax, 0.0, 1.0 / np.where(S > 0, S, 1.0))
+    return Vt.T @ (sinv * (U.T @ b)), int(np.sum(sinv == 0.0))
+
+
+def coulomb_breakup(box, z1z2, smallest_beta, num_levels, num_knots, kcut, kvecs, solve="lstsq"):
+    """The breakup tables.  solve: "lstsq" (the weighted design matrix, the
+    library's approach) or "normal_svd" (the reference's own procedure,
+    normal_equation_svd)."""
     box = np.asarray(box, dtype=float)
     omega = float(np.prod(box))
     rc = 0.5 * box.min()
@@ -155,7 +172,11 @@ def coulomb_breakup(box, z1z2, smallest_beta, num_levels, num_knots, kcut, kvecs
             coef = 1.0 if job else beta
             xk = -4.0 * np.pi * coef * z1z2 / kp ** 2 * np.cos(kp * rc) / omega
             # the least-squares problem of DoBreakup, on the weighted design matrix
-            t = np.linalg.lstsq(Dw, sw * xk, rcond=1e-8)[0]
+            if solve == "normal_svd":
+                t, nsing = normal_equation_svd(cnk, w, xk)
+                out.setdefault("singular_dropped", []).append(nsing)
+            else:
+                t = np.linalg.lstsq(Dw, sw * xk, rcond=1e-8)[0]
             r0.append(float(t @ h0))
             ur = np.where(rgrid <= rc, t @ hr, coef * z1z2 / np.where(rgrid > 0, rgrid, 1.0))
             cq, bs = quintic_coefficients(rgrid, ur)

@@ -58,7 +58,11 @@ __device__ __forceinline__ double na_block_sum(double v, double *sh) {
   return r;
 }
 
-// Same terms and fixed reduction order as the context-based entry point.
+// The same terms as the context-based entry point, in a fixed reduction
+// order; the order is that entry point's only while both launch the same
+// number of blocks (it caps its grid at 8 blocks per SM, this kernel launches
+// one block per 256 terms), so large calls may differ from it in the last
+// bits.
 __global__ void __launch_bounds__(256) sr_single_noalloc_kernel(const double *__restrict__ path, DevSystem sys,
                                                                 DDavid<double> d, ActiveList act, int slice1,
                                                                 int skip, int nlinks, int level,
@@ -138,7 +142,11 @@ extern "C" int pimc_shortrange_single_noalloc(const double *path, int num_partic
   }
   const int skip = 1 << level;
   const int nlinks = (slice2 - slice1 + skip - 1) / skip;
-  if (nlinks == 0) return PIMC_E_ARG;
+  if (nlinks == 0) {
+    // an empty link range sums no term: 0, as pimc_single_action returns
+    return cudaMemsetAsync(out, 0, sizeof(double), static_cast<cudaStream_t>(stream)) == cudaSuccess ? PIMC_OK
+                                                                                                    : PIMC_E_CUDA;
+  }
   if (slice1 + nlinks * skip >= num_time_slices) return PIMC_E_ARG;
   const long long items = (long long)n_active * num_particles * nlinks;
   if (items > kNoAllocMaxTerms) return PIMC_E_ARG;  // beyond the fixed scratch (2048 blocks x 256 threads)

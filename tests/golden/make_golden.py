@@ -12,6 +12,7 @@ arrays the DavidPA reader must reproduce are stored:
   grid       (r_start, r_end, n), tau grid (tau_min, tau_max, ntau)
 
 Run: python tests/golden/make_golden.py [path/to/testcoul.dm]
+(default: $PIMC_REFERENCE_ROOT/PIMC++/examples/testcoul.dm)
 """
 from __future__ import annotations
 
@@ -21,7 +22,7 @@ import sys
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-DEFAULT_SRC = "/root/reference/PIMC++/examples/testcoul.dm"
+DEFAULT_SRC = os.path.join(os.environ.get("PIMC_REFERENCE_ROOT", ""), "PIMC++", "examples", "testcoul.dm")
 
 
 def parse(path):

@@ -10,7 +10,10 @@ from pimcplusplus_b200 import workloads as W
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 GOLDEN = os.path.join(ROOT, "tests", "golden")
-REF_TESTCOUL = "/root/reference/PIMC++/examples/testcoul.dm"
+# The reference's own fixture, read when the reference tree is available: its
+# root in PIMC_REFERENCE_ROOT (tests that need it skip otherwise).
+_REF_ROOT = os.environ.get("PIMC_REFERENCE_ROOT", "")
+REF_TESTCOUL = os.path.join(_REF_ROOT, "PIMC++", "examples", "testcoul.dm") if _REF_ROOT else ""
 
 
 def random_walk_path(n, slices, box, step, seed, far=0.0):

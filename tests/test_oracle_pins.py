@@ -45,7 +45,8 @@ def _check_reader_against_golden(pa):
         assert np.array_equal(pa.table(2, lev), du[lev])
 
 
-@pytest.mark.skipif(not os.path.exists(REF_TESTCOUL), reason="reference fixture not mounted")
+@pytest.mark.skipif(not REF_TESTCOUL or not os.path.exists(REF_TESTCOUL),
+                    reason="PIMC_REFERENCE_ROOT unset or the reference fixture not mounted")
 def test_dm_reader_on_reference_testcoul():
     pa = O.PairAction.from_dm(REF_TESTCOUL, 1.0 / 64, 2)
     _check_reader_against_golden(pa)

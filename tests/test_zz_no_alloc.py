@@ -37,12 +37,18 @@ def test_noalloc_matches_context_entry_point(tmp_path):
     d.pa_david_from_dm(dm, 0)
     tables = P.read_dm(dm, tau)
     assert tables["grid_type"] == P.GRID_LINEAR
+    # the entry point sums the diagonal u_00 column only: this table has no off-diagonal terms
+    assert not np.any(tables["ukj"][:, :, 2:])
 
     dev_path = torch.tensor(path, dtype=torch.float64, device="cuda:0").contiguous()
     out = torch.zeros(1, dtype=torch.float64, device="cuda:0")
     boxc = np.ascontiguousarray(box, dtype=np.float64)
     stream = torch.cuda.current_stream().cuda_stream
-    calls = [(3, 11, [7], 0), (8, 16, [2, 40, 5], 1)]
+    # two small calls; every particle over all 40 links (163840 terms, 640
+    # blocks: the cross-block reduction at scale); a small call after it (the
+    # counter the large call left); an empty link range (0, as the context path)
+    calls = [(3, 11, [7], 0), (8, 16, [2, 40, 5], 1), (0, 40, list(range(n)), 0), (8, 16, [2, 40, 5], 1),
+             (5, 5, [3], 0)]
     for (s1, s2, active, level) in calls:
         lev = level + tables["tau_pos"]
         diag = np.stack([tables["ukj"][lev][:, 1], tables["ukj_d2"][lev][:, 1]], axis=1)
@@ -56,7 +62,10 @@ def test_noalloc_matches_context_entry_point(tmp_path):
         torch.cuda.synchronize()
         got = float(out.item())
         ref = d.single_action(P.ACTION_SHORTRANGE, P.OLDMODE, s1, s2, act, level)
-        assert abs(got - ref) <= REL64 * abs(ref), (s1, s2, active, level, got, ref)
+        if s1 == s2:
+            assert got == 0.0 and ref == 0.0
+        else:
+            assert abs(got - ref) <= REL64 * abs(ref), (s1, s2, active, level, got, ref)
 
 
 def test_noalloc_rejects_oversized_call():
