@@ -259,7 +259,46 @@ __device__ __forceinline__ StageSums stage_sums(const BisectionArgs &a, const do
     int T = 1;
     const int tmax = KIND == PA_TRICUBIC ? 8 : 2;
     while (T < tmax && items * T * 2 <= ethreads) T *= 2;
-    if (T == 1) {
+    // When the items outnumber the threads but not twice over, a thread with
+    // a second item would evaluate four terms while most evaluate two; as
+    // (item, copy) units each thread evaluates at most ceil(2 items / threads)
+    // terms (the partner is then read once per copy).
+    const int per_item = 2 * ((items + ethreads - 1) / ethreads), per_unit = (2 * items + ethreads - 1) / ethreads;
+    if (T == 1 && per_unit < per_item) {
+      const int units = 2 * items;
+      for (int u0 = etid; u0 < units; u0 += 2 * ethreads) {
+        double a2[2][3], b2[2][3];
+        int r0s[2];
+        bool live[2], isn[2];
+#pragma unroll
+        for (int u = 0; u < 2; u++) {
+          const int uu = u0 + u * ethreads;
+          live[u] = uu < units;
+          const int iu = live[u] ? uu : u0;
+          isn[u] = iu >= items;  // units [0, items) are the OLD copies, [items, 2 items) the NEW
+          const int it = beg + (isn[u] ? iu - items : iu);
+          const int link = it / np;
+          const int j = it - link * np;
+          const int p2 = plist ? plist[j] : (j < ptcl ? j : j + 1);
+          r0s[u] = link * skip;
+          const double *pa_ = path + ((size_t)(slice1 + r0s[u]) * N + p2) * 3;
+          const double *pb_ = path + ((size_t)(slice1 + r0s[u] + skip) * N + p2) * 3;
+          for (int i = 0; i < 3; i++) {
+            a2[u][i] = __ldcg(pa_ + i);
+            b2[u][i] = __ldcg(pb_ + i);
+          }
+        }
+#pragma unroll
+        for (int u = 0; u < 2; u++) {
+          if (!live[u]) continue;
+          const int r0 = r0s[u];
+          const double(*w)[3] = isn[u] ? w_new : w_old;
+          double dA[3], dB[3];
+          dist_disp(w[r0], a2[u], w[r0 + skip], b2[u], sys, dA, dB);
+          add_terms(link_geom<double>(dA, dB), isn[u], 0, 1);
+        }
+      }
+    } else if (T == 1) {
       // Two items per pass so a thread's partner and table loads overlap.
       // Item it is (link, j) = (it / np, it % np); both pass items advance
       // by the same stride, so (link, j) is carried instead of divided.
@@ -282,7 +321,7 @@ __device__ __forceinline__ StageSums stage_sums(const BisectionArgs &a, const do
           live[u] = it < end;
           const int link = live[u] ? lk[u] : lk[0];
           const int j = live[u] ? jj[u] : jj[0];
-          const int p2 = plist ? __ldg(&plist[j]) : (j < ptcl ? j : j + 1);
+          const int p2 = plist ? plist[j] : (j < ptcl ? j : j + 1);
           r0s[u] = link * skip;
           const double *pa_ = path + ((size_t)(slice1 + r0s[u]) * N + p2) * 3;
           const double *pb_ = path + ((size_t)(slice1 + r0s[u] + skip) * N + p2) * 3;
@@ -320,7 +359,7 @@ __device__ __forceinline__ StageSums stage_sums(const BisectionArgs &a, const do
       for (int it = beg + team; it < end; it += nteams) {
         const int link = it / np;
         const int j = it - link * np;
-        const int p2 = plist ? __ldg(&plist[j]) : (j < ptcl ? j : j + 1);
+        const int p2 = plist ? plist[j] : (j < ptcl ? j : j + 1);
         const int r0 = link * skip;
         const double *pa_ = path + ((size_t)(slice1 + r0) * N + p2) * 3;
         const double *pb_ = path + ((size_t)(slice1 + r0 + skip) * N + p2) * 3;
@@ -475,6 +514,10 @@ __device__ __forceinline__ void rng_store(RngSnap &s, const DevRandom &r) {
 //    the move ends at this stage (a rejection, or acceptance at level 0),
 //    unless the accepted particle was drawn again, whose window changes.
 // The draw order is therefore exactly the reference's.
+// Neighbour-list entries of the moved particle staged in shared memory per
+// move (longer lists are read from global memory).
+constexpr int kNbrStage = 1024;
+
 // Values reduced over a cluster per stage: S_old, S_new, the mixed bound and
 // the two shadow sums.
 constexpr int kRed = 5;
@@ -592,7 +635,8 @@ struct Group {
 template <int KIND, typename R, bool SHADOW, bool OUTLINE, bool PROP = false>
 __device__ void run_job(const BisectionArgs &a, ChainState *cs, int window, unsigned rank, unsigned CL,
                         cg::cluster_group &cluster, const Group &G, unsigned char *dyn, unsigned dyn_cap,
-                        KernelShared &S, uint64_t *bar_ptr, unsigned &phase, const RngTab &tab_mem) {
+                        KernelShared &S, uint64_t *bar_ptr, unsigned &phase, const RngTab &tab_mem,
+                        int *s_nbr = nullptr) {
   typedef typename Pair2<R>::T P2;
   typedef typename std::conditional<std::is_same<R, double>::value, float, double>::type RS;  // shadow precision
   typedef typename Pair2<RS>::T P2S;
@@ -821,6 +865,19 @@ __device__ void run_job(const BisectionArgs &a, ChainState *cs, int window, unsi
       const bool next_new_block = !a.concurrent && ((m + 1) % a.steps_per_block == 0);
       double(*w_old)[3] = win_old[cur];
       double(*w_new)[3] = win_new[cur];
+      // Neighbour lists: the moved particle's list (fixed for the launch) in
+      // shared memory for the whole move, so a stage's item loop starts with
+      // the partner loads instead of two dependent reads of the list.
+      int mv_cnt = -1;
+      if (a.nbr_on && s_nbr) {
+        const int cnt = __ldcg(&a.nbr_cnt[ptcl]);
+        if (cnt >= 0 && cnt <= kNbrStage) {
+          const int *src = a.nbr_idx + (size_t)ptcl * a.nbr_kmax;
+          for (int i = tid; i < cnt; i += G.size) s_nbr[i] = __ldcg(src + i);
+          mv_cnt = cnt;
+        }
+        G.sync();
+      }
 
       // prevDS: the previous stage's dS as the decision used it; prevE: a
       // bound on its error against the FP64 sums (0 when it is FP64's)
@@ -850,10 +907,15 @@ __device__ void run_job(const BisectionArgs &a, ChainState *cs, int window, unsi
         int np = N - 1;
         const int *plist = nullptr;
         if (a.nbr_on && !far && !S.s_allpairs) {
-          const int cnt = __ldcg(&a.nbr_cnt[ptcl]);
-          if (cnt >= 0) {
-            np = cnt;
-            plist = a.nbr_idx + (size_t)ptcl * a.nbr_kmax;
+          if (mv_cnt >= 0) {
+            np = mv_cnt;
+            plist = s_nbr;
+          } else {
+            const int cnt = __ldcg(&a.nbr_cnt[ptcl]);
+            if (cnt >= 0) {
+              np = cnt;
+              plist = a.nbr_idx + (size_t)ptcl * a.nbr_kmax;
+            }
           }
         }
         if (evaluator) {
@@ -1264,6 +1326,7 @@ __global__ void __launch_bounds__(512, 1) bisection_kernel(BisectionArgs a) {
   __shared__ KernelShared S;
   __shared__ RngStore<2> store;
   __shared__ __align__(8) uint64_t s_bar;
+  __shared__ int s_nbr[kNbrStage];
   extern __shared__ __align__(16) unsigned char dyn[];
   cg::cluster_group cluster = cg::this_cluster();
   const unsigned rank = cluster.block_rank();
@@ -1281,7 +1344,8 @@ __global__ void __launch_bounds__(512, 1) bisection_kernel(BisectionArgs a) {
   unsigned dyn_size;
   asm("mov.u32 %0, %%dynamic_smem_size;" : "=r"(dyn_size));
   const RngTab tab = store.part<2>(0, 2);
-  run_job<KIND, R, SHADOW, false, PROP>(a, cs, window, rank, CL, cluster, G, dyn, dyn_size, S, &s_bar, phase, tab);
+  run_job<KIND, R, SHADOW, false, PROP>(a, cs, window, rank, CL, cluster, G, dyn, dyn_size, S, &s_bar, phase, tab,
+                                        s_nbr);
 }
 
 // Many independent chains in one persistent launch (the reference's clone
