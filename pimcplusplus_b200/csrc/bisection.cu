@@ -951,6 +951,8 @@ __device__ void run_job(const BisectionArgs &a, ChainState *cs, int window, unsi
             DevRandom spec = rng_from(s_rng, seed, stream, &S.tab);
             const int ns1 = next_new_block ? spec.LocalInt(numLeft) : slice1;
             const int np_ = spec.LocalInt(N);
+            // the bounding sphere's load goes out with the window's
+            const double4 cb = a.nbr_on ? a.nbr_cb[np_] : make_double4(0.0, 0.0, 0.0, 0.0);
             double(*wo)[3] = win_old[cur ^ 1];
             double(*wn)[3] = win_new[cur ^ 1];
             for (int rel = lane; rel <= span; rel += 32) {
@@ -961,9 +963,7 @@ __device__ void run_job(const BisectionArgs &a, ChainState *cs, int window, unsi
             const double lsr = sample_level<OUTLINE>(wo, wn, gbuf[1], L, L - 1, sys, spec, lane);
             const double lu = spec.LocalLog();
             int far = 0;
-            double4 cb = make_double4(0.0, 0.0, 0.0, 0.0);
             if (a.nbr_on) {
-              cb = a.nbr_cb[np_];
               __syncwarp();
               far = window_outside(wn, span, cb, sys, lane);
             }
