@@ -352,6 +352,9 @@ def rates(ms, st):
            "accepted_moves_per_s": st["accepted"] / s}
     if st.get("stages_attempted"):
         out["reevaluated_per_stage"] = st.get("reevaluated", 0) / st["stages_attempted"]
+    if "evals_per_launch" in st:
+        out["evals_per_launch"] = st["evals_per_launch"]
+        out["ms_per_launch"] = ms / st["launches"]
     return out
 
 
@@ -456,8 +459,12 @@ def run_ours(args):
         if dist:
             dist.barrier()
         d.close()
-        launches["n"] += steps * nb_launches(schedule or args.schedule, nb)
-        return agg(ms, st)
+        nl = steps * nb_launches(schedule or args.schedule, nb)
+        launches["n"] += nl
+        ms, st = agg(ms, st)
+        st["evals_per_launch"] = st["pair_evals"] / world / nl
+        st["launches"] = nl
+        return ms, st
 
     sampler = ClockSampler(local) if rank == 0 else None
     if sampler:
