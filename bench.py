@@ -394,6 +394,16 @@ class Timer:
         return float(np.sum(times)), {k: s1[k] - s0[k] for k in COUNTERS if k in s1}
 
 
+def moves_and_shift(d, bb, n_blocks):
+    """One step of a run: n_blocks BisectionBlocks on the device, then one
+    ShiftMove (MetaMoves.cc:39-65), which rotates the path by a random number
+    of slices so that the slices no window moves (slice 0 = M, and each
+    round's window ends) are moved in later steps, as a reference run
+    interleaves ShiftMove with its bisection blocks."""
+    bb.launch_async(n_blocks)
+    d.ShiftMove()
+
+
 def stage_errors(rec):
     """Per-stage |dS - dS_FP64| of shadow records: raw (the mixed sums), the
     bound, and as used by the decision (FP64's for re-evaluated stages)."""
@@ -455,12 +465,12 @@ def run_ours(args):
         nb = blocks_for(schedule or args.schedule)
         if dist:
             dist.barrier()
-        ms, st = timer(P.lib().pimc_stream(d.h), lambda: bb.launch_async(nb), steps, args.warmup, bb.stats)
+        ms, st = timer(P.lib().pimc_stream(d.h), lambda: moves_and_shift(d, bb, nb), steps, args.warmup, bb.stats)
         if dist:
             dist.barrier()
         d.close()
         nl = steps * nb_launches(schedule or args.schedule, nb)
-        launches["n"] += nl
+        launches["n"] += nl + steps  # + the ShiftMove kernel of each step
         ms, st = agg(ms, st)
         st["evals_per_launch"] = st["pair_evals"] / world / nl
         st["launches"] = nl
@@ -522,11 +532,12 @@ def run_ours(args):
         t0 = time.perf_counter()
         d.set_path(host)
         bb.MakeMoves(blocks, trace=False)
+        d.ShiftMove()
         host = d.get_path(P.OLDMODE)
         e2e_t += time.perf_counter() - t0
     e2e_evals = bb.stats()["pair_evals"] - s0["pair_evals"]
     d.close()
-    launches["n"] += args.steps * nb_launches(args.schedule, blocks)
+    launches["n"] += args.steps * (nb_launches(args.schedule, blocks) + 1)
     if dist:
         t = torch.tensor([e2e_t], dtype=torch.float64, device=f"cuda:{local}")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
@@ -670,9 +681,9 @@ def run_c1(args, P, timer, local, rank, agg, launches):
             bb.MakeMoves(20, trace=False)  # equilibrate
             per_round = spb * 4.1  # about 4 of the 5 window slots fit a round
             rounds = max(1, int(math.ceil(args.c1_sweeps * sweep / per_round)))
-            ms, st = timer(P.lib().pimc_stream(d.h), lambda: bb.launch_async(rounds), args.steps, 0, bb.stats)
+            ms, st = timer(P.lib().pimc_stream(d.h), lambda: moves_and_shift(d, bb, rounds), args.steps, 0, bb.stats)
             d.close()
-            launches["n"] += args.steps * rounds
+            launches["n"] += args.steps * (rounds + 1)
             ms, st = agg(ms, st)
             r = rates(ms, st)
             r["sweeps_per_s"] = st["moves"] / sweep / (ms / 1000.0)
@@ -794,14 +805,14 @@ def run_c4(args, P, timer, local, rank, agg, launches):
 
     def timed(precision):
         d, bb, nk = make(precision)
-        ms, st = timer(P.lib().pimc_stream(d.h), lambda: bb.launch_async(rounds), args.steps, args.warmup,
+        ms, st = timer(P.lib().pimc_stream(d.h), lambda: moves_and_shift(d, bb, rounds), args.steps, args.warmup,
                        bb.stats)
         # share of moves that reach the lowest stage (its rho_k update covers 2^L + 1 slices)
         rec, _ = bb.MakeMoves(rounds, trace=True)
         live = rec["slice1"] >= 0
         frac0 = float(np.mean(rec["stages_passed"][live] >= L - 1)) if live.any() else 0.0
         d.close()
-        launches["n"] += args.steps * rounds
+        launches["n"] += args.steps * (rounds + 2)  # + ShiftMove and the rho_k recompute it calls for
         ms, st = agg(ms, st)
         return ms, st, frac0, nk
 
@@ -872,11 +883,12 @@ def run_c5(args, P, timer, local, rank, agg, launches):
 
     def timed(precision, skin, proposals=0):
         d, bb = make(precision, skin, eq, proposals)
-        ms, st = timer(P.lib().pimc_stream(d.h), lambda: bb.launch_async(rounds), args.steps, args.warmup,
+        ms, st = timer(P.lib().pimc_stream(d.h), lambda: moves_and_shift(d, bb, rounds), args.steps, args.warmup,
                        bb.stats)
         d.close()
-        # per round: the bisection launch, plus the neighbour-list kernels (bounds, fill, clear) with lists
-        launches["n"] += args.steps * rounds * (4 if skin > 0 else 1)
+        # per round: the bisection launch, plus the neighbour-list kernels (bounds, fill, clear) with
+        # lists; per step the ShiftMove kernel
+        launches["n"] += args.steps * (rounds * (4 if skin > 0 else 1) + 1)
         ms, st = agg(ms, st)
         out = rates(ms, st)
         out["pair_evals_per_move"] = st["pair_evals"] / st["moves"]

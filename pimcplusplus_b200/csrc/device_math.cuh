@@ -320,10 +320,7 @@ __device__ __forceinline__ R pot_V(const DTricubic<R> &t, R r) {
 // ---- PAtricubicFitClass::U / dU (PAtricubicFit.cc:659-721) ----
 // Inside the fitted region (q <= qmax, z < 2q, s < 2q) the tricubic spline at
 // (q, z/2q, (s-z)/(2q-z)) (at (0,0,0) when q == 0); outside it the primitive
-// action 1/2 beta_l (V(r) + V(r')) (dU: 1/2 (V(r) + V(r'))).  Both candidates
-// are evaluated unconditionally and one is selected, so a warp never splits
-// between the two branches and every table load of the item issues in one
-// phase; out-of-region lanes read the (0,0,0) cell, which coalesces.
+// action 1/2 beta_l (V(r) + V(r')) (dU: 1/2 (V(r) + V(r'))).
 template <typename R, bool DERIV>
 __device__ __forceinline__ R tricubic_pa(const DTricubic<R> &t, R q, R z, R s2, int level, int part = 0,
                                          int nparts = 1) {
@@ -339,7 +336,6 @@ __device__ __forceinline__ R tricubic_pa(const DTricubic<R> &t, R q, R z, R s2, 
   const R xt = nonzero ? (s - z) / (smax - z) : R(0);
   const R *F = (DERIV ? t.dU : t.U) + (size_t)level * t.nq * t.ny * t.nt * 8;
   const int k0 = (4 * part) / nparts, k1 = (4 * (part + 1)) / nparts;
-  const R tri = tricubic_eval(F, qg, yg, tg, xq, xy, xt, k0, k1);
   const R r = q + R(0.5) * z;
   const R rp = q - R(0.5) * z;
   R beta = R(0.5);
@@ -348,12 +344,17 @@ __device__ __forceinline__ R tricubic_pa(const DTricubic<R> &t, R q, R z, R s2, 
     for (int i = 0; i < level; i++) beta *= R(2.0);
     beta = R(0.5) * beta;
   }
-  R prim;
   if (nparts == 1) {
-    prim = beta * (pot_V(t, r) + pot_V(t, rp));
-  } else {  // part 0 takes V(r), part 1 takes V(r'), any other part nothing
-    prim = part < 2 ? beta * pot_V(t, part == 0 ? r : rp) : R(0);
+    // One lane, one term: a lane inside the fit gathers its cell, a lane
+    // outside reads the two potential splines; in a warp with both, each
+    // side's loads issue for its own lanes only.
+    if (inside) return tricubic_eval(F, qg, yg, tg, xq, xy, xt, k0, k1);
+    return beta * (pot_V(t, r) + pot_V(t, rp));
   }
+  // A team's parts: every lane takes both candidates and selects, so the
+  // parts of one term stay in step.  Part 0 takes V(r), part 1 V(r').
+  const R tri = tricubic_eval(F, qg, yg, tg, xq, xy, xt, k0, k1);
+  const R prim = part < 2 ? beta * pot_V(t, part == 0 ? r : rp) : R(0);
   return inside ? tri : prim;
 }
 
@@ -670,20 +671,28 @@ __device__ __forceinline__ MixedU tricubic_pa_mixed(const DTricubic<double> &t64
   const double xt = nonzero ? (s - z) / (smax - z) : 0.0;
   const size_t lvl = (size_t)level * t32.nq * t32.ny * t32.nt;
   const int k0 = (4 * part) / nparts, k1 = (4 * (part + 1)) / nparts;
-  int cell;
-  const float tri = tricubic_eval_mixed(t32.U + lvl * 8, t64.qg, t64.yg, t64.tg, xq, xy, xt, t32.ny, t32.nt, cell,
-                                        k0, k1);
-  const float trim = part == 0 ? __ldg(&t32.mbound[lvl + cell]) : 0.0f;
   const double r = q + 0.5 * z, rp = q - 0.5 * z;
   double beta = t64.smallest_beta;
   for (int i = 0; i < level; i++) beta *= 2.0;
   const float hb = (float)(0.5 * beta);
   MixedU prim;
-  if (nparts == 1) {
+  if (nparts == 1) {  // one lane, one term: only the side the lane needs (as tricubic_pa)
+    if (inside) {
+      int cell;
+      const float tri = tricubic_eval_mixed(t32.U + lvl * 8, t64.qg, t64.yg, t64.tg, xq, xy, xt, t32.ny, t32.nt,
+                                            cell, k0, k1);
+      return MixedU{(double)tri, __ldg(&t32.mbound[lvl + cell])};
+    }
     const MixedU va = pot_V_mixed(t64, t32, r), vb = pot_V_mixed(t64, t32, rp);
     prim.v = (double)(hb * ((float)va.v + (float)vb.v));
     prim.m = hb * (va.m + vb.m);
-  } else if (part < 2) {
+    return prim;
+  }
+  int cell;
+  const float tri = tricubic_eval_mixed(t32.U + lvl * 8, t64.qg, t64.yg, t64.tg, xq, xy, xt, t32.ny, t32.nt, cell,
+                                        k0, k1);
+  const float trim = part == 0 ? __ldg(&t32.mbound[lvl + cell]) : 0.0f;
+  if (part < 2) {
     const MixedU va = pot_V_mixed(t64, t32, part == 0 ? r : rp);
     prim.v = (double)(hb * (float)va.v);
     prim.m = hb * va.m;
