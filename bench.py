@@ -943,7 +943,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--moves", type=int, default=2048)
     ap.add_argument("--schedule", default="windows", choices=["windows", "sequential"])
-    ap.add_argument("--steps-per-block", type=int, default=64)
+    ap.add_argument("--steps-per-block", type=int, default=128)
     ap.add_argument("--cluster", type=int, default=16)
     ap.add_argument("--threads", type=int, default=512)
     ap.add_argument("--accuracy-moves", type=int, default=1000)
