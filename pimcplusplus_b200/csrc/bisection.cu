@@ -521,9 +521,6 @@ constexpr int kNbrStage = 1024;
 // Values reduced over a cluster per stage: S_old, S_new, the mixed bound and
 // the two shadow sums.
 constexpr int kRed = 5;
-// The stage reductions add at most 16 rows (warps of a 512-thread CTA, CTAs
-// of a cluster) in one 16-lane shuffle tree.
-static_assert(kMaxCluster <= 16, "cluster sums use a 16-lane tree");
 
 // Shared state of one CTA while it runs a job.
 struct KernelShared {
@@ -1000,46 +997,24 @@ __device__ void run_job(const BisectionArgs &a, ChainState *cs, int window, unsi
         // ---- reduce: warps -> CTA (warp 0) -> cluster (DSMEM, rank order) ----
         // The sums are bitwise the same in every CTA of the cluster, so every
         // CTA takes the same decision (and the same re-evaluation request).
-        // Both sums are a fixed 16-lane shuffle tree in warp 0 (lanes 0-15
-        // add values 0-2, lanes 16-31 values 3-4, lane l taking row l & 15),
-        // the same bits in every CTA; lane k < kRed returns value k.
-        auto tree16 = [&](const double (*rows)[kRed], int nrows) -> double {
-          const int row = lane & 15, g = lane >> 4;
-          double v0 = 0.0, v1 = 0.0, v2 = 0.0;
-          if (row < nrows) {
-            v0 = rows[row][3 * g];
-            v1 = rows[row][3 * g + 1];
-            v2 = g == 0 ? rows[row][2] : 0.0;
-          }
-#pragma unroll
-          for (int o = 8; o > 0; o >>= 1) {
-            v0 += __shfl_xor_sync(0xffffffffu, v0, o);
-            v1 += __shfl_xor_sync(0xffffffffu, v1, o);
-            v2 += __shfl_xor_sync(0xffffffffu, v2, o);
-          }
-          const double s0 = __shfl_sync(0xffffffffu, v0, 0), s1 = __shfl_sync(0xffffffffu, v1, 0);
-          const double s2 = __shfl_sync(0xffffffffu, v2, 0), s3 = __shfl_sync(0xffffffffu, v0, 16);
-          const double s4 = __shfl_sync(0xffffffffu, v1, 16);
-          return lane == 0 ? s0 : lane == 1 ? s1 : lane == 2 ? s2 : lane == 3 ? s3 : lane == 4 ? s4 : 0.0;
-        };
         auto reduce = [&]() -> double {
           const int par = xc & 1;
           xc++;
-          if (warp == 0) {
-            const double v = tree16(sh_red, nwarps);
-            if (lane < kRed) {
-              if (ECL > 1)
-                for (unsigned r = 0; r < CL; r++) cluster.map_shared_rank(&xchg[par][rank][0], r)[lane] = v;
-              else
-                xchg[par][0][lane] = v;
-            }
+          if (warp == 0 && lane < kRed) {
+            double v = 0.0;
+            for (int w = 0; w < nwarps; w++) v += sh_red[w][lane];
+            if (ECL > 1)
+              for (unsigned r = 0; r < CL; r++) cluster.map_shared_rank(&xchg[par][rank][0], r)[lane] = v;
+            else
+              xchg[par][0][lane] = v;
           }
           if (ECL > 1)
             cluster.sync();
           else
             __syncwarp();
           double v = 0.0;
-          if (warp == 0) v = ECL > 1 ? tree16(xchg[par], (int)ECL) : (lane < kRed ? xchg[par][0][lane] : 0.0);
+          if (warp == 0 && lane < kRed)
+            for (unsigned r = 0; r < ECL; r++) v += xchg[par][r][lane];
           return v;
         };
         // ---- Metropolis test, identical in every CTA (warp 0) ----
