@@ -210,6 +210,140 @@ __device__ __forceinline__ double2 rho_new_k(double2 ro, const double *kv, const
 struct StageSums {
   double so, sn, eb, so2, sn2;
 };
+
+// One in-fit tricubic term of a pass, listed per warp for its team.
+template <typename R>
+struct TriTerm;
+template <>
+struct TriTerm<double> {
+  double u[3];
+  int code;  // cell << 1 | copy (1: NEW)
+  int pad;
+};
+template <>
+struct TriTerm<float> {
+  float u[3];
+  int code;
+};
+// Terms listed per warp and pass (two (item, copy) units per lane).
+constexpr int kTriTermsPerWarp = 64;
+// Shared memory of the lists: 16 warps of TriTerm<double>, enough for either precision.
+constexpr unsigned kTriTermBytes = 16u * kTriTermsPerWarp * sizeof(TriTerm<double>);
+
+// The tricubic short-range sum of one stage over this CTA's items
+// [beg, beg + items) (item = link * np + partner index), each item evaluated
+// for the OLD and the NEW copy of the moved particle: 2 items (item, copy)
+// units.  Per pass every evaluating warp takes an even share of at most 64
+// consecutive units, two per lane.  A lane forms its units' geometry
+// (DistDisp, q, z, s, the fit-region test, the cell) and adds the primitive
+// fallback of the terms outside the fit itself, from the potential's (y, d2y)
+// pairs in shared memory (pp; null: the global tables).  The terms inside the
+// fit are listed in shared memory (tq: kTriTermsPerWarp per warp) and
+// gathered by teams of TS lanes (tricubic_team_part): TS = 4 FP64, 2 FP32.
+// Sums as stage_sums: (so, sn) the run's precision (mixed: two-sum with
+// (co, cn) and the magnitudes in mb), (so2, sn2) the other precision's terms
+// with SHADOW.
+template <typename R, bool SHADOW>
+__device__ __forceinline__ void tricubic_stage(const BisectionArgs &a, const double (*w_old)[3],
+                                               const double (*w_new)[3], const typename Pair2<R>::T *pp, int lv,
+                                               int slice1, int ptcl, int beg, int items, int etid, int ethreads,
+                                               const int *plist, int np, TriTerm<R> *tq, double &so, double &sn,
+                                               float &co, float &cn, float &mb, double &so2, double &sn2) {
+  constexpr bool MIX = std::is_same<R, float>::value;
+  constexpr int TS = MIX ? 2 : 4, TPW = 32 / TS;
+  const DevSystem &sys = a.sys;
+  const DTricubic<double> &t64 = a.pa.t64;
+  const int N = sys.N;
+  const int skip = 1 << lv;
+  const int lane = etid & 31, wi = etid >> 5, nw = ethreads >> 5;
+  const int pt = lane & (TS - 1);
+  TriTerm<R> *E = tq + wi * kTriTermsPerWarp;
+  const size_t lvl = (size_t)lv * t64.nq * t64.ny * t64.nt;
+  const R *F = tricubic_of<R>(a.pa).U + lvl * 8;
+  double beta = t64.smallest_beta;
+  for (int i = 0; i < lv; i++) beta *= 2.0;
+  beta = 0.5 * beta;
+  const float hb = (float)beta;
+  const int U = 2 * items;
+  const int P = (U + 2 * ethreads - 1) / (2 * ethreads);
+  const int cw = P > 0 ? (U + P * nw - 1) / (P * nw) : 0;  // <= 64
+  for (int p = 0; p < P; p++) {
+    const int ws = (p * nw + wi) * cw, we = min(U, ws + cw);
+    bool in[2];
+    TriTerm<R> tt[2];
+#pragma unroll
+    for (int s = 0; s < 2; s++) {
+      const int u = ws + lane + 32 * s;
+      in[s] = false;
+      if (u < we) {
+        const int it = beg + (u >> 1);
+        const int isn = u & 1;
+        const int link = it / np;
+        const int j = it - link * np;
+        const int p2 = plist ? plist[j] : (j < ptcl ? j : j + 1);
+        const int r0 = link * skip;
+        const double *pa_ = a.path + ((size_t)(slice1 + r0) * N + p2) * 3;
+        const double *pb_ = a.path + ((size_t)(slice1 + r0 + skip) * N + p2) * 3;
+        // L2-coherent loads: other CTAs write accepted windows during the launch.
+        const double a2[3] = {__ldcg(pa_), __ldcg(pa_ + 1), __ldcg(pa_ + 2)};
+        const double b2[3] = {__ldcg(pb_), __ldcg(pb_ + 1), __ldcg(pb_ + 2)};
+        const double(*w)[3] = isn ? w_new : w_old;
+        double dA[3], dB[3];
+        dist_disp(w[r0], a2, w[r0 + skip], b2, sys, dA, dB);
+        const LinkGeom<double> g = link_geom<double>(dA, dB);
+        const TriPrep<R> pr = tricubic_prep<R>(t64, g.q, g.z, g.s2);
+        if (pr.inside) {
+          in[s] = true;
+          tt[s].u[0] = pr.u[0];
+          tt[s].u[1] = pr.u[1];
+          tt[s].u[2] = pr.u[2];
+          tt[s].code = (pr.cell << 1) | isn;
+        } else if (MIX) {  // the primitive action 1/2 beta_l (V(r) + V(r'))
+          MixedU va, vb;
+          if (pp) {
+            va = pot_V_pairs_mixed(t64.pot_grid, reinterpret_cast<const float2 *>(pp), pr.r);
+            vb = pot_V_pairs_mixed(t64.pot_grid, reinterpret_cast<const float2 *>(pp), pr.rp);
+          } else {
+            va = pot_V_mixed(t64, a.pa.t32, pr.r);
+            vb = pot_V_mixed(t64, a.pa.t32, pr.rp);
+          }
+          two_sum_add(isn ? sn : so, isn ? cn : co, (double)(hb * ((float)va.v + (float)vb.v)));
+          mb += hb * (va.m + vb.m);
+        } else {
+          const double v = pp ? pot_V_pairs(t64.pot_grid, reinterpret_cast<const double2 *>(pp), pr.r) +
+                                    pot_V_pairs(t64.pot_grid, reinterpret_cast<const double2 *>(pp), pr.rp)
+                              : pot_V(t64, pr.r) + pot_V(t64, pr.rp);
+          (isn ? sn : so) += beta * v;
+        }
+        if (SHADOW) {
+          if (MIX)
+            (isn ? sn2 : so2) += tricubic_pa<double, false>(t64, g.q, g.z, g.s2, lv);
+          else
+            (isn ? sn2 : so2) += tricubic_pa_mixed(t64, a.pa.t32, g.q, g.z, g.s2, lv).v;
+        }
+      }
+    }
+    // list the in-fit terms, then each team gathers every TPW-th of them
+    const unsigned m0 = __ballot_sync(0xffffffffu, in[0]), m1 = __ballot_sync(0xffffffffu, in[1]);
+    const unsigned below = (1u << lane) - 1u;
+    const int n0 = __popc(m0), n = n0 + __popc(m1);
+    if (in[0]) E[__popc(m0 & below)] = tt[0];
+    if (in[1]) E[n0 + __popc(m1 & below)] = tt[1];
+    __syncwarp();
+    for (int e = lane / TS; e < n; e += TPW) {
+      const TriTerm<R> T = E[e];
+      const int cell = T.code >> 1;
+      const R v = tricubic_team_part(F, t64, cell, T.u, pt);
+      if (MIX) {
+        two_sum_add((T.code & 1) ? sn : so, (T.code & 1) ? cn : co, (double)v);
+        if (pt == 0) mb += __ldg(&a.pa.t32.mbound[lvl + cell]);
+      } else {
+        ((T.code & 1) ? sn : so) += (double)v;
+      }
+    }
+    __syncwarp();
+  }
+}
 // Bound on the error of one FP32 e^{ik.r}: the FP64 phase reduced to
 // [-pi, pi] and rounded to FP32 (<= 2^-22) and sincosf (2 ulp), doubled.
 constexpr double kCisErr = 2.0e-6;
@@ -218,7 +352,7 @@ template <int KIND, typename R, bool SHADOW>
 __device__ __forceinline__ StageSums stage_sums(const BisectionArgs &a, const double (*w_old)[3],
                                                 const double (*w_new)[3], const void *dg, const void *dgs, int lv,
                                                 int slice1, int ptcl, unsigned rank, unsigned CL, int etid,
-                                                int ethreads, const int *plist, int np) {
+                                                int ethreads, const int *plist, int np, void *tq) {
   constexpr bool MIX = std::is_same<R, float>::value;
   const DevSystem &sys = a.sys;
   const int N = sys.N;
@@ -243,7 +377,17 @@ __device__ __forceinline__ StageSums stage_sums(const BisectionArgs &a, const do
       if (SHADOW) (is_new ? sn2 : so2) += pa_U_mixed<KIND>(a.pa, dg32, g, lv, part, nparts).v;
     }
   };
-  if (lv == 0 || a.sr_higher) {  // ShortRangeClass::SingleAction over partners x links
+  if (KIND == PA_TRICUBIC && (lv == 0 || a.sr_higher)) {
+    // ShortRangeClass::SingleAction over partners x links with PAtricubicFit
+    // terms, by lane teams (tricubic_stage).
+    const int total = np * nlinks;
+    const int chunk = (total + (int)CL - 1) / (int)CL;
+    const int beg = chunk * (int)rank;
+    const int end = min(total, beg + chunk);
+    tricubic_stage<R, SHADOW>(a, w_old, w_new, reinterpret_cast<const typename Pair2<R>::T *>(dg), lv, slice1, ptcl,
+                              beg, max(0, end - beg), etid, ethreads, plist, np,
+                              reinterpret_cast<TriTerm<R> *>(tq), so, sn, co, cn, mb, so2, sn2);
+  } else if (lv == 0 || a.sr_higher) {  // ShortRangeClass::SingleAction over partners x links
     // partners: all others (plist null, np = N - 1) or the moved particle's
     // neighbour list (np entries, ascending)
     const int total = np * nlinks;  // < 2^31: N <= 2^20, 2^L <= 64 (host-checked)
@@ -453,7 +597,7 @@ __device__ __forceinline__ double4 stage_sums_reeval(const BisectionArgs &a, con
                                                      const double (*w_new)[3], int lv, int slice1, int ptcl,
                                                      unsigned rank, unsigned CL, int etid, int ethreads,
                                                      const int *plist, int np, int need_prev,
-                                                     const int *prev_plist, int prev_np) {
+                                                     const int *prev_plist, int prev_np, void *tq) {
   const DDavid<double> &d64 = a.pa.d64;
   auto dgl = [&](int l) -> const void * {
     return KIND == PA_DAVID ? reinterpret_cast<const double2 *>(d64.diag) + (size_t)(d64.tau_pos + l) * d64.diag_stride
@@ -463,7 +607,7 @@ __device__ __forceinline__ double4 stage_sums_reeval(const BisectionArgs &a, con
   for (int k = 0; k < 1 + need_prev; k++) {  // one loop body: the FP64 evaluation is inlined once
     const int l = lv + k;
     const StageSums v = stage_sums<KIND, double, false>(a, w_old, w_new, dgl(l), nullptr, l, slice1, ptcl, rank, CL,
-                                                        etid, ethreads, k ? prev_plist : plist, k ? prev_np : np);
+                                                        etid, ethreads, k ? prev_plist : plist, k ? prev_np : np, tq);
     if (k) {
       r.z = v.so;
       r.w = v.sn;
@@ -674,31 +818,51 @@ __device__ void run_job(const BisectionArgs &a, ChainState *cs, int window, unsi
   const int span = 1 << L;
   const bool lead = (erank == 0 && tid == 0);
 
-  // ---- stage the diagonal DavidPA columns into shared memory (bulk TMA) ----
-  // Each level's column is diag_stride pairs long, padded so every level and
-  // every copy is a multiple of 16 bytes.  The wait is bounded; the cluster
-  // then agrees on the outcome so every CTA takes the same path.
+  // ---- stage 1-D tables into shared memory (bulk TMA) ----
+  // DavidPA: the diagonal columns of every level, each diag_stride pairs
+  // long, padded so every level and every copy is a multiple of 16 bytes.
+  // Tricubic: the potential's (y, d2y) pairs of the primitive fallback when
+  // they fit beside the per-warp term lists (kTriTermBytes, after the tables).
+  // The wait is bounded; the cluster then agrees on the outcome so every CTA
+  // takes the same path.
   const P2 *diag_smem = nullptr;
   const P2S *diag_smem_s = nullptr;
+  const void *stage_src = nullptr, *stage_src_s = nullptr;
+  unsigned bytes = 0, bytes_s = 0, tail = 0;
   if (KIND == PA_DAVID) {
     const DDavid<R> &d = david_of<R>(a.pa);
-    const unsigned bytes = (unsigned)(L * d.diag_stride * sizeof(P2));
-    unsigned bytes_s = 0;
-    if (SHADOW) bytes_s = (unsigned)(L * david_of<RS>(a.pa).diag_stride * sizeof(P2S));
-    if (bytes + bytes_s > dyn_cap) {  // uniform over the cluster: same job, same launch
-      if (lead) atomicExch(&cs->status, PIMC_E_CAP);
-      return;
+    bytes = (unsigned)(L * d.diag_stride * sizeof(P2));
+    stage_src = reinterpret_cast<const P2 *>(d.diag) + (size_t)d.tau_pos * d.diag_stride;
+    if (SHADOW) {
+      const DDavid<RS> &ds = david_of<RS>(a.pa);
+      bytes_s = (unsigned)(L * ds.diag_stride * sizeof(P2S));
+      stage_src_s = reinterpret_cast<const P2S *>(ds.diag) + (size_t)ds.tau_pos * ds.diag_stride;
     }
+  } else if (KIND == PA_TRICUBIC) {
+    tail = kTriTermBytes;
+    const DTricubic<R> &t = tricubic_of<R>(a.pa);
+    const unsigned b0 = (unsigned)(t.pot_pairs_n * sizeof(P2));
+    const unsigned b1 = SHADOW ? (unsigned)(tricubic_of<RS>(a.pa).pot_pairs_n * sizeof(P2S)) : 0u;
+    if (b0 + b1 + tail <= dyn_cap) {
+      bytes = b0;
+      bytes_s = b1;
+      stage_src = t.pot_pairs;
+      if (SHADOW) stage_src_s = tricubic_of<RS>(a.pa).pot_pairs;
+    }
+  }
+  void *tq = dyn + ((bytes + bytes_s + 15u) & ~15u);
+  if (bytes + bytes_s + tail > dyn_cap) {  // uniform over the cluster: same job, same launch
+    if (lead) atomicExch(&cs->status, PIMC_E_CAP);
+    return;
+  }
+  const bool staged = bytes > 0;
+  if (staged) {
     G.sync();  // the previous job's readers of the staged tables are done
     if (tid == 0) {
       asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
       mbar_expect_tx(&s_bar, bytes + bytes_s);
-      bulk_g2s(dyn, reinterpret_cast<const P2 *>(d.diag) + (size_t)d.tau_pos * d.diag_stride, bytes, &s_bar);
-      if (SHADOW) {
-        const DDavid<RS> &ds = david_of<RS>(a.pa);
-        bulk_g2s(dyn + bytes, reinterpret_cast<const P2S *>(ds.diag) + (size_t)ds.tau_pos * ds.diag_stride, bytes_s,
-                 &s_bar);
-      }
+      bulk_g2s(dyn, stage_src, bytes, &s_bar);
+      if (SHADOW && bytes_s) bulk_g2s(dyn + bytes, stage_src_s, bytes_s, &s_bar);
     }
     G.sync();
     // Bounded wait for the copy; with test_wait, a further bounded wait on a
@@ -742,7 +906,7 @@ __device__ void run_job(const BisectionArgs &a, ChainState *cs, int window, unsi
     }
     phase ^= 1u;
     diag_smem = reinterpret_cast<const P2 *>(dyn);
-    if (SHADOW) diag_smem_s = reinterpret_cast<const P2S *>(dyn + bytes);
+    if (SHADOW && bytes_s) diag_smem_s = reinterpret_cast<const P2S *>(dyn + bytes);
   }
 
   const uint64_t seed = cs->seed;
@@ -778,11 +942,11 @@ __device__ void run_job(const BisectionArgs &a, ChainState *cs, int window, unsi
           const long long at = (long long)window * a.steps_per_block + st;
           a.trace[a.trace_offset + (prop ? at * a.proposals + rank : at)] = r;
         }
-      if (KIND == PA_DAVID && CL > 1) cluster.sync();  // xchg[1] no longer read by peers
+      if (staged && CL > 1) cluster.sync();  // xchg[1] no longer read by peers
       return;
     }
   }
-  if (KIND == PA_DAVID && CL > 1) cluster.sync();  // every CTA has read xchg[1]
+  if (staged && CL > 1) cluster.sync();  // every CTA has read xchg[1]
   G.sync();
   auto gsync = [&]() { G.sync(); };
   rng_tab_fill(S.tab, tab_mem.W, seed, stream, s_rng.n, tid, G.size, gsync);
@@ -923,7 +1087,7 @@ __device__ void run_job(const BisectionArgs &a, ChainState *cs, int window, unsi
           const size_t sts = (KIND == PA_DAVID && SHADOW) ? (size_t)david_of<RS>(a.pa).diag_stride : 0;
           const StageSums v = stage_sums<KIND, R, SHADOW>(a, w_old, w_new, diag_smem ? diag_smem + level * st : nullptr,
                                                           diag_smem_s ? diag_smem_s + level * sts : nullptr, level,
-                                                          slice1, ptcl, erank, ECL, tid, ethreads, plist, np);
+                                                          slice1, ptcl, erank, ECL, tid, ethreads, plist, np, tq);
           const double r0 = warp_sum(v.so), r1 = warp_sum(v.sn), r2 = warp_sum(v.eb);
           const double r3 = SHADOW ? warp_sum(v.so2) : 0.0, r4 = SHADOW ? warp_sum(v.sn2) : 0.0;
           if (lane == 0) {
@@ -1110,7 +1274,7 @@ __device__ void run_job(const BisectionArgs &a, ChainState *cs, int window, unsi
           const int need_prev = S.s_need[1];
           if (evaluator) {
             const double4 v = stage_sums_reeval<KIND>(a, w_old, w_new, level, slice1, ptcl, erank, ECL, tid, ethreads,
-                                                      plist, np, need_prev, prev_plist, prev_np);
+                                                      plist, np, need_prev, prev_plist, prev_np, tq);
             const double r0 = warp_sum(v.x), r1 = warp_sum(v.y), r2 = warp_sum(v.z), r3 = warp_sum(v.w);
             if (lane == 0) {
               sh_red[warp][0] = r0;
@@ -1545,6 +1709,16 @@ cudaError_t batch_occupancy(int precision, int shadow, int threads, size_t dyn, 
 }
 
 size_t bisection_dyn_smem(const BisectionArgs &a, int precision, int shadow) {
+  if (a.pa.kind == PA_TRICUBIC) {
+    // the potential's pairs (and the other precision's with shadow) when they
+    // fit in 160 KB with the term lists; the term lists alone otherwise
+    const size_t p64 = (size_t)a.pa.t64.pot_pairs_n * sizeof(double2);
+    const size_t p32 = (size_t)a.pa.t32.pot_pairs_n * sizeof(float2);
+    size_t pot = precision == PIMC_MIXED ? p32 : p64;
+    if (shadow) pot += precision == PIMC_MIXED ? p64 : p32;
+    pot = (pot + 15) & ~(size_t)15;
+    return pot + kTriTermBytes <= (size_t)160 * 1024 ? pot + kTriTermBytes : (size_t)kTriTermBytes;
+  }
   if (a.pa.kind != PA_DAVID) return 0;
   const size_t b64 = (size_t)a.num_levels * a.pa.d64.diag_stride * sizeof(double2);
   const size_t b32 = (size_t)a.num_levels * a.pa.d32.diag_stride * sizeof(float2);
