@@ -9,10 +9,12 @@
 //    (CL = 1..16).  The sampler warp (the last warp) of every CTA replays the
 //    same Philox stream (slice, particle, Gaussians, acceptance), so sampled
 //    positions and decisions are identical in every CTA without
-//    communication.  Only the stage action sums cross CTAs: warp 0 writes
-//    this CTA's partials into every peer's shared memory (DSMEM) and after
-//    one cluster barrier every CTA adds the partials in rank order — the same
-//    bits everywhere.
+//    communication.  Only the stage action sums cross CTAs: warp 0 stores
+//    this CTA's partials into every peer's shared memory (st.async, each
+//    store completing bytes on the peer's mbarrier); once its mbarrier has
+//    all CTAs' bytes, warp 0 of every CTA adds the partials in rank order —
+//    the same bits everywhere — while the other warps wait at the CTA
+//    barrier only, not at a cluster barrier.
 //  * Gaussians come from a warp-parallel polar method that reproduces the
 //    sequential draw order exactly (warp_gaussians); the per-midpoint work
 //    of a level runs one midpoint per lane.
@@ -71,6 +73,32 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, unsigned phase) {
       : "r"(smem_addr(bar)), "r"(phase)
       : "memory");
   return ok != 0;
+}
+// The same wait with acquire at cluster scope: the phase's bytes were stored
+// by other CTAs of the cluster (st.async).
+__device__ __forceinline__ bool mbar_try_wait_cluster(uint64_t *bar, unsigned phase) {
+  unsigned ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.acquire.cluster.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(smem_addr(bar)), "r"(phase)
+      : "memory");
+  return ok != 0;
+}
+// Address of the same shared-memory variable in CTA `rank` of the cluster.
+__device__ __forceinline__ unsigned mapa_u32(unsigned addr, unsigned rank) {
+  unsigned d;
+  asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(d) : "r"(addr), "r"(rank));
+  return d;
+}
+// Store of one double into a cluster CTA's shared memory that completes 8
+// transaction bytes on that CTA's mbarrier `bar`.
+__device__ __forceinline__ void st_async_f64(unsigned addr, double v, unsigned bar) {
+  asm volatile("st.async.shared::cluster.mbarrier::complete_tx::bytes.f64 [%0], %1, [%2];" ::"r"(addr), "d"(v),
+               "r"(bar)
+               : "memory");
 }
 // Bulk (non-tensor) TMA copy global -> this CTA's shared memory.  No multicast.
 __device__ __forceinline__ void bulk_g2s(void *dst, const void *src, unsigned bytes, uint64_t *bar) {
@@ -377,9 +405,12 @@ __device__ __forceinline__ StageSums stage_sums(const BisectionArgs &a, const do
       if (SHADOW) (is_new ? sn2 : so2) += pa_U_mixed<KIND>(a.pa, dg32, g, lv, part, nparts).v;
     }
   };
-  if (KIND == PA_TRICUBIC && (lv == 0 || a.sr_higher)) {
+  if (KIND == PA_TRICUBIC && !MIX && (lv == 0 || a.sr_higher)) {
     // ShortRangeClass::SingleAction over partners x links with PAtricubicFit
-    // terms, by lane teams (tricubic_stage).
+    // terms, by lane teams (tricubic_stage).  The FP64 path only: with FP32
+    // nodes (32 bytes) a lane's own 8-node gather is faster on the B200 than
+    // a 2-lane team's (4.13e9 vs 3.91e9 C2 evals/s), so the mixed path keeps
+    // one lane per term.
     const int total = np * nlinks;
     const int chunk = (total + (int)CL - 1) / (int)CL;
     const int beg = chunk * (int)rank;
@@ -693,7 +724,12 @@ struct KernelShared {
   int s_commit[4];  // first slot to redo, stop, any committed move left its sphere
   int s_need[2];    // mixed path: re-evaluate this stage in FP64; also the previous stage
   uint64_t test_bar;  // an mbarrier nothing arrives at (the give-up test of the staging wait)
+  // Stage reduction across the cluster: per parity an mbarrier that completes
+  // when every CTA's partials have landed in xchg[parity] (st.async).
+  uint64_t red_bar[2];
 };
+// Tries of the wait for a stage reduction's partials before PIMC_E_CAP.
+constexpr int kRedWaitCap = 1 << 24;
 
 // Whether any of the window's span+1 NEW positions lies outside the moved
 // particle's bounding sphere cb (minimum image), by one warp.
@@ -947,6 +983,18 @@ __device__ void run_job(const BisectionArgs &a, ChainState *cs, int window, unsi
     }
   }
   if (staged && CL > 1) cluster.sync();  // every CTA has read xchg[1]
+  // Stage reductions over a cluster: each CTA's red_bar[p] expects the
+  // partials of every CTA (kRed doubles each) for its next use; the first
+  // uses are posted before the cluster barrier, so before any peer can send.
+  const unsigned red_bytes = CL * kRed * (unsigned)sizeof(double);
+  unsigned rph = 0;  // phase parity of red_bar[0] (bit 0) and red_bar[1] (bit 1)
+  if (ECL > 1) {
+    if (tid == 0) {
+      mbar_expect_tx(&S.red_bar[0], red_bytes);
+      mbar_expect_tx(&S.red_bar[1], red_bytes);
+    }
+    cluster.sync();
+  }
   G.sync();
   auto gsync = [&]() { G.sync(); };
   rng_tab_fill(S.tab, tab_mem.W, seed, stream, s_rng.n, tid, G.size, gsync);
@@ -1164,21 +1212,47 @@ __device__ void run_job(const BisectionArgs &a, ChainState *cs, int window, unsi
         auto reduce = [&]() -> double {
           const int par = xc & 1;
           xc++;
-          if (warp == 0 && lane < kRed) {
-            double v = 0.0;
-            for (int w = 0; w < nwarps; w++) v += sh_red[w][lane];
-            if (ECL > 1)
-              for (unsigned r = 0; r < CL; r++) cluster.map_shared_rank(&xchg[par][rank][0], r)[lane] = v;
-            else
-              xchg[par][0][lane] = v;
-          }
-          if (ECL > 1)
-            cluster.sync();
-          else
-            __syncwarp();
           double v = 0.0;
-          if (warp == 0 && lane < kRed)
-            for (unsigned r = 0; r < ECL; r++) v += xchg[par][r][lane];
+          if (warp != 0) return v;
+          if (lane < kRed) {
+            // all loads first, then a fixed pairwise tree (16 warps at most)
+            double t[16];
+#pragma unroll
+            for (int w = 0; w < 16; w++) t[w] = w < nwarps ? sh_red[w][lane] : 0.0;
+#pragma unroll
+            for (int h = 8; h > 0; h >>= 1)
+#pragma unroll
+              for (int w = 0; w < h; w++) t[w] += t[w + h];
+            v = t[0];
+            if (ECL > 1) {
+              // this CTA's partials into xchg[par][rank] of every CTA of the cluster
+              const unsigned dst = smem_addr(&xchg[par][rank][lane]), bar = smem_addr(&S.red_bar[par]);
+              for (unsigned r = 0; r < CL; r++) st_async_f64(mapa_u32(dst, r), v, mapa_u32(bar, r));
+            } else {
+              xchg[par][0][lane] = v;
+            }
+          }
+          if (ECL > 1) {
+            // Bounded wait for every CTA's partials.  A peer sends to this
+            // buffer again only for the reduction after next, which needs
+            // this CTA's next partials, so the next use is posted now.
+            bool ok = false;
+            for (int it = 0; it < kRedWaitCap && !ok; it++) ok = mbar_try_wait_cluster(&S.red_bar[par], (rph >> par) & 1u);
+            rph ^= 1u << par;
+            if (!ok) status = PIMC_E_CAP;
+            __syncwarp();
+            if (lane == 0) mbar_expect_tx(&S.red_bar[par], red_bytes);
+          } else {
+            __syncwarp();
+          }
+          v = 0.0;
+          if (lane < kRed) {  // rank order, loads first
+            double t[kMaxCluster];
+#pragma unroll
+            for (int r = 0; r < kMaxCluster; r++) t[r] = r < (int)ECL ? xchg[par][r][lane] : 0.0;
+#pragma unroll
+            for (int r = 0; r < kMaxCluster; r++) v += t[r];
+          }
           return v;
         };
         // ---- Metropolis test, identical in every CTA (warp 0) ----
@@ -1499,6 +1573,8 @@ __global__ void __launch_bounds__(512, 1) bisection_kernel(BisectionArgs a) {
   if (threadIdx.x == 0) {
     mbar_init(&s_bar, 1);
     mbar_init(&S.test_bar, 1);
+    mbar_init(&S.red_bar[0], 1);
+    mbar_init(&S.red_bar[1], 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   __syncthreads();
