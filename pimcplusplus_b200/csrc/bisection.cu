@@ -113,6 +113,16 @@ __device__ __forceinline__ double warp_sum(double v) {
   for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
   return v;
 }
+// warp_sum when only lanes [0, n) can hold nonzero values: the butterfly
+// starts at the half of the smallest power of two >= n (the steps skipped
+// would add exact zeros to lane 0, so lane 0's sum has the same bits), and
+// lane 0's sum is broadcast.
+__device__ __forceinline__ double warp_sum_n(double v, int n) {
+  int o = 16;
+  while (o > 1 && o >= n) o >>= 1;
+  for (; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return __shfl_sync(0xffffffffu, v, 0);
+}
 
 // BisectionStageClass::Sample (BisectionStage.cc:128-289) for one level on
 // the window held in shared memory, run by one full warp: writes the NEW
@@ -171,8 +181,8 @@ __device__ __forceinline__ double sample_level_warp(double (*w_old)[3], double (
     }
     for (int i = 0; i < 3; i++) w_new[mid][i] = rbar[i] + Delta[i];
   }
-  lo = warp_sum(lo);
-  ln = warp_sum(ln);
+  lo = warp_sum_n(lo, nmid);
+  ln = warp_sum_n(ln, nmid);
   __syncwarp();
   return -ln + lo;
 }
@@ -240,25 +250,17 @@ struct StageSums {
 };
 
 // One in-fit tricubic term of a pass, listed per warp for its team.
-template <typename R>
-struct TriTerm;
-template <>
-struct TriTerm<double> {
+struct TriTerm {
   double u[3];
   int code;  // cell << 1 | copy (1: NEW)
   int pad;
 };
-template <>
-struct TriTerm<float> {
-  float u[3];
-  int code;
-};
 // Terms listed per warp and pass (two (item, copy) units per lane).
 constexpr int kTriTermsPerWarp = 64;
-// Shared memory of the lists: 16 warps of TriTerm<double>, enough for either precision.
-constexpr unsigned kTriTermBytes = 16u * kTriTermsPerWarp * sizeof(TriTerm<double>);
+// Shared memory of the lists: 16 warps.
+constexpr unsigned kTriTermBytes = 16u * kTriTermsPerWarp * sizeof(TriTerm);
 
-// The tricubic short-range sum of one stage over this CTA's items
+// The FP64 tricubic short-range sum of one stage over this CTA's items
 // [beg, beg + items) (item = link * np + partner index), each item evaluated
 // for the OLD and the NEW copy of the moved particle: 2 items (item, copy)
 // units.  Per pass every evaluating warp takes an even share of at most 64
@@ -267,38 +269,34 @@ constexpr unsigned kTriTermBytes = 16u * kTriTermsPerWarp * sizeof(TriTerm<doubl
 // fallback of the terms outside the fit itself, from the potential's (y, d2y)
 // pairs in shared memory (pp; null: the global tables).  The terms inside the
 // fit are listed in shared memory (tq: kTriTermsPerWarp per warp) and
-// gathered by teams of TS lanes (tricubic_team_part): TS = 4 FP64, 2 FP32.
-// Sums as stage_sums: (so, sn) the run's precision (mixed: two-sum with
-// (co, cn) and the magnitudes in mb), (so2, sn2) the other precision's terms
-// with SHADOW.
-template <typename R, bool SHADOW>
+// gathered by teams of 4 lanes (tricubic_team_part).  Sums into (so, sn);
+// with SHADOW the mixed path's terms into (so2, sn2).
+template <bool SHADOW>
 __device__ __forceinline__ void tricubic_stage(const BisectionArgs &a, const double (*w_old)[3],
-                                               const double (*w_new)[3], const typename Pair2<R>::T *pp, int lv,
-                                               int slice1, int ptcl, int beg, int items, int etid, int ethreads,
-                                               const int *plist, int np, TriTerm<R> *tq, double &so, double &sn,
-                                               float &co, float &cn, float &mb, double &so2, double &sn2) {
-  constexpr bool MIX = std::is_same<R, float>::value;
-  constexpr int TS = MIX ? 2 : 4, TPW = 32 / TS;
+                                               const double (*w_new)[3], const double2 *pp, int lv, int slice1,
+                                               int ptcl, int beg, int items, int etid, int ethreads,
+                                               const int *plist, int np, TriTerm *tq, double &so, double &sn,
+                                               double &so2, double &sn2) {
+  constexpr int TS = 4, TPW = 32 / TS;
   const DevSystem &sys = a.sys;
   const DTricubic<double> &t64 = a.pa.t64;
   const int N = sys.N;
   const int skip = 1 << lv;
   const int lane = etid & 31, wi = etid >> 5, nw = ethreads >> 5;
   const int pt = lane & (TS - 1);
-  TriTerm<R> *E = tq + wi * kTriTermsPerWarp;
+  TriTerm *E = tq + wi * kTriTermsPerWarp;
   const size_t lvl = (size_t)lv * t64.nq * t64.ny * t64.nt;
-  const R *F = tricubic_of<R>(a.pa).U + lvl * 8;
+  const double *F = t64.U + lvl * 8;
   double beta = t64.smallest_beta;
   for (int i = 0; i < lv; i++) beta *= 2.0;
   beta = 0.5 * beta;
-  const float hb = (float)beta;
   const int U = 2 * items;
   const int P = (U + 2 * ethreads - 1) / (2 * ethreads);
   const int cw = P > 0 ? (U + P * nw - 1) / (P * nw) : 0;  // <= 64
   for (int p = 0; p < P; p++) {
     const int ws = (p * nw + wi) * cw, we = min(U, ws + cw);
     bool in[2];
-    TriTerm<R> tt[2];
+    TriTerm tt[2];
 #pragma unroll
     for (int s = 0; s < 2; s++) {
       const int u = ws + lane + 32 * s;
@@ -319,36 +317,19 @@ __device__ __forceinline__ void tricubic_stage(const BisectionArgs &a, const dou
         double dA[3], dB[3];
         dist_disp(w[r0], a2, w[r0 + skip], b2, sys, dA, dB);
         const LinkGeom<double> g = link_geom<double>(dA, dB);
-        const TriPrep<R> pr = tricubic_prep<R>(t64, g.q, g.z, g.s2);
+        const TriPrep<double> pr = tricubic_prep<double>(t64, g.q, g.z, g.s2);
         if (pr.inside) {
           in[s] = true;
           tt[s].u[0] = pr.u[0];
           tt[s].u[1] = pr.u[1];
           tt[s].u[2] = pr.u[2];
           tt[s].code = (pr.cell << 1) | isn;
-        } else if (MIX) {  // the primitive action 1/2 beta_l (V(r) + V(r'))
-          MixedU va, vb;
-          if (pp) {
-            va = pot_V_pairs_mixed(t64.pot_grid, reinterpret_cast<const float2 *>(pp), pr.r);
-            vb = pot_V_pairs_mixed(t64.pot_grid, reinterpret_cast<const float2 *>(pp), pr.rp);
-          } else {
-            va = pot_V_mixed(t64, a.pa.t32, pr.r);
-            vb = pot_V_mixed(t64, a.pa.t32, pr.rp);
-          }
-          two_sum_add(isn ? sn : so, isn ? cn : co, (double)(hb * ((float)va.v + (float)vb.v)));
-          mb += hb * (va.m + vb.m);
-        } else {
-          const double v = pp ? pot_V_pairs(t64.pot_grid, reinterpret_cast<const double2 *>(pp), pr.r) +
-                                    pot_V_pairs(t64.pot_grid, reinterpret_cast<const double2 *>(pp), pr.rp)
+        } else {  // the primitive action 1/2 beta_l (V(r) + V(r'))
+          const double v = pp ? pot_V_pairs(t64.pot_grid, pp, pr.r) + pot_V_pairs(t64.pot_grid, pp, pr.rp)
                               : pot_V(t64, pr.r) + pot_V(t64, pr.rp);
           (isn ? sn : so) += beta * v;
         }
-        if (SHADOW) {
-          if (MIX)
-            (isn ? sn2 : so2) += tricubic_pa<double, false>(t64, g.q, g.z, g.s2, lv);
-          else
-            (isn ? sn2 : so2) += tricubic_pa_mixed(t64, a.pa.t32, g.q, g.z, g.s2, lv).v;
-        }
+        if (SHADOW) (isn ? sn2 : so2) += tricubic_pa_mixed(t64, a.pa.t32, g.q, g.z, g.s2, lv).v;
       }
     }
     // list the in-fit terms, then each team gathers every TPW-th of them
@@ -359,15 +340,8 @@ __device__ __forceinline__ void tricubic_stage(const BisectionArgs &a, const dou
     if (in[1]) E[n0 + __popc(m1 & below)] = tt[1];
     __syncwarp();
     for (int e = lane / TS; e < n; e += TPW) {
-      const TriTerm<R> T = E[e];
-      const int cell = T.code >> 1;
-      const R v = tricubic_team_part(F, t64, cell, T.u, pt);
-      if (MIX) {
-        two_sum_add((T.code & 1) ? sn : so, (T.code & 1) ? cn : co, (double)v);
-        if (pt == 0) mb += __ldg(&a.pa.t32.mbound[lvl + cell]);
-      } else {
-        ((T.code & 1) ? sn : so) += (double)v;
-      }
+      const TriTerm T = E[e];
+      ((T.code & 1) ? sn : so) += tricubic_team_part(F, t64, T.code >> 1, T.u, pt);
     }
     __syncwarp();
   }
@@ -415,9 +389,10 @@ __device__ __forceinline__ StageSums stage_sums(const BisectionArgs &a, const do
     const int chunk = (total + (int)CL - 1) / (int)CL;
     const int beg = chunk * (int)rank;
     const int end = min(total, beg + chunk);
-    tricubic_stage<R, SHADOW>(a, w_old, w_new, reinterpret_cast<const typename Pair2<R>::T *>(dg), lv, slice1, ptcl,
-                              beg, max(0, end - beg), etid, ethreads, plist, np,
-                              reinterpret_cast<TriTerm<R> *>(tq), so, sn, co, cn, mb, so2, sn2);
+    if constexpr (!MIX)
+      tricubic_stage<SHADOW>(a, w_old, w_new, reinterpret_cast<const double2 *>(dg), lv, slice1, ptcl, beg,
+                             max(0, end - beg), etid, ethreads, plist, np, reinterpret_cast<TriTerm *>(tq), so, sn,
+                             so2, sn2);
   } else if (lv == 0 || a.sr_higher) {  // ShortRangeClass::SingleAction over partners x links
     // partners: all others (plist null, np = N - 1) or the moved particle's
     // neighbour list (np entries, ascending)
@@ -616,7 +591,7 @@ __device__ __forceinline__ double2 kinetic_sums(const double (*w_old)[3], const 
       sn += kinetic_link(vn, F, sys.num_images, sys);
     }
   }
-  return make_double2(warp_sum(so), warp_sum(sn));
+  return make_double2(warp_sum_n(so, (1 << num_levels) >> lv), warp_sum_n(sn, (1 << num_levels) >> lv));
 }
 
 // The mixed path's FP64 re-evaluation of a stage (and, with need_prev, of the
@@ -847,6 +822,10 @@ __device__ void run_job(const BisectionArgs &a, ChainState *cs, int window, unsi
   // move may start from a window another slot is about to write)
   const int specwarp = (nwarps >= 4 && !prop) ? nwarps - 2 : -1;
   const int ethreads = (nwarps - (specwarp >= 0 ? 2 : 1)) * 32;  // evaluating threads: warps below the samplers
+  // The moved particle's kinetic links: with 8 or more evaluating warps the
+  // last of them sums them after its pair terms (the item split leaves it the
+  // fewest), so the level sampler's warp only samples; otherwise the sampler.
+  const int kinwarp = (ethreads >> 5) >= 8 ? (ethreads >> 5) - 1 : -1;
   const bool evaluator = tid < ethreads;
   const DevSystem &sys = a.sys;
   const int N = sys.N;
@@ -875,15 +854,13 @@ __device__ void run_job(const BisectionArgs &a, ChainState *cs, int window, unsi
       stage_src_s = reinterpret_cast<const P2S *>(ds.diag) + (size_t)ds.tau_pos * ds.diag_stride;
     }
   } else if (KIND == PA_TRICUBIC) {
+    // the FP64 path's team stage (the mixed path's one-lane terms read the
+    // global tables; its FP64 re-evaluation too)
     tail = kTriTermBytes;
-    const DTricubic<R> &t = tricubic_of<R>(a.pa);
-    const unsigned b0 = (unsigned)(t.pot_pairs_n * sizeof(P2));
-    const unsigned b1 = SHADOW ? (unsigned)(tricubic_of<RS>(a.pa).pot_pairs_n * sizeof(P2S)) : 0u;
-    if (b0 + b1 + tail <= dyn_cap) {
+    const unsigned b0 = (unsigned)(a.pa.t64.pot_pairs_n * sizeof(double2));
+    if (!std::is_same<R, float>::value && b0 + tail <= dyn_cap) {
       bytes = b0;
-      bytes_s = b1;
-      stage_src = t.pot_pairs;
-      if (SHADOW) stage_src_s = tricubic_of<RS>(a.pa).pot_pairs;
+      stage_src = a.pa.t64.pot_pairs;
     }
   }
   void *tq = dyn + ((bytes + bytes_s + 15u) & ~15u);
@@ -1136,8 +1113,17 @@ __device__ void run_job(const BisectionArgs &a, ChainState *cs, int window, unsi
           const StageSums v = stage_sums<KIND, R, SHADOW>(a, w_old, w_new, diag_smem ? diag_smem + level * st : nullptr,
                                                           diag_smem_s ? diag_smem_s + level * sts : nullptr, level,
                                                           slice1, ptcl, erank, ECL, tid, ethreads, plist, np, tq);
-          const double r0 = warp_sum(v.so), r1 = warp_sum(v.sn), r2 = warp_sum(v.eb);
-          const double r3 = SHADOW ? warp_sum(v.so2) : 0.0, r4 = SHADOW ? warp_sum(v.sn2) : 0.0;
+          double r0 = warp_sum(v.so), r1 = warp_sum(v.sn);
+          const double r2 = warp_sum(v.eb);
+          double r3 = SHADOW ? warp_sum(v.so2) : 0.0, r4 = SHADOW ? warp_sum(v.sn2) : 0.0;
+          if (warp == kinwarp && erank == 0) {
+            // the moved particle's kinetic links, once per evaluation group
+            const double2 k = kinetic_sums(w_old, w_new, L, level, sys, lane);
+            r0 += k.x;
+            r1 += k.y;
+            r3 += k.x;
+            r4 += k.y;
+          }
           if (lane == 0) {
             sh_red[warp][0] = r0;
             sh_red[warp][1] = r1;
@@ -1191,7 +1177,7 @@ __device__ void run_job(const BisectionArgs &a, ChainState *cs, int window, unsi
             }
           }
           if (lane < kRed) sh_red[warp][lane] = 0.0;
-          if (warp == sampler && erank == 0) {
+          if (warp == sampler && erank == 0 && kinwarp < 0) {
             // the moved particle's kinetic links, once per evaluation group
             const double2 k = kinetic_sums(w_old, w_new, L, level, sys, lane);
             __syncwarp();
@@ -1349,7 +1335,16 @@ __device__ void run_job(const BisectionArgs &a, ChainState *cs, int window, unsi
           if (evaluator) {
             const double4 v = stage_sums_reeval<KIND>(a, w_old, w_new, level, slice1, ptcl, erank, ECL, tid, ethreads,
                                                       plist, np, need_prev, prev_plist, prev_np, tq);
-            const double r0 = warp_sum(v.x), r1 = warp_sum(v.y), r2 = warp_sum(v.z), r3 = warp_sum(v.w);
+            double r0 = warp_sum(v.x), r1 = warp_sum(v.y), r2 = warp_sum(v.z), r3 = warp_sum(v.w);
+            if (warp == kinwarp && erank == 0) {  // the kinetic links, as in the first pass
+              const double2 k = kinetic_sums(w_old, w_new, L, level, sys, lane);
+              const double2 kp = need_prev ? kinetic_sums(w_old, w_new, L, level + 1, sys, lane)
+                                           : make_double2(0.0, 0.0);
+              r0 += k.x;
+              r1 += k.y;
+              r2 += kp.x;
+              r3 += kp.y;
+            }
             if (lane == 0) {
               sh_red[warp][0] = r0;
               sh_red[warp][1] = r1;
@@ -1359,7 +1354,7 @@ __device__ void run_job(const BisectionArgs &a, ChainState *cs, int window, unsi
             }
           } else {
             if (lane < kRed) sh_red[warp][lane] = 0.0;
-            if (warp == sampler && erank == 0) {  // the kinetic links, as in the first pass
+            if (warp == sampler && erank == 0 && kinwarp < 0) {  // the kinetic links, as in the first pass
               const double2 k = kinetic_sums(w_old, w_new, L, level, sys, lane);
               const double2 kp = need_prev ? kinetic_sums(w_old, w_new, L, level + 1, sys, lane)
                                            : make_double2(0.0, 0.0);
@@ -1786,13 +1781,10 @@ cudaError_t batch_occupancy(int precision, int shadow, int threads, size_t dyn, 
 
 size_t bisection_dyn_smem(const BisectionArgs &a, int precision, int shadow) {
   if (a.pa.kind == PA_TRICUBIC) {
-    // the potential's pairs (and the other precision's with shadow) when they
-    // fit in 160 KB with the term lists; the term lists alone otherwise
-    const size_t p64 = (size_t)a.pa.t64.pot_pairs_n * sizeof(double2);
-    const size_t p32 = (size_t)a.pa.t32.pot_pairs_n * sizeof(float2);
-    size_t pot = precision == PIMC_MIXED ? p32 : p64;
-    if (shadow) pot += precision == PIMC_MIXED ? p64 : p32;
-    pot = (pot + 15) & ~(size_t)15;
+    // FP64: the potential's pairs when they fit in 160 KB with the term
+    // lists; the term lists alone otherwise (and on the mixed path, whose
+    // FP64 re-evaluation uses them)
+    const size_t pot = precision == PIMC_MIXED ? 0 : (size_t)a.pa.t64.pot_pairs_n * sizeof(double2);
     return pot + kTriTermBytes <= (size_t)160 * 1024 ? pot + kTriTermBytes : (size_t)kTriTermBytes;
   }
   if (a.pa.kind != PA_DAVID) return 0;

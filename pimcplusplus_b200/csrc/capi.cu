@@ -445,19 +445,18 @@ int pimc_pa_tricubic(pimc_context *ctx, int sp1, int sp2, const double qgrid[3],
     if ((rc = upload(ctx, d32.data(), d32.size(), &t32.pot_d2))) return rc;
   }
   {
-    // (y, d2y) pairs for the device moves' shared-memory copy; the padding row is zero.
+    // FP64 (y, d2y) pairs for the device moves' shared-memory copy (the FP64
+    // path); the padding row is zero.
     const int np2 = (pot_n + 1) & ~1;
     std::vector<double> p64((size_t)np2 * 2, 0.0);
-    std::vector<float> p32((size_t)np2 * 2, 0.0f);
     for (int i = 0; i < pot_n; i++) {
       p64[2 * i] = pot_data[i];
       p64[2 * i + 1] = pd2[i];
-      p32[2 * i] = (float)pot_data[i];
-      p32[2 * i + 1] = (float)pd2[i];
     }
     if ((rc = upload(ctx, p64.data(), p64.size(), &t64.pot_pairs))) return rc;
-    if ((rc = upload(ctx, p32.data(), p32.size(), &t32.pot_pairs))) return rc;
-    t64.pot_pairs_n = t32.pot_pairs_n = np2;
+    t64.pot_pairs_n = np2;
+    t32.pot_pairs = nullptr;
+    t32.pot_pairs_n = 0;
   }
   ctx->pa.kind = PA_TRICUBIC;
   return PIMC_OK;

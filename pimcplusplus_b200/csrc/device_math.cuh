@@ -748,15 +748,14 @@ __device__ __forceinline__ void ld4_nc(const double *p, double v[4]) {
   asm("ld.global.nc.v4.f64 {%0, %1, %2, %3}, [%4];" : "=d"(v[0]), "=d"(v[1]), "=d"(v[2]), "=d"(v[3]) : "l"(p));
 }
 
-// One lane's part of a term evaluated by a team.  The cell's four (x, y) node
-// pairs k = 2 dx + dy each hold the nodes iz and iz + 1 back to back (128
-// bytes FP64, 64 bytes FP32).  FP64: a team of 4 lanes; part pt takes
-// components 4 (pt & 1) .. 4 (pt & 1) + 3 of node iz + (pt >> 1) of every
-// pair.  FP32: a team of 2 lanes; part pt takes the 8 components of node
-// iz + pt of every pair.  A lane loads 4 x 32 bytes per term and the team's
-// lanes load the same pairs together, so a warp-wide load touches one or two
-// cache lines per team instead of one per lane.  The parts add up to
-// tricubic_eval's value (summed in another order).  F: this level's nodes.
+// One lane's part of a term evaluated by a team of 4 lanes (the FP64 path).
+// The cell's four (x, y) node pairs k = 2 dx + dy each hold the nodes iz and
+// iz + 1 back to back (128 bytes); part pt takes components 4 (pt & 1) ..
+// 4 (pt & 1) + 3 of node iz + (pt >> 1) of every pair.  A lane loads 4 x 32
+// bytes per term and the team's lanes load the same pairs together, so a
+// warp-wide load touches one or two cache lines per team instead of one per
+// lane.  The parts add up to tricubic_eval's value (summed in another order).
+// F: this level's nodes.
 __device__ __forceinline__ double tricubic_team_part(const double *F, const DTricubic<double> &t, int cell,
                                                      const double u[3], int pt) {
   double a[4], b[4], c[4];
@@ -782,43 +781,11 @@ __device__ __forceinline__ double tricubic_team_part(const double *F, const DTri
   }
   return s;
 }
-__device__ __forceinline__ float tricubic_team_part(const float *F, const DTricubic<double> &t, int cell,
-                                                    const float u[3], int pt) {
-  float a[4], b[4], c[4];
-  hermite4(u[0], (float)t.qg.delta, a);
-  hermite4(u[1], (float)t.yg.delta, b);
-  hermite4(u[2], (float)t.tg.delta, c);
-  const size_t sy = (size_t)t.nt * 8, sx = (size_t)t.ny * sy;
-  const float *p = F + (size_t)cell * 8 + pt * 8;
-  Node8<float> v[4];
-#pragma unroll
-  for (int k = 0; k < 4; k++) v[k].load(p + (k >> 1) * sx + (k & 1) * sy);
-  const float Cv = pt ? c[1] : c[0], Cd = pt ? c[3] : c[2];
-  float s = 0.0f;
-#pragma unroll
-  for (int k = 0; k < 4; k++) {
-    const int dx = k >> 1, dy = k & 1;
-    const float A0 = a[dx], A1 = a[2 + dx], B0 = b[dy], B1 = b[2 + dy];
-    const float P00 = A0 * B0, P10 = A1 * B0, P01 = A0 * B1, P11 = A1 * B1;
-    s += Cv * (P00 * v[k].v[0] + P10 * v[k].v[1] + P01 * v[k].v[2] + P11 * v[k].v[4]) +
-         Cd * (P00 * v[k].v[3] + P10 * v[k].v[5] + P01 * v[k].v[6] + P11 * v[k].v[7]);
-  }
-  return s;
-}
-
 // SplinePot::V from (y, d2y) pairs (a shared-memory copy): the same
-// arithmetic as pot_V and pot_V_mixed, zero beyond the grid end.
+// arithmetic as pot_V, zero beyond the grid end.
 __device__ __forceinline__ double pot_V_pairs(const DGrid<double> &g, const double2 *pp, double r) {
   const double v = spline_pairs(g, pp, r <= g.end ? r : g.end);
   return r <= g.end ? v : 0.0;
-}
-__device__ __forceinline__ MixedU pot_V_pairs_mixed(const DGrid<double> &g, const float2 *pp, double r) {
-  MixedU u = spline_pairs_mixed(g, pp, r <= g.end ? r : g.end);
-  if (!(r <= g.end)) {
-    u.v = 0.0;
-    u.m = 0.0f;
-  }
-  return u;
 }
 
 // QuinticSpline::operator() on the mixed path: interval and P = x - x_I in

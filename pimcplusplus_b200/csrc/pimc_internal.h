@@ -78,7 +78,7 @@ struct DTricubic {
   const R *dU;  // same
   DGrid<R> pot_grid;
   const R *pot_y, *pot_d2;  // SplinePot natural cubic spline
-  const R *pot_pairs;        // the same as interleaved (y, d2y) pairs [pot_pairs_n][2], staged in shared memory
+  const R *pot_pairs;        // FP64: the same as interleaved (y, d2y) pairs [pot_pairs_n][2] (FP32: null)
   int pot_pairs_n;           // pot_grid.n rounded up to an even count (16-byte rows)
   // Mixed path: per level and cell (indexed by the cell's low node, [beta][nq][ny][nt])
   // a bound on sum_j |c_j| |b_j| of the U evaluation anywhere in the cell

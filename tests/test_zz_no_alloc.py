@@ -76,3 +76,40 @@ def test_noalloc_rejects_oversized_call():
         1, 600000, 3, box.ctypes.data_as(C.POINTER(C.c_double)), 1, 1.0, 5.0, 100, 0, 1,
         act.ctypes.data_as(C.POINTER(C.c_int)), 1, 0, 1, None)
     assert rc == P.PIMC_E_ARG if hasattr(P, "PIMC_E_ARG") else rc == 1
+
+
+def test_noalloc_matches_oracle_below_grid_start(tmp_path):
+    """Against the FP64 oracle directly, on a path where particle 8 sits closer
+    to particle 7 than the table's first grid point at every slice (the
+    r < rmin clamp of calcUsqzFast), with 7 and 8 both moved (their pair
+    counted once) and alone."""
+    import torch
+
+    import oracle as O
+
+    cfg, tau, box, dm = lj_case(tmp_path)
+    n, slices = cfg["N"], cfg["M"] + 1
+    tables = P.read_dm(dm, tau)
+    path = random_walk_path(n, slices, box, 0.35, 321, far=0.1)
+    path[:, 8, :] = path[:, 7, :] + np.array([0.5 * tables["grid_start"], 0.0, 0.0])
+    o = O.System(n, slices, box, tau, W.HE4_LAMBDA, 0)
+    o.set_pa(O.PairAction.from_dm(dm, tau, 0))
+    o.set_path(path)
+    dev_path = torch.tensor(path, dtype=torch.float64, device="cuda:0").contiguous()
+    out = torch.zeros(1, dtype=torch.float64, device="cuda:0")
+    boxc = np.ascontiguousarray(box, dtype=np.float64)
+    stream = torch.cuda.current_stream().cuda_stream
+    for (s1, s2, active, level) in [(0, 8, [7, 8], 0), (4, 12, [8], 1), (0, 40, [7, 8, 30], 0)]:
+        lev = level + tables["tau_pos"]
+        diag = np.stack([tables["ukj"][lev][:, 1], tables["ukj_d2"][lev][:, 1]], axis=1)
+        dev_diag = torch.tensor(diag, dtype=torch.float64, device="cuda:0").contiguous()
+        act = np.ascontiguousarray(active, dtype=np.int32)
+        rc = P.lib().pimc_shortrange_single_noalloc(
+            dev_path.data_ptr(), n, slices, boxc.ctypes.data_as(C.POINTER(C.c_double)), dev_diag.data_ptr(),
+            tables["grid_start"], tables["grid_end"], tables["num_grid"], s1, s2,
+            act.ctypes.data_as(C.POINTER(C.c_int)), len(act), level, out.data_ptr(), stream)
+        assert rc == P.PIMC_OK
+        torch.cuda.synchronize()
+        got = float(out.item())
+        ref = o.shortrange_single(s1, s2, list(active), level)
+        assert abs(got - ref) <= REL64 * abs(ref), (s1, s2, active, level, got, ref)
