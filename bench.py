@@ -796,7 +796,7 @@ def run_c4(args, P, timer, local, rank, agg, launches):
         d.longrange_coulomb(49, use_background=True)
         d.set_path(start)
         bb = P.BisectionBlock(d, L, spb, precision=precision, shadow=shadow, cluster_ctas=args.c4_cluster,
-                              threads_per_cta=256, schedule=schedule if schedule is not None else P.WINDOWS,
+                              threads_per_cta=args.c4_threads, schedule=schedule if schedule is not None else P.WINDOWS,
                               use_longrange=True)
         bb.seed(500 + rank)
         return d, bb, nk
@@ -964,6 +964,7 @@ def main():
     ap.add_argument("--c5-prop-threads", type=int, default=512)
     ap.add_argument("--c4-cluster", type=int, default=8)
     ap.add_argument("--c4-steps-per-block", type=int, default=16)
+    ap.add_argument("--c4-threads", type=int, default=256)
     ap.add_argument("--c5-steps-per-block", type=int, default=16)
     ap.add_argument("--c3-chains", type=int, default=1024)
     ap.add_argument("--c3-blocks", type=int, default=4)
