@@ -964,7 +964,7 @@ def main():
     ap.add_argument("--c5-prop-threads", type=int, default=512)
     ap.add_argument("--c4-cluster", type=int, default=8)
     ap.add_argument("--c4-steps-per-block", type=int, default=16)
-    ap.add_argument("--c4-threads", type=int, default=256)
+    ap.add_argument("--c4-threads", type=int, default=512)
     ap.add_argument("--c5-steps-per-block", type=int, default=16)
     ap.add_argument("--c3-chains", type=int, default=1024)
     ap.add_argument("--c3-blocks", type=int, default=4)
