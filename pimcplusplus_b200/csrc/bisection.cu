@@ -255,16 +255,17 @@ struct TriTerm {
   int code;  // cell << 1 | copy (1: NEW)
   int pad;
 };
-// Terms listed per warp and pass (two (item, copy) units per lane).
-constexpr int kTriTermsPerWarp = 64;
+// Terms listed per warp and pass (three (item, copy) units per lane).
+constexpr int kTriTermsPerWarp = 96;
 // Shared memory of the lists: 16 warps.
 constexpr unsigned kTriTermBytes = 16u * kTriTermsPerWarp * sizeof(TriTerm);
 
 // The FP64 tricubic short-range sum of one stage over this CTA's items
 // [beg, beg + items) (item = link * np + partner index), each item evaluated
 // for the OLD and the NEW copy of the moved particle: 2 items (item, copy)
-// units.  Per pass every evaluating warp takes an even share of at most 64
-// consecutive units, two per lane.  A lane forms its units' geometry
+// units.  Per pass every evaluating warp takes an even share of at most 96
+// consecutive units, three per lane (C2's 1022 level-0 units of a CTA in one
+// pass).  A lane forms its units' geometry
 // (DistDisp, q, z, s, the fit-region test, the cell) and adds the primitive
 // fallback of the terms outside the fit itself, from the potential's (y, d2y)
 // pairs in shared memory (pp; null: the global tables).  The terms inside the
@@ -291,14 +292,14 @@ __device__ __forceinline__ void tricubic_stage(const BisectionArgs &a, const dou
   for (int i = 0; i < lv; i++) beta *= 2.0;
   beta = 0.5 * beta;
   const int U = 2 * items;
-  const int P = (U + 2 * ethreads - 1) / (2 * ethreads);
-  const int cw = P > 0 ? (U + P * nw - 1) / (P * nw) : 0;  // <= 64
+  const int P = (U + 3 * ethreads - 1) / (3 * ethreads);
+  const int cw = P > 0 ? (U + P * nw - 1) / (P * nw) : 0;  // <= 96
   for (int p = 0; p < P; p++) {
     const int ws = (p * nw + wi) * cw, we = min(U, ws + cw);
-    bool in[2];
-    TriTerm tt[2];
+    bool in[3];
+    TriTerm tt[3];
 #pragma unroll
-    for (int s = 0; s < 2; s++) {
+    for (int s = 0; s < 3; s++) {
       const int u = ws + lane + 32 * s;
       in[s] = false;
       if (u < we) {
@@ -334,10 +335,12 @@ __device__ __forceinline__ void tricubic_stage(const BisectionArgs &a, const dou
     }
     // list the in-fit terms, then each team gathers every TPW-th of them
     const unsigned m0 = __ballot_sync(0xffffffffu, in[0]), m1 = __ballot_sync(0xffffffffu, in[1]);
+    const unsigned m2 = __ballot_sync(0xffffffffu, in[2]);
     const unsigned below = (1u << lane) - 1u;
-    const int n0 = __popc(m0), n = n0 + __popc(m1);
+    const int n0 = __popc(m0), n1 = n0 + __popc(m1), n = n1 + __popc(m2);
     if (in[0]) E[__popc(m0 & below)] = tt[0];
     if (in[1]) E[n0 + __popc(m1 & below)] = tt[1];
+    if (in[2]) E[n1 + __popc(m2 & below)] = tt[2];
     __syncwarp();
     for (int e = lane / TS; e < n; e += TPW) {
       const TriTerm T = E[e];

@@ -3,9 +3,9 @@ oracle's replay of the same moves (BisectionBlock.cc:380-451 on the same
 Philox streams):
 
 * C2: 512 atoms, M = 128, PAtricubicFit 200x50x50, level 4, the bench's
-  launch (concurrent windows, 16-CTA clusters x 512 threads, StepsPerBlock 64);
+  launch (concurrent windows, 16-CTA clusters x 512 threads, StepsPerBlock 128);
 * C4: jellium, 128 electrons, M = 64, 510 k-vectors, the bench's launch
-  (windows, 8-CTA clusters x 256 threads, StepsPerBlock 16), trace and rho_k;
+  (windows, 8-CTA clusters x 512 threads, StepsPerBlock 16), trace and rho_k;
 * C5: 4096 atoms, M = 256, level 5, neighbour lists on the device against the
   oracle's all-partner sums (windows, 16-CTA clusters x 512 threads);
 * C3: a subset of the bench's 1024-chain set holding its costliest chains
@@ -53,7 +53,7 @@ def test_c2_bench_launch(precision):
     d = P.PathData(n, S, box, tau, W.HE4_LAMBDA, 0)
     d.pa_tricubic(qg, yg, tg, tau, umat, dumat, pg, pot)
     d.set_path(o.get_path(0))
-    spb, rounds = 64, 2
+    spb, rounds = 128, 2
     o.bisection_config(L, spb)
     o.rng_seed(1000)
     ref = o.run_windows(rounds)
@@ -74,7 +74,7 @@ def test_c4_bench_launch(precision):
     o.bisection_config(L, spb, use_longrange=True)
     o.rng_seed(500)
     ref = o.run_windows(rounds)
-    bb = P.BisectionBlock(d, L, spb, precision=precision, cluster_ctas=8, threads_per_cta=256, schedule=P.WINDOWS,
+    bb = P.BisectionBlock(d, L, spb, precision=precision, cluster_ctas=8, threads_per_cta=512, schedule=P.WINDOWS,
                           use_longrange=True)
     bb.seed(500)
     got, stats = bb.MakeMoves(rounds)
