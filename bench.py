@@ -675,7 +675,7 @@ def run_c1(args, P, timer, local, rank, agg, launches):
             d = P.PathData(n, m + 1, box, tau, W.HE4_LAMBDA, 0, device=local)
             d.pa_david_from_dm(dm, 0)
             d.set_path(start)
-            bb = P.BisectionBlock(d, L, spb, precision=prec, cluster_ctas=1, threads_per_cta=128,
+            bb = P.BisectionBlock(d, L, spb, precision=prec, cluster_ctas=args.c1_cluster, threads_per_cta=args.c1_threads,
                                   schedule=P.WINDOWS)
             bb.seed(70 + rank)
             bb.MakeMoves(20, trace=False)  # equilibrate
@@ -868,7 +868,8 @@ def run_c5(args, P, timer, local, rank, agg, launches):
             bb = P.BisectionBlock(d, L, spb, precision=precision, cluster_ctas=proposals,
                                   threads_per_cta=args.c5_prop_threads, schedule=P.PROPOSALS, neighbor_skin=skin)
         else:
-            bb = P.BisectionBlock(d, L, spb, precision=precision, cluster_ctas=args.c5_cluster, threads_per_cta=512,
+            bb = P.BisectionBlock(d, L, spb, precision=precision, cluster_ctas=args.c5_cluster,
+                                  threads_per_cta=args.c5_threads,
                                   schedule=P.WINDOWS, neighbor_skin=skin)
         bb.seed(900 + rank)
         return d, bb
@@ -965,6 +966,9 @@ def main():
     ap.add_argument("--c4-cluster", type=int, default=8)
     ap.add_argument("--c4-steps-per-block", type=int, default=16)
     ap.add_argument("--c4-threads", type=int, default=512)
+    ap.add_argument("--c1-cluster", type=int, default=8)
+    ap.add_argument("--c1-threads", type=int, default=256)
+    ap.add_argument("--c5-threads", type=int, default=512)
     ap.add_argument("--c5-steps-per-block", type=int, default=16)
     ap.add_argument("--c3-chains", type=int, default=1024)
     ap.add_argument("--c3-blocks", type=int, default=4)

@@ -4,6 +4,8 @@ Philox streams):
 
 * C2: 512 atoms, M = 128, PAtricubicFit 200x50x50, level 4, the bench's
   launch (concurrent windows, 16-CTA clusters x 512 threads, StepsPerBlock 128);
+* C1: 64 atoms, M = 40, 1-D primitive table, level 3, the bench's launch
+  (windows, 8-CTA clusters x 256 threads, StepsPerBlock 64);
 * C4: jellium, 128 electrons, M = 64, 510 k-vectors, the bench's launch
   (windows, 8-CTA clusters x 512 threads, StepsPerBlock 16), trace and rho_k;
 * C5: 4096 atoms, M = 256, level 5, neighbour lists on the device against the
@@ -62,6 +64,31 @@ def test_c2_bench_launch(precision):
     bb.seed(1000)
     got, stats = bb.MakeMoves(rounds)
     assert compare(ref, got, stats) > 700
+    assert np.max(np.abs(d.get_path(P.OLDMODE) - o.get_path(0))) < 1e-9
+    d.close()
+
+
+@pytest.mark.parametrize("precision", [P.FP64, P.MIXED])
+def test_c1_bench_launch(precision, tmp_path):
+    cfg = dict(W.CONFIGS["C1"])
+    tau, box = W.derived(cfg)
+    n, S, L = cfg["N"], cfg["M"] + 1, cfg["levels"]
+    dm = W.make_dm_for(cfg, str(tmp_path))
+    o = O.System(n, S, box, tau, W.HE4_LAMBDA, 0)
+    o.set_pa(O.PairAction.from_dm(dm, tau, 0))
+    o.init_random_fixed(17, 0.45 * W.LJ_SIGMA)
+    d = P.PathData(n, S, box, tau, W.HE4_LAMBDA, 0)
+    d.pa_david_from_dm(dm, 0)
+    d.set_path(o.get_path(0))
+    spb, rounds = 64, 3
+    o.bisection_config(L, spb)
+    o.rng_seed(70)
+    ref = o.run_windows(rounds)
+    bb = P.BisectionBlock(d, L, spb, precision=precision, cluster_ctas=8, threads_per_cta=256,
+                          schedule=P.WINDOWS)
+    bb.seed(70)
+    got, stats = bb.MakeMoves(rounds)
+    assert compare(ref, got, stats) > 300
     assert np.max(np.abs(d.get_path(P.OLDMODE) - o.get_path(0))) < 1e-9
     d.close()
 
