@@ -517,23 +517,26 @@ def run_ours(args):
     head_prec, head_guard = (P.MIXED, P.GUARD_RELATIVE) if head_mixed else (P.FP64, P.GUARD_DECISION)
     ms_h, st_h = (msr, strl) if head_mixed else (ms64, st64)
 
-    # end to end through the public API: host path in, moves, path + counters out
+    # end to end through the public API: host path in, moves, path + counters out.  The
+    # host path lives in pinned memory; each step copies it into the OLD copy (the one the
+    # device moves read; NEW is re-synchronised by the moves) and reads OLD back into it.
     progress("C2 end to end")
     d, bb = make(head_prec, guard=head_guard)
-    host = start.copy()
+    host = torch.empty((slices, n, 3), dtype=torch.float64, pin_memory=True).numpy()
+    host[...] = start
     for _ in range(2):
-        d.set_path(host)
+        d.set_path(host, P.OLDMODE)
         bb.MakeMoves(blocks, trace=False)
-        host = d.get_path(P.OLDMODE)
+        d.get_path(P.OLDMODE, out=host)
     s0 = bb.stats()
     e2e_t = 0.0
     for _ in range(args.steps):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        d.set_path(host)
+        d.set_path(host, P.OLDMODE)
         bb.MakeMoves(blocks, trace=False)
         d.ShiftMove()
-        host = d.get_path(P.OLDMODE)
+        d.get_path(P.OLDMODE, out=host)
         e2e_t += time.perf_counter() - t0
     e2e_evals = bb.stats()["pair_evals"] - s0["pair_evals"]
     d.close()

@@ -309,8 +309,12 @@ class PathData:
         assert path.shape == (self.S, self.N, 3), path.shape
         self._check(_lib.pimc_set_path(self.h, copy, _dptr(path)), "set_path")
 
-    def get_path(self, copy=OLDMODE):
-        out = np.empty((self.S, self.N, 3))
+    def get_path(self, copy=OLDMODE, out=None):
+        """The path copy as [slices][particles][3]; into `out` (a C-contiguous
+        float64 array of that shape, e.g. a view of pinned host memory) when given."""
+        if out is None:
+            out = np.empty((self.S, self.N, 3))
+        assert out.shape == (self.S, self.N, 3) and out.dtype == np.float64 and out.flags.c_contiguous, out.shape
         self._check(_lib.pimc_get_path(self.h, copy, _dptr(out)), "get_path")
         return out
 
