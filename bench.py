@@ -596,8 +596,7 @@ def run_ours(args):
             "warmup": args.warmup, "ms_per_step": ms_h / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32 tables, f64 geometry+sums" if head_mixed else "f64",
             "data": "synthetic",
-            "config": {"workload": "C2: 512 LJ He-4, rho 0.02186, T=1.5 K, M=128, tricubic 200x50x50, level 4, "
-                                   "1 chain", "value_leg": "mixed, relative guard" if head_mixed else "fp64",
+            "config": {"workload": W_NAME, "value_leg": "mixed, relative guard" if head_mixed else "fp64",
                        "schedule": args.schedule, "l2": "flushed between steps", "parallelism": f"replicas x{world}"},
             # [pair evals/s, accepted moves/s] of the three C2 legs
             "legs": {"fp64": _pair(r64), "mixed_decision": _pair(rd), "mixed_relative": _pair(rr)},
