@@ -22,7 +22,10 @@
 //    accumulated in FP64.  Partners are identical in the OLD and NEW copies,
 //    so each item reads its partner once and evaluates the pair action for
 //    the OLD and the NEW position of the moved particle, while the sampler
-//    warp draws the next level speculatively.
+//    warp draws the next level speculatively.  The FP64 tricubic path splits
+//    (item, copy) units evenly over the evaluating warps and gathers the
+//    terms inside the fit by 4-lane teams (tricubic_stage).  The moved
+//    particle's kinetic links are summed by the last evaluating warp.
 //  * Three schedules.  Sequential: one window at a time, slice1 drawn from the
 //    Local stream exactly as ChooseTimeSlices does (BisectionBlock.cc:362-374).
 //    Concurrent windows: one launch is one round; the round draws an offset o
@@ -37,11 +40,13 @@
 //    the window has the result of slots 0..P-1 moving one after another, and
 //    a slot whose particle an earlier slot's accepted move came near is made
 //    again (the in-order commit in run_job).
-//  * The 1-D DavidPA diagonal column of every level is staged into shared
-//    memory once per launch by a bulk TMA copy (cp.async.bulk) completing on
-//    an mbarrier; tricubic tables stay in L2/HBM.
-//  * No unbounded waits: the mbarrier wait and the Gaussian rejection loop
-//    carry iteration caps that set the status word and stop the run.
+//  * The 1-D DavidPA diagonal column of every level (tricubic, FP64 path:
+//    the potential's (y, d2y) pairs of the primitive fallback) is staged into
+//    shared memory once per launch by a bulk TMA copy (cp.async.bulk)
+//    completing on an mbarrier; tricubic node tables stay in L2/HBM.
+//  * No unbounded waits: the mbarrier waits (table staging, stage
+//    reductions) and the Gaussian rejection loop carry iteration caps that
+//    set the status word and stop the run.
 #include <cooperative_groups.h>
 #include <cuda_runtime.h>
 
